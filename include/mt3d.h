@@ -1,0 +1,168 @@
+/*
+ * mt3d.h -- C ABI of the B200-native 3D magnetotelluric forward/adjoint
+ * solver (libmt3d.so).
+ *
+ * The library replaces the solver calls of ModEM's 3D-MT forward problem:
+ * the model-operator set-up (modelOperator3D), the Krylov call BICG/cuBiCG
+ * and the driver FWDsolve3D with its divergence correction SdivCorr.  The
+ * Fortran host keeps its types; a thin ISO_C_BINDING shim
+ * flattens them with getCVector and calls the functions below.
+ *
+ * Conventions
+ *  - Complex arrays are interleaved (re, im) doubles, i.e. the memory layout
+ *    of Fortran complex(kind=8) and C double _Complex.
+ *  - A "full edge vector" has nE = nx(ny+1)(nz+1) + (nx+1)ny(nz+1) +
+ *    (nx+1)(ny+1)nz complex entries in ModEM's getCVector order
+ *    (f90/3D_MT/SP_Topology/vecTranslate.f90:41-79): all x-edges, then all
+ *    y-edges, then all z-edges, each block column-major (x fastest).
+ *  - An "interior vector" has nEi entries: the interior edges in ascending
+ *    full-edge order, i.e. the EDGEi list of boundaryIndex
+ *    (vecTranslate.f90:436-526).
+ *  - Model parameters are ln(sigma) (paramType LOGE) of the nx*ny*nzEarth
+ *    earth cells, x fastest; the air cells take exp(airCond).
+ *  - Every function returns an mt3d_status; nothing aborts the host process.
+ *    mt3d_last_error() returns the message of the last failure on a handle.
+ *  - A handle owns one CUDA stream and its device memory; it is not thread
+ *    safe.  Host buffers are only borrowed for the duration of a call.
+ */
+#ifndef MT3D_H
+#define MT3D_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define MT3D_API __attribute__((visibility("default")))
+#else
+#define MT3D_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct mt3d_solver *mt3d_handle;
+
+typedef enum {
+    MT3D_OK = 0,               /* converged */
+    MT3D_NOT_CONVERGED = 1,    /* iteration limits reached; best iterate returned */
+    MT3D_BREAKDOWN = 2,        /* Krylov breakdown (rho, alpha, omega or beta zero) */
+    MT3D_NAN_INPUT = 3,        /* NaN/Inf in the right-hand side or model */
+    MT3D_CUDA_ERROR = 4,       /* a CUDA runtime call failed */
+    MT3D_INVALID_ARGUMENT = 5, /* bad sizes, null pointers, unknown options */
+    MT3D_DEVICE_TIMEOUT = 6,   /* a bounded device-side wait gave up */
+    MT3D_NO_DEVICE = 7,        /* no usable CUDA device / library built without one */
+    MT3D_OUT_OF_MEMORY = 8
+} mt3d_status;
+
+/* Krylov solver and precision choices */
+enum { MT3D_SOLVER_BICG = 1 };
+enum { MT3D_PREC_FP64 = 0, MT3D_PREC_MIXED = 1 };
+
+/* Library version string. */
+MT3D_API const char *mt3d_version(void);
+
+/* Number of CUDA devices visible (0 when none); replaces kernelc_getDevNum
+ * (f90/3D_MT/FWD_SP2/kernel_c.cu:463-500). */
+MT3D_API int mt3d_device_count(void);
+
+/* Create a solver for one grid on device `device_id`.  Replaces
+ * ModelDataInit + ModelOperatorSetUp (f90/3D_MT/FWD/modelOperator3D.f90:139-175,
+ * f90/3D_MT/FWD/EMsolve3D.f90:497-512): metric elements and the curl-curl
+ * coefficients are set up here.  dz lists the nzAir air layers first. */
+MT3D_API int mt3d_create(int device_id, int nx, int ny, int nz, int nzAir, const double *dx, const double *dy,
+                const double *dz, mt3d_handle *out);
+
+/* Release all device memory of the handle (ModelDataCleanUp,
+ * f90/3D_MT/FWD/modelOperator3D.f90:177-194). */
+MT3D_API int mt3d_destroy(mt3d_handle h);
+
+/* Solver control (setEMsolveControl / readEMsolveControl,
+ * f90/3D_MT/FWD/EMsolve3D.f90:690-844): iterations per divergence correction,
+ * maximum number of divergence corrections, maximum PCG iterations per
+ * correction, forward / adjoint / div-correction tolerances, Krylov solver
+ * (MT3D_SOLVER_BICG) and precision (MT3D_PREC_FP64 or MT3D_PREC_MIXED: complex
+ * FP32 inner iterations wrapped in FP64 iterative refinement). */
+MT3D_API int mt3d_set_control(mt3d_handle h, int IterPerDivCor, int MaxDivCor, int MaxIterDivCor, double tolEMfwd,
+                     double tolEMadj, double tolDivCor, int solver, int precision);
+
+/* Set the conductivity model (UpdateCond, f90/3D_MT/FWD/modelOperator3D.f90:
+ * 211-232): ModelParamToEdge (LOGE, ModelMap.inc:88-188) and DivCorrSetUp. */
+MT3D_API int mt3d_update_cond(mt3d_handle h, const double *m_earth, double airCond);
+
+/* Set the angular frequency (UpdateFreq, f90/3D_MT/FWD/modelOperator3D.f90:
+ * 196-204). */
+MT3D_API int mt3d_update_freq(mt3d_handle h, double omega);
+
+/* Sizes: number of edges, interior edges and nodes. */
+MT3D_API int mt3d_sizes(mt3d_handle h, int64_t *nE, int64_t *nEi, int64_t *nN);
+
+/* Interior edge list EDGEi, 1-based like the Fortran (boundaryIndex,
+ * f90/3D_MT/SP_Topology/vecTranslate.f90:436-526); `edgei` holds nEi entries. */
+MT3D_API int mt3d_interior_index(mt3d_handle h, int32_t *edgei);
+
+/* y = A x on interior vectors, A = V_E (curl curl + ISIGN i omega mu0 sigma)
+ * (Mult_Aii, f90/3D_MT/FWD_SP2/modelOperator3D.f90:415-436; the same
+ * operator as MultA_N, f90/3D_MT/FWD/modelOperator3D.f90:879-918).  With
+ * adjt != 0 the conjugate-transposed operator is applied. */
+MT3D_API int mt3d_mult_aii(mt3d_handle h, int adjt, const double *x, double *y);
+
+/* One Krylov call on the interior system A x = b: BICG(b, x, KSSiter,
+ * device_id) -> cuBiCG (f90/3D_MT/FWD_SP2/EMsolve3D.f90:369-387,
+ * f90/3D_MT/FWD_SP2/solver.f90:931-2009; algorithm of BICG,
+ * f90/3D_MT/FWD/solver.f90:346-555) with the diagonal preconditioner.
+ * b and x are interior vectors; x holds the initial guess on entry and the
+ * solution (or the best iterate) on return.  rerr (maxit entries, may be
+ * NULL) receives the relative residual of every iteration; *niter and
+ * *failed mirror KSSiter%niter and KSSiter%failed. */
+MT3D_API int mt3d_bicg(mt3d_handle h, const double *b, double *x, int maxit, double tol, int *niter, double *rerr,
+              int *failed);
+
+/* The forward or transposed solve FWDsolve3D (f90/3D_MT/FWD/EMsolve3D.f90:
+ * 116-391, entry point of f90/3D_MT/FWD_SP2/EMsolve3D.f90:129-501).
+ *   trans = 0: forward problem; bc (full edge vector, boundary entries used)
+ *              holds the tangential boundary field, src (full edge vector,
+ *              interior entries used, may be NULL) an interior source already
+ *              multiplied by -ISIGN i omega mu0.
+ *   trans = 1: transposed problem; src is the adjoint source (required), bc
+ *              optional boundary data.
+ *   e: full edge vector; interior entries are the initial guess on entry, the
+ *      solution on return (boundary entries as in the reference's post-
+ *      processing).
+ * Returns MT3D_OK when converged. */
+MT3D_API int mt3d_fwdsolve(mt3d_handle h, int trans, const double *bc, const double *src, double *e);
+
+/* Batched FWDsolve3D: nrhs independent right-hand sides on the handle's grid
+ * and model, each with its own angular frequency omegas[r] and transposition
+ * flag trans[r], solved together.  bc and src hold nrhs full edge vectors each
+ * (either may be NULL; an individual vector may be all zero); e holds nrhs full
+ * edge vectors (initial guess in, solution out); status[r] receives each
+ * right-hand side's mt3d_status.  The handle's frequency (mt3d_update_freq) is
+ * left unchanged. */
+MT3D_API int mt3d_fwdsolve_batch(mt3d_handle h, int nrhs, const double *omegas, const int *trans, const double *bc,
+                        const double *src, double *e, int *status);
+
+/* Solver diagnostics of the last mt3d_fwdsolve (getEMsolveDiag,
+ * f90/3D_MT/FWD/EMsolve3D.f90:866-876): total Krylov iterations, number of
+ * divergence corrections, failure flag, the relative residual history
+ * EMrelErr (up to len entries), divJ before/after each correction (pairs, up
+ * to lenDivJ pairs) and the relative residual of the returned field. */
+MT3D_API int mt3d_get_diag(mt3d_handle h, int *nIterTotal, int *nDivCor, int *failed, double *EMrelErr, int len,
+                  double *divJ, int lenDivJ, double *final_relres);
+
+/* Gradient with respect to ln(sigma) of the earth cells from background
+ * fields e0 and adjoint fields eadj of npol polarisations (npol full edge
+ * vectors each) at the handle's frequency: PmultT (f90/3D_MT/SolverSens.f90:
+ * 63-116) followed by dEdgeToModelParam (f90/3D_MT/modelParam/ModelMap.inc:
+ * 302-374).  m0_earth is the background model; dm receives nx*ny*nzEarth
+ * values. */
+MT3D_API int mt3d_pmult_t(mt3d_handle h, int npol, const double *e0, const double *eadj, const double *m0_earth,
+                 double *dm);
+
+/* Message of the last error on the handle (NUL-terminated, truncated to len). */
+MT3D_API int mt3d_last_error(mt3d_handle h, char *buf, int len);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MT3D_H */

@@ -1,0 +1,216 @@
+// capi.cu -- extern "C" entry points of libmt3d.so (declared in include/mt3d.h).
+// Each call validates its arguments, runs on the handle's device and
+// returns an mt3d_status; exceptions never cross the boundary.
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "../../include/mt3d.h"
+#include "solver.h"
+
+struct mt3d_solver {
+    mt3d::Solver s;
+    int device = 0;
+};
+
+namespace {
+thread_local std::string g_create_error;
+
+int guard_device(mt3d_handle h)
+{
+    if (!h) return MT3D_INVALID_ARGUMENT;
+    if (cudaSetDevice(h->device) != cudaSuccess) {
+        cudaGetLastError();
+        h->s.last_error = "cudaSetDevice failed";
+        return MT3D_CUDA_ERROR;
+    }
+    return 0;
+}
+
+template <typename F> int wrap(mt3d_handle h, F &&f)
+{
+    int rc = guard_device(h);
+    if (rc) return rc;
+    try {
+        return f();
+    } catch (const std::bad_alloc &) {
+        h->s.last_error = "host out of memory";
+        return MT3D_OUT_OF_MEMORY;
+    } catch (...) {
+        h->s.last_error = "unexpected exception";
+        return MT3D_CUDA_ERROR;
+    }
+}
+}  // namespace
+
+extern "C" {
+
+const char *mt3d_version(void) { return "mt3d-b200 0.1 (sm_100a)"; }
+
+int mt3d_device_count(void)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+int mt3d_create(int device_id, int nx, int ny, int nz, int nzAir, const double *dx, const double *dy, const double *dz,
+                mt3d_handle *out)
+{
+    if (!out) return MT3D_INVALID_ARGUMENT;
+    *out = nullptr;
+    mt3d_solver *h = nullptr;
+    try {
+        h = new mt3d_solver();
+    } catch (...) {
+        g_create_error = "host out of memory";
+        return MT3D_OUT_OF_MEMORY;
+    }
+    h->device = device_id;
+    int rc = h->s.create(device_id, nx, ny, nz, nzAir, dx, dy, dz);
+    if (rc) {
+        g_create_error = h->s.last_error;
+        delete h;
+        return rc;
+    }
+    *out = h;
+    return MT3D_OK;
+}
+
+int mt3d_destroy(mt3d_handle h)
+{
+    if (!h) return MT3D_INVALID_ARGUMENT;
+    cudaSetDevice(h->device);
+    delete h;
+    return MT3D_OK;
+}
+
+int mt3d_set_control(mt3d_handle h, int IterPerDivCor, int MaxDivCor, int MaxIterDivCor, double tolEMfwd,
+                     double tolEMadj, double tolDivCor, int solver, int precision)
+{
+    if (!h) return MT3D_INVALID_ARGUMENT;
+    if (IterPerDivCor < 1 || MaxDivCor < 1 || MaxIterDivCor < 1 || !(tolEMfwd > 0) || !(tolEMadj > 0) ||
+        !(tolDivCor > 0)) {
+        h->s.last_error = "mt3d_set_control: iteration counts must be >= 1 and tolerances > 0";
+        return MT3D_INVALID_ARGUMENT;
+    }
+    if (solver != MT3D_SOLVER_BICG) {
+        h->s.last_error = "mt3d_set_control: only the BICG solver is implemented on the device";
+        return MT3D_INVALID_ARGUMENT;
+    }
+    if (precision != MT3D_PREC_FP64 && precision != MT3D_PREC_MIXED) {
+        h->s.last_error = "mt3d_set_control: unknown precision mode";
+        return MT3D_INVALID_ARGUMENT;
+    }
+    mt3d::Control &c = h->s.ctl;
+    c.IterPerDivCor = IterPerDivCor;
+    c.MaxDivCor = MaxDivCor;
+    c.MaxIterDivCor = MaxIterDivCor;
+    c.tolEMfwd = tolEMfwd;
+    c.tolEMadj = tolEMadj;
+    c.tolDivCor = tolDivCor;
+    c.solver = solver;
+    c.precision = precision;
+    return MT3D_OK;
+}
+
+int mt3d_update_cond(mt3d_handle h, const double *m_earth, double airCond)
+{
+    return wrap(h, [&] { return h->s.update_cond(m_earth, airCond); });
+}
+
+int mt3d_update_freq(mt3d_handle h, double omega)
+{
+    return wrap(h, [&] { return h->s.update_freq(omega); });
+}
+
+int mt3d_sizes(mt3d_handle h, int64_t *nE, int64_t *nEi, int64_t *nN)
+{
+    if (!h) return MT3D_INVALID_ARGUMENT;
+    if (nE) *nE = h->s.nE;
+    if (nEi) *nEi = h->s.nEi;
+    if (nN) *nN = h->s.nN;
+    return MT3D_OK;
+}
+
+int mt3d_interior_index(mt3d_handle h, int32_t *edgei)
+{
+    if (!h || !edgei) return MT3D_INVALID_ARGUMENT;
+    for (size_t i = 0; i < h->s.edgei.size(); i++) edgei[i] = h->s.edgei[i] + 1;
+    return MT3D_OK;
+}
+
+int mt3d_mult_aii(mt3d_handle h, int adjt, const double *x, double *y)
+{
+    return wrap(h, [&] { return h->s.mult_aii(adjt, x, y); });
+}
+
+int mt3d_bicg(mt3d_handle h, const double *b, double *x, int maxit, double tol, int *niter, double *rerr, int *failed)
+{
+    return wrap(h, [&] { return h->s.bicg(b, x, maxit, tol, niter, rerr, failed); });
+}
+
+int mt3d_fwdsolve(mt3d_handle h, int trans, const double *bc, const double *src, double *e)
+{
+    return wrap(h, [&] {
+        if (trans && !src) {
+            // the reference returns the boundary data (or zero) when the
+            // transposed problem has no source (EMsolve3D.f90:170-181)
+        }
+        double om = h->s.omega;
+        if (!(om > 0)) {
+            h->s.last_error = "mt3d_fwdsolve: frequency not set (call mt3d_update_freq)";
+            return (int)MT3D_INVALID_ARGUMENT;
+        }
+        int tr = trans ? 1 : 0, st = 0;
+        return h->s.solve(1, &om, &tr, bc, src, e, &st);
+    });
+}
+
+int mt3d_fwdsolve_batch(mt3d_handle h, int nrhs, const double *omegas, const int *trans, const double *bc,
+                        const double *src, double *e, int *status)
+{
+    return wrap(h, [&] { return h->s.solve(nrhs, omegas, trans, bc, src, e, status); });
+}
+
+int mt3d_get_diag(mt3d_handle h, int *nIterTotal, int *nDivCor, int *failed, double *EMrelErr, int len, double *divJ,
+                  int lenDivJ, double *final_relres)
+{
+    if (!h) return MT3D_INVALID_ARGUMENT;
+    const mt3d::Diag &d = h->s.diag;
+    if (nIterTotal) *nIterTotal = d.nIterTotal;
+    if (nDivCor) *nDivCor = d.nDivCor;
+    if (failed) *failed = d.failed;
+    if (EMrelErr && len > 0) {
+        const int n = std::min<int>(len, (int)d.EMrelErr.size());
+        std::memcpy(EMrelErr, d.EMrelErr.data(), n * sizeof(double));
+        for (int i = n; i < len; i++) EMrelErr[i] = 0.0;
+    }
+    if (divJ && lenDivJ > 0) {
+        const int n = std::min<int>(2 * lenDivJ, (int)d.divJ.size());
+        std::memcpy(divJ, d.divJ.data(), n * sizeof(double));
+        for (int i = n; i < 2 * lenDivJ; i++) divJ[i] = 0.0;
+    }
+    if (final_relres) *final_relres = d.final_relres;
+    return MT3D_OK;
+}
+
+int mt3d_pmult_t(mt3d_handle h, int npol, const double *e0, const double *eadj, const double *m0_earth, double *dm)
+{
+    return wrap(h, [&] { return h->s.pmult_t(npol, e0, eadj, m0_earth, dm); });
+}
+
+int mt3d_last_error(mt3d_handle h, char *buf, int len)
+{
+    if (!buf || len < 1) return MT3D_INVALID_ARGUMENT;
+    const std::string &m = h ? h->s.last_error : g_create_error;
+    const int n = std::min<int>(len - 1, (int)m.size());
+    std::memcpy(buf, m.data(), n);
+    buf[n] = '\0';
+    return MT3D_OK;
+}
+
+}  // extern "C"

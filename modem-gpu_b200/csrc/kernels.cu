@@ -1,0 +1,1025 @@
+// kernels.cu -- CUDA kernels of the 3D-MT forward/adjoint solve (sm_100a).
+//
+// All kernels are batched over right-hand sides: blockIdx.y selects the
+// right-hand side, blockIdx.x a contiguous chunk of edges (or nodes).  Every
+// Krylov scalar lives in device memory (BicgState / PcgState); the last
+// block of each right-hand side reduces the block partials in a fixed order
+// and updates the scalars, so an iteration needs no host synchronisation and
+// is bitwise reproducible.  A right-hand side whose state is not RUNNING is
+// skipped by every block.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace mt3d {
+
+__device__ __forceinline__ int chunk_begin(int chunk) { return blockIdx.x * chunk + threadIdx.x; }
+
+template <typename T> __device__ __forceinline__ T dterm_of(const Geo<T> &g, const EdgeIdx &q, T wmu, T sig)
+{
+    return wmu * sig * edge_volume(g, q);
+}
+
+// ph = v / d, d = V_E*ccdiag + i*dterm (diagonal of A)
+template <typename T> __device__ __forceinline__ C2<T> jacobi(const Geo<T> &g, const EdgeIdx &q, T dterm, C2<T> v)
+{
+    const T dr = cc_diag(g, q), di = dterm;
+    const T inv = T(1) / (dr * dr + di * di);
+    return mk<T>((v.x * dr + v.y * di) * inv, (v.y * dr - v.x * di) * inv);
+}
+
+template <typename T> __device__ __forceinline__ T rhs_wmu(const KArgs<T> &a, int r)
+{
+    return (T)(a.dsgn * a.ost[r].omega * kMu0);
+}
+
+// ---------------------------------------------------------------------------
+// operator apply: y = A x (interior; boundary of y set to zero).  Optional
+// mode 1: y = b - A x with reduction of |y|^2 into parts (no finalisation).
+// ---------------------------------------------------------------------------
+template <typename T> __global__ void __launch_bounds__(kThreads) k_apply(KArgs<T> a, const C2<T> *x, C2<T> *y, int neg)
+{
+    const int r = blockIdx.y;
+    const size_t off = (size_t)r * a.stride;
+    const Geo<T> &g = a.g;
+    const T wmu = rhs_wmu(a, r);
+    const int end = min((blockIdx.x + 1) * a.chunk, g.nE);
+    for (int e = chunk_begin(a.chunk); e < end; e += kThreads) {
+        EdgeIdx q = edge_decode(g, e);
+        C2<T> out = mk<T>(0, 0);
+        if (edge_interior(g, q)) {
+            out = stencil(g, x + off, q, dterm_of(g, q, wmu, a.sigma[e]));
+            if (neg) { out.x = -out.x; out.y = -out.y; }
+        }
+        y[off + e] = out;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// BiCGStab (f90/3D_MT/FWD/solver.f90:346-555) with the diagonal preconditioner
+// applied where M1solve/M2solve sit (right preconditioning).
+// ---------------------------------------------------------------------------
+
+// start of a call: r = b - A x, rt = r; |b|^2, |r|^2
+template <typename T> __global__ void __launch_bounds__(kThreads) kb_init(KArgs<T> a)
+{
+    const int r = blockIdx.y;
+    BicgState &st = a.st[r];
+    if (!a.ost[r].active) return;
+    const size_t off = (size_t)r * a.stride;
+    const Geo<T> &g = a.g;
+    const T wmu = rhs_wmu(a, r);
+    const C2<T> *x = a.x0 + off;
+    double v[2] = {0.0, 0.0};
+    const int end = min((blockIdx.x + 1) * a.chunk, g.nE);
+    for (int e = chunk_begin(a.chunk); e < end; e += kThreads) {
+        EdgeIdx q = edge_decode(g, e);
+        C2<T> res = mk<T>(0, 0);
+        if (edge_interior(g, q)) {
+            C2<T> ax = stencil(g, x, q, dterm_of(g, q, wmu, a.sigma[e]));
+            C2<T> bb = a.b[off + e];
+            res = csub(bb, ax);
+            v[0] += (double)bb.x * bb.x + (double)bb.y * bb.y;
+            v[1] += (double)res.x * res.x + (double)res.y * res.y;
+        }
+        a.r[off + e] = res;
+        a.rt[off + e] = res;
+    }
+    double tot[2];
+    if (block_reduce_last<2>(v, a.parts, a.cnt, r, blockIdx.x, gridDim.x, tot) && threadIdx.x == 0) {
+        const double bnorm = sqrt(tot[0]), rnorm = sqrt(tot[1]);
+        double *rerr = a.rerr + (size_t)r * a.rerr_stride;
+        st.iter = 0;
+        st.maxit = a.maxit;
+        st.xcur = 0;
+        st.xbest = 0;
+        st.imin = 0;
+        st.first = 1;
+        st.bnorm = bnorm;
+        st.rnorm = rnorm;
+        st.rnormin = rnorm;
+        st.btol = (a.inner ? a.ost[r].tol_inner : a.ost[r].tol) * bnorm;
+        st.rho1 = {1.0, 0.0};
+        st.omega = {1.0, 0.0};
+        st.alpha = {0.0, 0.0};
+        st.rho = {tot[1], 0.0};
+        if (!isfinite(bnorm)) {
+            st.status = KS_NAN;
+        } else if (bnorm == 0.0) {
+            st.status = KS_CONVERGED;  // zero right-hand side: zero solution
+            st.xbest = -1;
+            st.iter = 1;
+            rerr[0] = 0.0;
+        } else if (rnorm <= st.btol) {
+            st.status = KS_CONVERGED;  // the first guess is already good enough
+            st.iter = 1;
+            rerr[0] = rnorm / bnorm;
+        } else {
+            st.status = KS_RUNNING;
+            rerr[0] = rnorm / bnorm;
+            if (tot[1] == 0.0) st.status = KS_BREAKDOWN;
+        }
+    }
+}
+
+// p = r (first iteration) or p = r + beta (p - omega v); ph = M^-1 p
+template <typename T> __global__ void __launch_bounds__(kThreads) kb_p(KArgs<T> a)
+{
+    const int r = blockIdx.y;
+    const BicgState &st = a.st[r];
+    if (st.status != KS_RUNNING || !a.ost[r].active) return;
+    const size_t off = (size_t)r * a.stride;
+    const Geo<T> &g = a.g;
+    const T wmu = rhs_wmu(a, r);
+    const bool first = st.first;
+    const C2<T> beta = mk<T>((T)st.beta.re, (T)st.beta.im);
+    const C2<T> om = mk<T>((T)st.omega.re, (T)st.omega.im);
+    const int end = min((blockIdx.x + 1) * a.chunk, g.nE);
+    for (int e = chunk_begin(a.chunk); e < end; e += kThreads) {
+        C2<T> rr = a.r[off + e];
+        C2<T> p;
+        if (first) {
+            p = rr;
+        } else {
+            C2<T> pv = csub(a.p[off + e], cmul(om, a.v[off + e]));
+            p = cadd(rr, cmul(beta, pv));
+        }
+        a.p[off + e] = p;
+        EdgeIdx q = edge_decode(g, e);
+        C2<T> ph = mk<T>(0, 0);
+        if (edge_interior(g, q)) ph = jacobi(g, q, dterm_of(g, q, wmu, a.sigma[e]), p);
+        a.ph[off + e] = ph;
+    }
+}
+
+// v = A ph; rtv = rt . v ; alpha = rho / rtv
+template <typename T> __global__ void __launch_bounds__(kThreads) kb_v(KArgs<T> a)
+{
+    const int r = blockIdx.y;
+    BicgState &st = a.st[r];
+    if (st.status != KS_RUNNING || !a.ost[r].active) return;
+    const size_t off = (size_t)r * a.stride;
+    const Geo<T> &g = a.g;
+    const T wmu = rhs_wmu(a, r);
+    double v[2] = {0.0, 0.0};
+    const int end = min((blockIdx.x + 1) * a.chunk, g.nE);
+    for (int e = chunk_begin(a.chunk); e < end; e += kThreads) {
+        EdgeIdx q = edge_decode(g, e);
+        C2<T> out = mk<T>(0, 0);
+        if (edge_interior(g, q)) {
+            out = stencil(g, a.ph + off, q, dterm_of(g, q, wmu, a.sigma[e]));
+            C2<T> t = a.rt[off + e];
+            v[0] += (double)t.x * out.x + (double)t.y * out.y;  // conj(rt)*v
+            v[1] += (double)t.x * out.y - (double)t.y * out.x;
+        }
+        a.v[off + e] = out;
+    }
+    double tot[2];
+    if (block_reduce_last<2>(v, a.parts, a.cnt, r, blockIdx.x, gridDim.x, tot) && threadIdx.x == 0) {
+        cd rtv = {tot[0], tot[1]};
+        if (!cd_finite(rtv)) { st.status = KS_NAN; return; }
+        if (cd_zero(rtv)) { st.status = KS_BREAKDOWN; return; }
+        st.alpha = cd_div(st.rho, rtv);
+        if (cd_zero(st.alpha)) st.status = KS_BREAKDOWN;
+    }
+}
+
+// s = r - alpha v ; sh = M^-1 s
+template <typename T> __global__ void __launch_bounds__(kThreads) kb_s(KArgs<T> a)
+{
+    const int r = blockIdx.y;
+    const BicgState &st = a.st[r];
+    if (st.status != KS_RUNNING || !a.ost[r].active) return;
+    const size_t off = (size_t)r * a.stride;
+    const Geo<T> &g = a.g;
+    const T wmu = rhs_wmu(a, r);
+    const C2<T> al = mk<T>((T)st.alpha.re, (T)st.alpha.im);
+    const int end = min((blockIdx.x + 1) * a.chunk, g.nE);
+    for (int e = chunk_begin(a.chunk); e < end; e += kThreads) {
+        C2<T> s = csub(a.r[off + e], cmul(al, a.v[off + e]));
+        a.s[off + e] = s;
+        EdgeIdx q = edge_decode(g, e);
+        C2<T> sh = mk<T>(0, 0);
+        if (edge_interior(g, q)) sh = jacobi(g, q, dterm_of(g, q, wmu, a.sigma[e]), s);
+        a.sh[off + e] = sh;
+    }
+}
+
+// t = A sh ; ts = t . s, tt = t . t ; omega = ts / tt
+template <typename T> __global__ void __launch_bounds__(kThreads) kb_t(KArgs<T> a)
+{
+    const int r = blockIdx.y;
+    BicgState &st = a.st[r];
+    if (st.status != KS_RUNNING || !a.ost[r].active) return;
+    const size_t off = (size_t)r * a.stride;
+    const Geo<T> &g = a.g;
+    const T wmu = rhs_wmu(a, r);
+    double v[3] = {0.0, 0.0, 0.0};
+    const int end = min((blockIdx.x + 1) * a.chunk, g.nE);
+    for (int e = chunk_begin(a.chunk); e < end; e += kThreads) {
+        EdgeIdx q = edge_decode(g, e);
+        C2<T> out = mk<T>(0, 0);
+        if (edge_interior(g, q)) {
+            out = stencil(g, a.sh + off, q, dterm_of(g, q, wmu, a.sigma[e]));
+            C2<T> s = a.s[off + e];
+            v[0] += (double)out.x * s.x + (double)out.y * s.y;  // conj(t)*s
+            v[1] += (double)out.x * s.y - (double)out.y * s.x;
+            v[2] += (double)out.x * out.x + (double)out.y * out.y;
+        }
+        a.t[off + e] = out;
+    }
+    double tot[3];
+    if (block_reduce_last<3>(v, a.parts, a.cnt, r, blockIdx.x, gridDim.x, tot) && threadIdx.x == 0) {
+        if (!isfinite(tot[0]) || !isfinite(tot[1]) || !isfinite(tot[2])) { st.status = KS_NAN; return; }
+        if (tot[2] == 0.0) { st.status = KS_BREAKDOWN; return; }
+        cd ts = {tot[0], tot[1]};
+        st.omega = {ts.re / tot[2], ts.im / tot[2]};
+        if (cd_zero(st.omega)) st.status = KS_BREAKDOWN;
+    }
+}
+
+// x += alpha ph + omega sh (into the buffer that does not hold the best
+// iterate); r = s - omega t; |r|, rho = rt . r ; convergence, best iterate,
+// beta for the next iteration
+template <typename T> __global__ void __launch_bounds__(kThreads) kb_xr(KArgs<T> a)
+{
+    const int r = blockIdx.y;
+    BicgState &st = a.st[r];
+    if (st.status != KS_RUNNING || !a.ost[r].active) return;
+    const size_t off = (size_t)r * a.stride;
+    const Geo<T> &g = a.g;
+    const C2<T> al = mk<T>((T)st.alpha.re, (T)st.alpha.im);
+    const C2<T> om = mk<T>((T)st.omega.re, (T)st.omega.im);
+    const int cur = st.xcur, dst = (st.xcur == st.xbest) ? 1 - st.xcur : st.xcur;
+    const C2<T> *xs = (cur == 0 ? a.x0 : a.x1) + off;
+    C2<T> *xd = (dst == 0 ? a.x0 : a.x1) + off;
+    double v[3] = {0.0, 0.0, 0.0};
+    const int end = min((blockIdx.x + 1) * a.chunk, g.nE);
+    for (int e = chunk_begin(a.chunk); e < end; e += kThreads) {
+        C2<T> xn = cadd(cadd(xs[e], cmul(al, a.ph[off + e])), cmul(om, a.sh[off + e]));
+        xd[e] = xn;
+        C2<T> rn = csub(a.s[off + e], cmul(om, a.t[off + e]));
+        a.r[off + e] = rn;
+        C2<T> t = a.rt[off + e];
+        v[0] += (double)rn.x * rn.x + (double)rn.y * rn.y;
+        v[1] += (double)t.x * rn.x + (double)t.y * rn.y;  // conj(rt)*r
+        v[2] += (double)t.x * rn.y - (double)t.y * rn.x;
+    }
+    double tot[3];
+    if (block_reduce_last<3>(v, a.parts, a.cnt, r, blockIdx.x, gridDim.x, tot) && threadIdx.x == 0) {
+        double *rerr = a.rerr + (size_t)r * a.rerr_stride;
+        const double rnorm = sqrt(tot[0]);
+        st.iter += 1;
+        st.xcur = dst;
+        st.first = 0;
+        st.rnorm = rnorm;
+        rerr[st.iter - 1] = rnorm / st.bnorm;
+        if (!isfinite(rnorm)) { st.status = KS_NAN; return; }
+        if (rnorm < st.btol) {
+            st.status = KS_CONVERGED;
+            st.xbest = dst;
+            return;
+        }
+        if (rnorm < st.rnormin) {
+            st.rnormin = rnorm;
+            st.xbest = dst;
+            st.imin = st.iter;
+        }
+        if (st.iter >= st.maxit) {
+            st.status = KS_MAXIT;
+            return;
+        }
+        cd rho_new = {tot[1], tot[2]};
+        st.rho1 = st.rho;
+        st.rho = rho_new;
+        if (cd_zero(st.rho)) { st.status = KS_BREAKDOWN; return; }
+        st.beta = cd_mul(cd_div(st.rho, st.rho1), cd_div(st.alpha, st.omega));
+        if (cd_zero(st.beta)) st.status = KS_BREAKDOWN;
+    }
+}
+
+// end of a call: bring the returned iterate (best iterate unless converged)
+// into x0; zero solution for a zero right-hand side
+template <typename T> __global__ void __launch_bounds__(kThreads) kb_finish(KArgs<T> a)
+{
+    const int r = blockIdx.y;
+    const BicgState &st = a.st[r];
+    if (!a.ost[r].active) return;
+    const size_t off = (size_t)r * a.stride;
+    const int end = min((blockIdx.x + 1) * a.chunk, a.g.nE);
+    if (st.xbest == -1) {
+        for (int e = chunk_begin(a.chunk); e < end; e += kThreads) a.x0[off + e] = mk<T>(0, 0);
+    } else if (st.xbest == 1) {
+        for (int e = chunk_begin(a.chunk); e < end; e += kThreads) a.x0[off + e] = a.x1[off + e];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// divergence correction (SdivCorr, f90/3D_MT/FWD/EMsolve3D.f90:403-492) with
+// PCG (f90/3D_MT/FWD/solver.f90:40-118) on DivCgrad and a diagonal
+// preconditioner, FP64 throughout.
+// ---------------------------------------------------------------------------
+
+// DivC (f90/3D_MT/FWD/modelOperator3D.f90:1817-1925) at interior node (i,j,k)
+__device__ __forceinline__ double2 divc_node(const DArgs &a, const double2 *E, int i, int j, int k)
+{
+    const Geo<double> &g = a.g;
+    const double *s = a.sigma;
+    const double rx = 1.0 / g.delX[i], ry = 1.0 / g.delY[j], rz = 1.0 / g.delZ[k];
+    const int kz = k + 1;  // 1-based iz
+    const int ex = iX(g, i, j, k), exm = iX(g, i - 1, j, k);
+    const int ey = iY(g, i, j, k), eym = iY(g, i, j - 1, k);
+    const int ez = iZ(g, i, j, k), ezm = iZ(g, i, j, k - 1);
+    double2 o;
+    if (kz <= g.nzAir) {
+        const double sa = kSigmaAir;
+        o.x = sa * (E[ex].x - E[exm].x) * rx + sa * (E[ey].x - E[eym].x) * ry + sa * (E[ez].x - E[ezm].x) * rz;
+        o.y = sa * (E[ex].y - E[exm].y) * rx + sa * (E[ey].y - E[eym].y) * ry + sa * (E[ez].y - E[ezm].y) * rz;
+    } else {
+        const double szm = (kz == g.nzAir + 1) ? kSigmaAir : s[ezm];
+        o.x = (s[ex] * E[ex].x - s[exm] * E[exm].x) * rx + (s[ey] * E[ey].x - s[eym] * E[eym].x) * ry +
+              (s[ez] * E[ez].x - szm * E[ezm].x) * rz;
+        o.y = (s[ex] * E[ex].y - s[exm] * E[exm].y) * rx + (s[ey] * E[ey].y - s[eym] * E[eym].y) * ry +
+              (s[ez] * E[ez].y - szm * E[ezm].y) * rz;
+    }
+    return o;
+}
+
+__device__ __forceinline__ bool node_interior(const Geo<double> &g, int i, int j, int k)
+{
+    return i >= 1 && i <= g.nx - 1 && j >= 1 && j <= g.ny - 1 && k >= 1 && k <= g.nz - 1;
+}
+__device__ __forceinline__ void node_decode(const Geo<double> &g, int n, int &i, int &j, int &k)
+{
+    i = n % (g.nx + 1);
+    int t = n / (g.nx + 1);
+    j = t % (g.ny + 1);
+    k = t / (g.ny + 1);
+}
+
+// phiRHS = V_N (DivC(E) - phi0); x = 0; r = b; divJ_before, ||b||, delta = r . M^-1 r
+__global__ void __launch_bounds__(kThreads) kd_rhs(DArgs a)
+{
+    const int r = blockIdx.y;
+    if (!a.ost[r].dc_run) return;
+    const size_t off = (size_t)r * a.stride;
+    const size_t eoff = (size_t)r * a.estride;
+    const Geo<double> &g = a.g;
+    double v[4] = {0, 0, 0, 0};
+    const int end = min((blockIdx.x + 1) * a.chunk, g.nN);
+    for (int n = chunk_begin(a.chunk); n < end; n += kThreads) {
+        int i, j, k;
+        node_decode(g, n, i, j, k);
+        double2 b = make_double2(0, 0);
+        if (node_interior(g, i, j, k)) {
+            double2 d = divc_node(a, a.E + eoff, i, j, k);
+            if (a.phi0) {
+                double2 p0 = a.phi0[off + n];
+                d.x -= p0.x;
+                d.y -= p0.y;
+            }
+            v[0] += d.x * d.x + d.y * d.y;
+            const double vn = g.delX[i] * g.delY[j] * g.delZ[k];
+            b = make_double2(vn * d.x, vn * d.y);
+            v[1] += b.x * b.x + b.y * b.y;
+            const double rc = 1.0 / a.coef[6 * (size_t)g.nN + n];
+            v[2] += (b.x * b.x + b.y * b.y) * rc;  // conj(r)*(r/c): real
+        }
+        a.pr[off + n] = b;
+        a.px[off + n] = make_double2(0, 0);
+        a.pp[off + n] = make_double2(0, 0);
+    }
+    double tot[4];
+    if (block_reduce_last<4>(v, a.parts, a.cnt, r, blockIdx.x, gridDim.x, tot) && threadIdx.x == 0) {
+        PcgState &st = a.pst[r];
+        OuterState &os = a.ost[r];
+        os.divJ[0] = sqrt(tot[0]);
+        st.bnorm = sqrt(tot[1]);
+        st.rnorm = st.bnorm;
+        st.iter = 1;
+        st.maxit = a.maxit;
+        st.tol = a.tol;
+        st.delta = {tot[2], 0.0};
+        st.deltaOld = {1.0, 0.0};
+        st.beta = {0.0, 0.0};
+        double *rerr = a.rerr + (size_t)r * a.rerr_stride;
+        const double rel = st.rnorm / st.bnorm;  // NaN for a zero right-hand side, as in the reference
+        rerr[0] = rel;
+        st.status = (rel > st.tol && st.iter < st.maxit) ? KS_RUNNING : KS_CONVERGED;
+    }
+}
+
+// p = M^-1 r + beta p
+__global__ void __launch_bounds__(kThreads) kd_p(DArgs a)
+{
+    const int r = blockIdx.y;
+    const PcgState &st = a.pst[r];
+    if (!a.ost[r].dc_run || st.status != KS_RUNNING) return;
+    const size_t off = (size_t)r * a.stride;
+    const Geo<double> &g = a.g;
+    const double2 be = make_double2(st.beta.re, st.beta.im);
+    const int end = min((blockIdx.x + 1) * a.chunk, g.nN);
+    for (int n = chunk_begin(a.chunk); n < end; n += kThreads) {
+        int i, j, k;
+        node_decode(g, n, i, j, k);
+        if (!node_interior(g, i, j, k)) continue;
+        const double rc = 1.0 / a.coef[6 * (size_t)g.nN + n];
+        double2 rr = a.pr[off + n];
+        double2 p = a.pp[off + n];
+        double2 s = make_double2(rr.x * rc, rr.y * rc);
+        a.pp[off + n] = cadd(s, cmul(be, p));
+    }
+}
+
+// q = DivCgrad p (f90/3D_MT/FWD/modelOperator3D.f90:1760-1810); alpha = delta / (p . q)
+__global__ void __launch_bounds__(kThreads) kd_q(DArgs a)
+{
+    const int r = blockIdx.y;
+    PcgState &st = a.pst[r];
+    if (!a.ost[r].dc_run || st.status != KS_RUNNING) return;
+    const size_t off = (size_t)r * a.stride;
+    const Geo<double> &g = a.g;
+    const double2 *p = a.pp + off;
+    double v[2] = {0, 0};
+    const int end = min((blockIdx.x + 1) * a.chunk, g.nN);
+    const int sx = 1, sy = g.nx + 1, sz = (g.nx + 1) * (g.ny + 1);
+    for (int n = chunk_begin(a.chunk); n < end; n += kThreads) {
+        int i, j, k;
+        node_decode(g, n, i, j, k);
+        double2 q = make_double2(0, 0);
+        if (node_interior(g, i, j, k)) {
+            const size_t N = (size_t)g.nN;
+            const double c0 = a.coef[n], c1 = a.coef[N + n], c2 = a.coef[2 * N + n], c3 = a.coef[3 * N + n];
+            const double c4 = a.coef[4 * N + n], c5 = a.coef[5 * N + n], c6 = a.coef[6 * N + n];
+            const double2 pc = p[n];
+            q.x = p[n + sx].x * c1 + p[n - sx].x * c0 + p[n + sy].x * c3 + p[n - sy].x * c2 + p[n + sz].x * c5 +
+                  p[n - sz].x * c4 + pc.x * c6;
+            q.y = p[n + sx].y * c1 + p[n - sx].y * c0 + p[n + sy].y * c3 + p[n - sy].y * c2 + p[n + sz].y * c5 +
+                  p[n - sz].y * c4 + pc.y * c6;
+            v[0] += pc.x * q.x + pc.y * q.y;  // conj(p)*q
+            v[1] += pc.x * q.y - pc.y * q.x;
+        }
+        a.pq[off + n] = q;
+    }
+    double tot[2];
+    if (block_reduce_last<2>(v, a.parts, a.cnt, r, blockIdx.x, gridDim.x, tot) && threadIdx.x == 0) {
+        cd pq = {tot[0], tot[1]};
+        st.alpha = cd_div(st.delta, pq);
+        if (!cd_finite(st.alpha)) st.status = KS_NAN;
+    }
+}
+
+// x += alpha p; r -= alpha q; rerr; delta_new = r . M^-1 r; beta
+__global__ void __launch_bounds__(kThreads) kd_xr(DArgs a)
+{
+    const int r = blockIdx.y;
+    PcgState &st = a.pst[r];
+    if (!a.ost[r].dc_run || st.status != KS_RUNNING) return;
+    const size_t off = (size_t)r * a.stride;
+    const Geo<double> &g = a.g;
+    const double2 al = make_double2(st.alpha.re, st.alpha.im);
+    double v[2] = {0, 0};
+    const int end = min((blockIdx.x + 1) * a.chunk, g.nN);
+    for (int n = chunk_begin(a.chunk); n < end; n += kThreads) {
+        int i, j, k;
+        node_decode(g, n, i, j, k);
+        if (!node_interior(g, i, j, k)) continue;
+        a.px[off + n] = cadd(a.px[off + n], cmul(al, a.pp[off + n]));
+        double2 rr = csub(a.pr[off + n], cmul(al, a.pq[off + n]));
+        a.pr[off + n] = rr;
+        const double m2 = rr.x * rr.x + rr.y * rr.y;
+        v[0] += m2;
+        v[1] += m2 / a.coef[6 * (size_t)g.nN + n];
+    }
+    double tot[2];
+    if (block_reduce_last<2>(v, a.parts, a.cnt, r, blockIdx.x, gridDim.x, tot) && threadIdx.x == 0) {
+        double *rerr = a.rerr + (size_t)r * a.rerr_stride;
+        st.iter += 1;
+        st.rnorm = sqrt(tot[0]);
+        const double rel = st.rnorm / st.bnorm;
+        rerr[st.iter - 1] = rel;
+        st.deltaOld = st.delta;
+        st.delta = {tot[1], 0.0};
+        st.beta = cd_div(st.delta, st.deltaOld);
+        if (!isfinite(rel)) st.status = KS_NAN;
+        else if (!(rel > st.tol && st.iter < st.maxit)) st.status = KS_CONVERGED;
+    }
+}
+
+// E -= Grad(phi) on interior edges (Grad, f90/FIELDS/FiniteDiff3D/sg_diff_oper.f90:98-200)
+__global__ void __launch_bounds__(kThreads) kd_grad(DArgs a)
+{
+    const int r = blockIdx.y;
+    if (!a.ost[r].dc_run) return;
+    const size_t off = (size_t)r * a.stride;
+    const size_t eoff = (size_t)r * a.estride;
+    const Geo<double> &g = a.g;
+    const double2 *phi = a.px + off;
+    double2 *E = a.E + eoff;
+    const int end = min((blockIdx.x + 1) * a.echunk, g.nE);
+    for (int e = chunk_begin(a.echunk); e < end; e += kThreads) {
+        EdgeIdx q = edge_decode(g, e);
+        if (!edge_interior(g, q)) continue;
+        double2 gr;
+        if (q.c == 0) {
+            const double2 a1 = phi[iN(g, q.i + 1, q.j, q.k)], a0 = phi[iN(g, q.i, q.j, q.k)];
+            gr = make_double2((a1.x - a0.x) / g.dx[q.i], (a1.y - a0.y) / g.dx[q.i]);
+        } else if (q.c == 1) {
+            const double2 a1 = phi[iN(g, q.i, q.j + 1, q.k)], a0 = phi[iN(g, q.i, q.j, q.k)];
+            gr = make_double2((a1.x - a0.x) / g.dy[q.j], (a1.y - a0.y) / g.dy[q.j]);
+        } else {
+            const double2 a1 = phi[iN(g, q.i, q.j, q.k + 1)], a0 = phi[iN(g, q.i, q.j, q.k)];
+            gr = make_double2((a1.x - a0.x) / g.dz[q.k], (a1.y - a0.y) / g.dz[q.k]);
+        }
+        E[e] = csub(E[e], gr);
+    }
+}
+
+// divJ after the correction: ||DivC(E) - phi0||
+__global__ void __launch_bounds__(kThreads) kd_divj(DArgs a)
+{
+    const int r = blockIdx.y;
+    if (!a.ost[r].dc_run) return;
+    const size_t off = (size_t)r * a.stride;
+    const size_t eoff = (size_t)r * a.estride;
+    const Geo<double> &g = a.g;
+    double v[1] = {0};
+    const int end = min((blockIdx.x + 1) * a.chunk, g.nN);
+    for (int n = chunk_begin(a.chunk); n < end; n += kThreads) {
+        int i, j, k;
+        node_decode(g, n, i, j, k);
+        if (!node_interior(g, i, j, k)) continue;
+        double2 d = divc_node(a, a.E + eoff, i, j, k);
+        if (a.phi0) {
+            d.x -= a.phi0[off + n].x;
+            d.y -= a.phi0[off + n].y;
+        }
+        v[0] += d.x * d.x + d.y * d.y;
+    }
+    double tot[1];
+    if (block_reduce_last<1>(v, a.parts, a.cnt, r, blockIdx.x, gridDim.x, tot) && threadIdx.x == 0) {
+        a.ost[r].divJ[1] = sqrt(tot[0]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// right-hand sides, post-processing, precision glue
+// ---------------------------------------------------------------------------
+
+// keep only the boundary entries of v (interior set to zero)
+__global__ void __launch_bounds__(kThreads) k_keep_boundary(Geo<double> g, double2 *v, size_t stride)
+{
+    const size_t off = (size_t)blockIdx.y * stride;
+    for (int e = blockIdx.x * kThreads + threadIdx.x; e < g.nE; e += gridDim.x * kThreads) {
+        EdgeIdx q = edge_decode(g, e);
+        if (edge_interior(g, q)) v[off + e] = make_double2(0, 0);
+    }
+}
+
+// keep only the interior entries of v (boundary set to zero)
+__global__ void __launch_bounds__(kThreads) k_keep_interior(Geo<double> g, double2 *v, size_t stride)
+{
+    const size_t off = (size_t)blockIdx.y * stride;
+    for (int e = blockIdx.x * kThreads + threadIdx.x; e < g.nE; e += gridDim.x * kThreads) {
+        EdgeIdx q = edge_decode(g, e);
+        if (!edge_interior(g, q)) v[off + e] = make_double2(0, 0);
+    }
+}
+
+// b += w * src on interior edges: w = V_E for a forward source, 1 for the
+// (already V_E-weighted) adjoint source of the transposed problem
+// (f90/3D_MT/FWD/EMsolve3D.f90:166-183, 202-218)
+__global__ void __launch_bounds__(kThreads) k_add_src(Geo<double> g, double2 *b, const double2 *src, size_t stride,
+                                                       const OuterState *ost)
+{
+    const int r = blockIdx.y;
+    if (!ost[r].has_src) return;
+    const bool tr = ost[r].trans != 0;
+    const size_t off = (size_t)r * stride;
+    for (int e = blockIdx.x * kThreads + threadIdx.x; e < g.nE; e += gridDim.x * kThreads) {
+        EdgeIdx q = edge_decode(g, e);
+        if (!edge_interior(g, q)) continue;
+        const double w = tr ? 1.0 : edge_volume(g, q);
+        b[off + e] = cadd(b[off + e], make_double2(w * src[off + e].x, w * src[off + e].y));
+    }
+}
+
+// phi0 = Div(w * src) / (i ISIGN mu0 omega) on interior nodes, w = 1/V_E when
+// divide_ve (transposed problem) else 1 (Div, sg_diff_oper.f90:26-93)
+__global__ void __launch_bounds__(kThreads) k_phi0(Geo<double> g, const double2 *src, size_t estride, double2 *phi0,
+                                                    size_t nstride, const OuterState *ost)
+{
+    const int r = blockIdx.y;
+    const size_t off = (size_t)r * nstride, eoff = (size_t)r * estride;
+    const OuterState &os = ost[r];
+    if (!os.has_src) return;
+    const bool dv = os.trans != 0;
+    // 1 / (i * ISIGN * mu0 * omega) = i / (mu0 * omega) for ISIGN = -1
+    const double inv = 1.0 / (kMu0 * os.omega);
+    for (int n = blockIdx.x * kThreads + threadIdx.x; n < g.nN; n += gridDim.x * kThreads) {
+        int i = n % (g.nx + 1), t = n / (g.nx + 1), j = t % (g.ny + 1), k = t / (g.ny + 1);
+        double2 out = make_double2(0, 0);
+        if (i >= 1 && i <= g.nx - 1 && j >= 1 && j <= g.ny - 1 && k >= 1 && k <= g.nz - 1) {
+            auto val = [&](int e, const EdgeIdx &q) {
+                double2 s = src[eoff + e];
+                if (!edge_interior(g, q)) return make_double2(0, 0);
+                if (dv) {
+                    double ve = edge_volume(g, q);
+                    s.x /= ve;
+                    s.y /= ve;
+                }
+                return s;
+            };
+            EdgeIdx q;
+            q = {0, i, j, k}; double2 ex = val(iX(g, i, j, k), q);
+            q = {0, i - 1, j, k}; double2 exm = val(iX(g, i - 1, j, k), q);
+            q = {1, i, j, k}; double2 ey = val(iY(g, i, j, k), q);
+            q = {1, i, j - 1, k}; double2 eym = val(iY(g, i, j - 1, k), q);
+            q = {2, i, j, k}; double2 ez = val(iZ(g, i, j, k), q);
+            q = {2, i, j, k - 1}; double2 ezm = val(iZ(g, i, j, k - 1), q);
+            double2 d;
+            d.x = (ex.x - exm.x) / g.delX[i] + (ey.x - eym.x) / g.delY[j] + (ez.x - ezm.x) / g.delZ[k];
+            d.y = (ex.y - exm.y) / g.delX[i] + (ey.y - eym.y) / g.delY[j] + (ez.y - ezm.y) / g.delZ[k];
+            // d * i * inv
+            out = make_double2(-d.y * inv, d.x * inv);
+        }
+        phi0[off + n] = out;
+    }
+}
+
+// true FP64 residual of the mixed path: r64 = b - A X; |r64|^2 -> relres,
+// convergence test and the scale of the FP32 right-hand side
+__global__ void __launch_bounds__(kThreads) km_res64(KArgs<double> a, double tol_unused)
+{
+    const int r = blockIdx.y;
+    OuterState &os = a.ost[r];
+    if (!os.active) return;
+    const size_t off = (size_t)r * a.stride;
+    const Geo<double> &g = a.g;
+    const double wmu = rhs_wmu(a, r);
+    double v[1] = {0};
+    const int end = min((blockIdx.x + 1) * a.chunk, g.nE);
+    for (int e = chunk_begin(a.chunk); e < end; e += kThreads) {
+        EdgeIdx q = edge_decode(g, e);
+        double2 res = make_double2(0, 0);
+        if (edge_interior(g, q)) {
+            res = csub(a.b[off + e], stencil(g, a.x0 + off, q, dterm_of(g, q, wmu, a.sigma[e])));
+            v[0] += res.x * res.x + res.y * res.y;
+        }
+        a.r[off + e] = res;
+    }
+    double tot[1];
+    if (block_reduce_last<1>(v, a.parts, a.cnt, r, blockIdx.x, gridDim.x, tot) && threadIdx.x == 0) {
+        const double rn = sqrt(tot[0]);
+        os.relres = rn / os.bnorm64;
+        os.scale = rn > 0.0 ? 1.0 / rn : 0.0;
+    }
+}
+
+// FP32 right-hand side of the correction equation: b32 = r64 * scale, x32 = 0
+__global__ void __launch_bounds__(kThreads) km_cast(const OuterState *ost, int nE, size_t stride, const double2 *r64,
+                                                     float2 *b32, float2 *x32)
+{
+    const int r = blockIdx.y;
+    if (!ost[r].active) return;
+    const size_t off = (size_t)r * stride;
+    const double sc = ost[r].scale;
+    for (int e = blockIdx.x * kThreads + threadIdx.x; e < nE; e += gridDim.x * kThreads) {
+        double2 v = r64[off + e];
+        b32[off + e] = make_float2((float)(v.x * sc), (float)(v.y * sc));
+        x32[off + e] = make_float2(0.f, 0.f);
+    }
+}
+
+// X += d32 / scale
+__global__ void __launch_bounds__(kThreads) km_update(const OuterState *ost, int nE, size_t stride, const float2 *d32,
+                                                       double2 *X)
+{
+    const int r = blockIdx.y;
+    if (!ost[r].active) return;
+    const size_t off = (size_t)r * stride;
+    const double inv = ost[r].scale > 0.0 ? 1.0 / ost[r].scale : 0.0;
+    for (int e = blockIdx.x * kThreads + threadIdx.x; e < nE; e += gridDim.x * kThreads) {
+        float2 d = d32[off + e];
+        double2 x = X[off + e];
+        X[off + e] = make_double2(x.x + (double)d.x * inv, x.y + (double)d.y * inv);
+    }
+}
+
+// ||b||^2 per right-hand side (FP64 interior system)
+__global__ void __launch_bounds__(kThreads) k_norm_b(KArgs<double> a)
+{
+    const int r = blockIdx.y;
+    const size_t off = (size_t)r * a.stride;
+    double v[1] = {0};
+    const int end = min((blockIdx.x + 1) * a.chunk, a.g.nE);
+    for (int e = chunk_begin(a.chunk); e < end; e += kThreads) {
+        double2 b = a.b[off + e];
+        v[0] += b.x * b.x + b.y * b.y;
+    }
+    double tot[1];
+    if (block_reduce_last<1>(v, a.parts, a.cnt, r, blockIdx.x, gridDim.x, tot) && threadIdx.x == 0)
+        a.ost[r].bnorm64 = sqrt(tot[0]);
+}
+
+// Post-processing of FWDsolve3D (f90/3D_MT/FWD/EMsolve3D.f90:356-385):
+// forward: boundary = bc (or 0); transposed: e = V_E e and boundary =
+// bc - AdjtBC(e) (or -AdjtBC(e)), AdjtBC (f90/3D_MT/FWD/modelOperator3D.f90:
+// 920-1057) with the face precedence of copy_bcvector.  Step 1 scales the
+// interior of transposed solutions by V_E.
+__global__ void __launch_bounds__(kThreads) k_post_scale(Geo<double> g, double2 *E, size_t stride, const OuterState *ost)
+{
+    const int r = blockIdx.y;
+    if (!ost[r].trans) return;
+    const size_t off = (size_t)r * stride;
+    for (int e = blockIdx.x * kThreads + threadIdx.x; e < g.nE; e += gridDim.x * kThreads) {
+        EdgeIdx q = edge_decode(g, e);
+        if (!edge_interior(g, q)) continue;
+        E[off + e] = cscale(E[off + e], edge_volume(g, q));
+    }
+}
+
+__device__ double2 adjt_bc_value(const Geo<double> &g, const double2 *E, const EdgeIdx &q)
+{
+    const int nx = g.nx, ny = g.ny, nz = g.nz, i = q.i, j = q.j, k = q.k;
+    const double *dx = g.dx, *dy = g.dy, *dz = g.dz, *dX = g.delX, *dY = g.delY, *dZ = g.delZ;
+    double2 z = make_double2(0, 0);
+    // a*E[iu] + b*E[iv] + c*E[iw]; a zero coefficient skips its load, so only
+    // interior entries are read while the boundary entries are rewritten
+    auto lin3i = [&](double a, int iu, double b, int iv, double c, int iw) {
+        double2 u = a != 0.0 ? E[iu] : z, v = b != 0.0 ? E[iv] : z, w = E[iw];
+        return make_double2(a * u.x + b * v.x + c * w.x, a * u.y + b * v.y + c * w.y);
+    };
+    if (q.c == 0) {  // Ex
+        if (k == 0 || k == nz) {
+            if (j == 0 || j == ny) return z;
+            if (k == 0) {
+                double a1 = (i >= 1 && i <= nx - 1) ? 1.0 / (dX[i] * dz[0]) : 0.0;
+                double a2 = (i <= nx - 2) ? 1.0 / (dX[i + 1] * dz[0]) : 0.0;
+                return lin3i(-a1, iZ(g, i, j, 0), a2, iZ(g, i + 1, j, 0), -1.0 / (dZ[1] * dz[0]), iX(g, i, j, 1));
+            } else {
+                double a1 = (i >= 1 && i <= nx - 1) ? 1.0 / (dX[i] * dz[nz - 1]) : 0.0;
+                double a2 = (i <= nx - 2) ? 1.0 / (dX[i + 1] * dz[nz - 1]) : 0.0;
+                return lin3i(a1, iZ(g, i, j, nz - 1), -a2, iZ(g, i + 1, j, nz - 1), -1.0 / (dZ[nz - 1] * dz[nz - 1]),
+                            iX(g, i, j, nz - 1));
+            }
+        }
+        if (j == 0) {
+            double a1 = (i >= 1 && i <= nx - 1) ? 1.0 / (dX[i] * dy[0]) : 0.0;
+            double a2 = (i <= nx - 2) ? 1.0 / (dX[i + 1] * dy[0]) : 0.0;
+            return lin3i(-a1, iY(g, i, 0, k), a2, iY(g, i + 1, 0, k), -1.0 / (dY[1] * dy[0]), iX(g, i, 1, k));
+        } else {
+            double a1 = (i >= 1 && i <= nx - 1) ? 1.0 / (dX[i] * dy[ny - 1]) : 0.0;
+            double a2 = (i <= nx - 2) ? 1.0 / (dX[i + 1] * dy[ny - 1]) : 0.0;
+            return lin3i(a1, iY(g, i, ny - 1, k), -a2, iY(g, i + 1, ny - 1, k), -1.0 / (dY[ny - 1] * dy[ny - 1]),
+                        iX(g, i, ny - 1, k));
+        }
+    } else if (q.c == 1) {  // Ey
+        if (k == 0 || k == nz) {
+            if (i == 0 || i == nx) return z;
+            if (k == 0) {
+                double a1 = (j >= 1 && j <= ny - 1) ? 1.0 / (dY[j] * dz[0]) : 0.0;
+                double a2 = (j <= ny - 2) ? 1.0 / (dY[j + 1] * dz[0]) : 0.0;
+                return lin3i(-a1, iZ(g, i, j, 0), a2, iZ(g, i, j + 1, 0), -1.0 / (dZ[1] * dz[0]), iY(g, i, j, 1));
+            } else {
+                double a1 = (j >= 1 && j <= ny - 1) ? 1.0 / (dY[j] * dz[nz - 1]) : 0.0;
+                double a2 = (j <= ny - 2) ? 1.0 / (dY[j + 1] * dz[nz - 1]) : 0.0;
+                return lin3i(a1, iZ(g, i, j, nz - 1), -a2, iZ(g, i, j + 1, nz - 1), -1.0 / (dZ[nz - 1] * dz[nz - 1]),
+                            iY(g, i, j, nz - 1));
+            }
+        }
+        if (i == 0) {
+            double a1 = (j >= 1 && j <= ny - 1) ? 1.0 / (dY[j] * dx[0]) : 0.0;
+            double a2 = (j <= ny - 2) ? 1.0 / (dY[j + 1] * dx[0]) : 0.0;
+            return lin3i(-a1, iX(g, 0, j, k), a2, iX(g, 0, j + 1, k), -1.0 / (dX[1] * dx[0]), iY(g, 1, j, k));
+        } else {
+            double a1 = (j >= 1 && j <= ny - 1) ? 1.0 / (dY[j] * dx[nx - 1]) : 0.0;
+            double a2 = (j <= ny - 2) ? 1.0 / (dY[j + 1] * dx[nx - 1]) : 0.0;
+            return lin3i(a1, iX(g, nx - 1, j, k), -a2, iX(g, nx - 1, j + 1, k), -1.0 / (dX[nx - 1] * dx[nx - 1]),
+                        iY(g, nx - 1, j, k));
+        }
+    } else {  // Ez
+        if (i == 0 || i == nx) {
+            if (j == 0 || j == ny) return z;
+            if (i == 0) {
+                double a1 = (k >= 1 && k <= nz - 1) ? 1.0 / (dZ[k] * dx[0]) : 0.0;
+                double a2 = (k <= nz - 2) ? 1.0 / (dZ[k + 1] * dx[0]) : 0.0;
+                return lin3i(-a1, iX(g, 0, j, k), a2, iX(g, 0, j, k + 1), -1.0 / (dX[1] * dx[0]), iZ(g, 1, j, k));
+            } else {
+                double a1 = (k >= 1 && k <= nz - 1) ? 1.0 / (dZ[k] * dx[nx - 1]) : 0.0;
+                double a2 = (k <= nz - 2) ? 1.0 / (dZ[k + 1] * dx[nx - 1]) : 0.0;
+                return lin3i(a1, iX(g, nx - 1, j, k), -a2, iX(g, nx - 1, j, k + 1), -1.0 / (dX[nx - 1] * dx[nx - 1]),
+                            iZ(g, nx - 1, j, k));
+            }
+        }
+        if (j == 0) {
+            double a1 = (k >= 1 && k <= nz - 1) ? 1.0 / (dZ[k] * dy[0]) : 0.0;
+            double a2 = (k <= nz - 2) ? 1.0 / (dZ[k + 1] * dy[0]) : 0.0;
+            return lin3i(-a1, iY(g, i, 0, k), a2, iY(g, i, 0, k + 1), -1.0 / (dY[1] * dy[0]), iZ(g, i, 1, k));
+        } else {
+            double a1 = (k >= 1 && k <= nz - 1) ? 1.0 / (dZ[k] * dy[ny - 1]) : 0.0;
+            double a2 = (k <= nz - 2) ? 1.0 / (dZ[k + 1] * dy[ny - 1]) : 0.0;
+            return lin3i(a1, iY(g, i, ny - 1, k), -a2, iY(g, i, ny - 1, k + 1), -1.0 / (dY[ny - 1] * dy[ny - 1]),
+                        iZ(g, i, ny - 1, k));
+        }
+    }
+}
+
+// boundary entries of the returned field (bc is the uploaded boundary data,
+// may be null; has_bc per right-hand side)
+__global__ void __launch_bounds__(kThreads) k_post_boundary(Geo<double> g, double2 *E, const double2 *bc, size_t stride,
+                                                             const OuterState *ost)
+{
+    const int r = blockIdx.y;
+    const size_t off = (size_t)r * stride;
+    const bool tr = ost[r].trans != 0;
+    const bool hb = bc != nullptr && ost[r].has_bc;
+    for (int e = blockIdx.x * kThreads + threadIdx.x; e < g.nE; e += gridDim.x * kThreads) {
+        EdgeIdx q = edge_decode(g, e);
+        if (edge_interior(g, q)) continue;
+        double2 v = hb ? bc[off + e] : make_double2(0, 0);
+        if (tr) v = csub(v, adjt_bc_value(g, E + off, q));
+        E[off + e] = v;
+    }
+}
+
+// PmultT + dEdgeToModelParam (f90/3D_MT/SolverSens.f90:63-116,
+// f90/3D_MT/modelParam/ModelMap.inc:302-374), gathered per earth cell: each
+// cell sums Re(i*mu0*omega*sum_pol e0*eadj)/V_E_ghost over its 12 edges with
+// the Edge2Cell weights (1/4, 1/2 or 1 by the number of cells sharing the
+// edge), then multiplies by V_C and exp(m0).
+__device__ __forceinline__ int edge_ncells(const Geo<double> &g, int c, int i, int j, int k)
+{
+    int a = 2, b = 2;
+    if (c == 0) { a = (j == 0 || j == g.ny) ? 1 : 2; b = (k == 0 || k == g.nz) ? 1 : 2; }
+    if (c == 1) { a = (i == 0 || i == g.nx) ? 1 : 2; b = (k == 0 || k == g.nz) ? 1 : 2; }
+    if (c == 2) { a = (i == 0 || i == g.nx) ? 1 : 2; b = (j == 0 || j == g.ny) ? 1 : 2; }
+    return a * b;
+}
+__device__ __forceinline__ double cellvol(const Geo<double> &g, int i, int j, int k)
+{
+    return g.dx[i] * g.dy[j] * g.dz[k];
+}
+// V_E_ghost = sum of the adjacent cell volumes / their number (Cell2Edge of V_C)
+__device__ double edge_vghost(const Geo<double> &g, int c, int i, int j, int k)
+{
+    double s = 0.0;
+    int n = 0;
+    for (int a = -1; a <= 0; a++)
+        for (int b = -1; b <= 0; b++) {
+            int ci = i, cj = j, ck = k;
+            if (c == 0) { cj = j + a; ck = k + b; }
+            if (c == 1) { ci = i + a; ck = k + b; }
+            if (c == 2) { ci = i + a; cj = j + b; }
+            if (ci < 0 || ci >= g.nx || cj < 0 || cj >= g.ny || ck < 0 || ck >= g.nz) continue;
+            s += cellvol(g, ci, cj, ck);
+            n++;
+        }
+    return s / n;
+}
+
+__global__ void __launch_bounds__(kThreads) k_pmult_t(Geo<double> g, int npol, const double2 *e0, const double2 *ea,
+                                                       double omega, const double *m0, double *dm)
+{
+    const int nEarth = g.nx * g.ny * (g.nz - g.nzAir);
+    const double w = kMu0 * omega;  // -ISIGN*mu0*omega with ISIGN = -1: factor i*w
+    for (int c = blockIdx.x * kThreads + threadIdx.x; c < nEarth; c += gridDim.x * kThreads) {
+        const int i = c % g.nx, t = c / g.nx, j = t % g.ny, k = t / g.ny + g.nzAir;
+        double acc = 0.0;
+        auto edge = [&](int comp, int ei, int ej, int ek, int idx) {
+            double re = 0.0;
+            for (int p = 0; p < npol; p++) {
+                double2 a = e0[(size_t)p * g.nE + idx], b = ea[(size_t)p * g.nE + idx];
+                // Re(i*w*a*b) = -w * Im(a*b)
+                re += -w * (a.x * b.y + a.y * b.x);
+            }
+            return re / edge_vghost(g, comp, ei, ej, ek) / edge_ncells(g, comp, ei, ej, ek);
+        };
+        for (int b = 0; b <= 1; b++)
+            for (int a = 0; a <= 1; a++) {
+                acc += edge(0, i, j + a, k + b, iX(g, i, j + a, k + b));
+                acc += edge(1, i + a, j, k + b, iY(g, i + a, j, k + b));
+                acc += edge(2, i + a, j + b, k, iZ(g, i + a, j + b, k));
+            }
+        dm[c] = (acc * cellvol(g, i, j, k)) * exp(m0[c]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// gather / scatter between interior vectors (EDGEi order) and full vectors
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads) k_scatter_interior(int nEi, const int *edgei, const double2 *vi, double2 *vf)
+{
+    for (int n = blockIdx.x * kThreads + threadIdx.x; n < nEi; n += gridDim.x * kThreads) vf[edgei[n]] = vi[n];
+}
+__global__ void __launch_bounds__(kThreads) k_gather_interior(int nEi, const int *edgei, const double2 *vf, double2 *vi)
+{
+    for (int n = blockIdx.x * kThreads + threadIdx.x; n < nEi; n += gridDim.x * kThreads) vi[n] = vf[edgei[n]];
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+template <typename T> void launch_apply(const KArgs<T> &a, const C2<T> *x, C2<T> *y, int neg, int nrhs, cudaStream_t s)
+{
+    k_apply<T><<<dim3(a.nblk, nrhs), kThreads, 0, s>>>(a, x, y, neg);
+}
+template <typename T> void launch_bicg_init(const KArgs<T> &a, int nrhs, cudaStream_t s)
+{
+    kb_init<T><<<dim3(a.nblk, nrhs), kThreads, 0, s>>>(a);
+}
+template <typename T> void launch_bicg_iter(const KArgs<T> &a, int nrhs, cudaStream_t s)
+{
+    dim3 grid(a.nblk, nrhs);
+    kb_p<T><<<grid, kThreads, 0, s>>>(a);
+    kb_v<T><<<grid, kThreads, 0, s>>>(a);
+    kb_s<T><<<grid, kThreads, 0, s>>>(a);
+    kb_t<T><<<grid, kThreads, 0, s>>>(a);
+    kb_xr<T><<<grid, kThreads, 0, s>>>(a);
+}
+template <typename T> void launch_bicg_finish(const KArgs<T> &a, int nrhs, cudaStream_t s)
+{
+    kb_finish<T><<<dim3(a.nblk, nrhs), kThreads, 0, s>>>(a);
+}
+template void launch_apply<double>(const KArgs<double> &, const double2 *, double2 *, int, int, cudaStream_t);
+template void launch_apply<float>(const KArgs<float> &, const float2 *, float2 *, int, int, cudaStream_t);
+template void launch_bicg_init<double>(const KArgs<double> &, int, cudaStream_t);
+template void launch_bicg_init<float>(const KArgs<float> &, int, cudaStream_t);
+template void launch_bicg_iter<double>(const KArgs<double> &, int, cudaStream_t);
+template void launch_bicg_iter<float>(const KArgs<float> &, int, cudaStream_t);
+template void launch_bicg_finish<double>(const KArgs<double> &, int, cudaStream_t);
+template void launch_bicg_finish<float>(const KArgs<float> &, int, cudaStream_t);
+
+void launch_norm_b(const KArgs<double> &a, int nrhs, cudaStream_t s)
+{
+    k_norm_b<<<dim3(a.nblk, nrhs), kThreads, 0, s>>>(a);
+}
+void launch_res64(const KArgs<double> &a, int nrhs, cudaStream_t s)
+{
+    km_res64<<<dim3(a.nblk, nrhs), kThreads, 0, s>>>(a, 0.0);
+}
+static int grid_for(long n) { return (int)std::min<long>((n + kThreads - 1) / kThreads, 148L * 16); }
+void launch_cast(const OuterState *ost, int nE, size_t stride, const double2 *r64, float2 *b32, float2 *x32, int nrhs,
+                 cudaStream_t s)
+{
+    km_cast<<<dim3(grid_for(nE), nrhs), kThreads, 0, s>>>(ost, nE, stride, r64, b32, x32);
+}
+void launch_update(const OuterState *ost, int nE, size_t stride, const float2 *d32, double2 *X, int nrhs, cudaStream_t s)
+{
+    km_update<<<dim3(grid_for(nE), nrhs), kThreads, 0, s>>>(ost, nE, stride, d32, X);
+}
+void launch_divcorr_start(const DArgs &a, int nrhs, cudaStream_t s)
+{
+    kd_rhs<<<dim3(a.nblk, nrhs), kThreads, 0, s>>>(a);
+}
+void launch_divcorr_iter(const DArgs &a, int nrhs, cudaStream_t s)
+{
+    dim3 grid(a.nblk, nrhs);
+    kd_p<<<grid, kThreads, 0, s>>>(a);
+    kd_q<<<grid, kThreads, 0, s>>>(a);
+    kd_xr<<<grid, kThreads, 0, s>>>(a);
+}
+void launch_divcorr_finish(const DArgs &a, int nrhs, cudaStream_t s)
+{
+    kd_grad<<<dim3(a.enblk, nrhs), kThreads, 0, s>>>(a);
+    kd_divj<<<dim3(a.nblk, nrhs), kThreads, 0, s>>>(a);
+}
+void launch_keep_boundary(const Geo<double> &g, double2 *v, size_t stride, int nrhs, cudaStream_t s)
+{
+    k_keep_boundary<<<dim3(grid_for(g.nE), nrhs), kThreads, 0, s>>>(g, v, stride);
+}
+void launch_keep_interior(const Geo<double> &g, double2 *v, size_t stride, int nrhs, cudaStream_t s)
+{
+    k_keep_interior<<<dim3(grid_for(g.nE), nrhs), kThreads, 0, s>>>(g, v, stride);
+}
+void launch_add_src(const Geo<double> &g, double2 *b, const double2 *src, size_t stride, const OuterState *ost, int nrhs,
+                    cudaStream_t s)
+{
+    k_add_src<<<dim3(grid_for(g.nE), nrhs), kThreads, 0, s>>>(g, b, src, stride, ost);
+}
+void launch_phi0(const Geo<double> &g, const double2 *src, size_t estride, double2 *phi0, size_t nstride,
+                 const OuterState *ost, int nrhs, cudaStream_t s)
+{
+    k_phi0<<<dim3(grid_for(g.nN), nrhs), kThreads, 0, s>>>(g, src, estride, phi0, nstride, ost);
+}
+void launch_post(const Geo<double> &g, double2 *E, const double2 *bc, size_t stride, const OuterState *ost, int nrhs,
+                 cudaStream_t s)
+{
+    k_post_scale<<<dim3(grid_for(g.nE), nrhs), kThreads, 0, s>>>(g, E, stride, ost);
+    k_post_boundary<<<dim3(grid_for(g.nE), nrhs), kThreads, 0, s>>>(g, E, bc, stride, ost);
+}
+void launch_pmult_t(const Geo<double> &g, int npol, const double2 *e0, const double2 *ea, double omega, const double *m0,
+                    double *dm, cudaStream_t s)
+{
+    const int nEarth = g.nx * g.ny * (g.nz - g.nzAir);
+    k_pmult_t<<<grid_for(nEarth), kThreads, 0, s>>>(g, npol, e0, ea, omega, m0, dm);
+}
+void launch_scatter_interior(int nEi, const int *edgei, const double2 *vi, double2 *vf, cudaStream_t s)
+{
+    k_scatter_interior<<<grid_for(nEi), kThreads, 0, s>>>(nEi, edgei, vi, vf);
+}
+void launch_gather_interior(int nEi, const int *edgei, const double2 *vf, double2 *vi, cudaStream_t s)
+{
+    k_gather_interior<<<grid_for(nEi), kThreads, 0, s>>>(nEi, edgei, vf, vi);
+}
+
+}  // namespace mt3d

@@ -1,0 +1,73 @@
+// kernels.h -- kernel argument blocks and launchers (host-visible).
+#pragma once
+#include "common.cuh"
+
+namespace mt3d {
+
+// arguments of the edge-vector Krylov kernels (one precision T)
+template <typename T> struct KArgs {
+    Geo<T> g;
+    const T *sigma;   // edge conductivity of the forward operator (air zeroed)
+    OuterState *ost;  // per right-hand side: omega, activity, tolerances
+    BicgState *st;
+    C2<T> *r, *rt, *p, *v, *ph, *s, *sh, *t, *x0, *x1;
+    const C2<T> *b;
+    double *parts;
+    unsigned *cnt;
+    double *rerr;  // [nrhs][rerr_stride]
+    int rerr_stride;
+    size_t stride;  // elements between right-hand sides
+    int chunk, nblk;
+    int maxit;
+    int inner;    // 1: tolerance from OuterState::tol_inner (mixed inner solve)
+    double dsgn;  // ISIGN (-1) for A, +1 for the conjugate transpose
+};
+
+// arguments of the divergence-correction kernels (FP64)
+struct DArgs {
+    Geo<double> g;
+    const double *sigma;  // edge conductivity (air zeroed), as DivC uses it
+    const double *coef;   // 7 node arrays (SoA): db1x db2x db1y db2y db1z db2z c
+    OuterState *ost;
+    PcgState *pst;
+    double2 *E;            // fields being corrected [nrhs][estride]
+    const double2 *phi0;   // scaled source divergence or null [nrhs][stride]
+    double2 *px, *pr, *pp, *pq;
+    double *parts;
+    unsigned *cnt;
+    double *rerr;
+    int rerr_stride;
+    size_t stride;   // node vector stride
+    size_t estride;  // edge vector stride
+    int chunk, nblk;    // node chunking
+    int echunk, enblk;  // edge chunking
+    int maxit;
+    double tol;
+};
+
+template <typename T> void launch_apply(const KArgs<T> &a, const C2<T> *x, C2<T> *y, int neg, int nrhs, cudaStream_t s);
+template <typename T> void launch_bicg_init(const KArgs<T> &a, int nrhs, cudaStream_t s);
+template <typename T> void launch_bicg_iter(const KArgs<T> &a, int nrhs, cudaStream_t s);
+template <typename T> void launch_bicg_finish(const KArgs<T> &a, int nrhs, cudaStream_t s);
+void launch_norm_b(const KArgs<double> &a, int nrhs, cudaStream_t s);
+void launch_res64(const KArgs<double> &a, int nrhs, cudaStream_t s);
+void launch_cast(const OuterState *ost, int nE, size_t stride, const double2 *r64, float2 *b32, float2 *x32, int nrhs,
+                 cudaStream_t s);
+void launch_update(const OuterState *ost, int nE, size_t stride, const float2 *d32, double2 *X, int nrhs, cudaStream_t s);
+void launch_divcorr_start(const DArgs &a, int nrhs, cudaStream_t s);
+void launch_divcorr_iter(const DArgs &a, int nrhs, cudaStream_t s);
+void launch_divcorr_finish(const DArgs &a, int nrhs, cudaStream_t s);
+void launch_keep_boundary(const Geo<double> &g, double2 *v, size_t stride, int nrhs, cudaStream_t s);
+void launch_keep_interior(const Geo<double> &g, double2 *v, size_t stride, int nrhs, cudaStream_t s);
+void launch_add_src(const Geo<double> &g, double2 *b, const double2 *src, size_t stride, const OuterState *ost, int nrhs,
+                    cudaStream_t s);
+void launch_phi0(const Geo<double> &g, const double2 *src, size_t estride, double2 *phi0, size_t nstride,
+                 const OuterState *ost, int nrhs, cudaStream_t s);
+void launch_post(const Geo<double> &g, double2 *E, const double2 *bc, size_t stride, const OuterState *ost, int nrhs,
+                 cudaStream_t s);
+void launch_pmult_t(const Geo<double> &g, int npol, const double2 *e0, const double2 *ea, double omega, const double *m0,
+                    double *dm, cudaStream_t s);
+void launch_scatter_interior(int nEi, const int *edgei, const double2 *vi, double2 *vf, cudaStream_t s);
+void launch_gather_interior(int nEi, const int *edgei, const double2 *vf, double2 *vi, cudaStream_t s);
+
+}  // namespace mt3d

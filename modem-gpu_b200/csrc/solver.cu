@@ -1,0 +1,759 @@
+// solver.cu -- host driver of the B200 3D-MT solve: operator set-up, the
+// divergence-corrected Krylov loop of FWDsolve3D and the mixed-precision
+// refinement.  Everything numeric runs in the kernels of kernels.cu; this
+// file sequences launches on the handle's stream and reads back only the
+// per-right-hand-side scalar state once per outer (divergence-correction)
+// cycle.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+#include "solver.h"
+
+namespace mt3d {
+
+int DevBuf::alloc(size_t bytes)
+{
+    if (bytes <= bytes_ && ptr_) return 0;
+    release();
+    if (bytes == 0) return 0;
+    cudaError_t e = cudaMalloc(&ptr_, bytes);
+    if (e != cudaSuccess) {
+        ptr_ = nullptr;
+        return (int)e;
+    }
+    bytes_ = bytes;
+    return 0;
+}
+void DevBuf::release()
+{
+    if (ptr_) cudaFree(ptr_);
+    ptr_ = nullptr;
+    bytes_ = 0;
+}
+
+Solver::~Solver()
+{
+    if (stream_) {
+        cudaSetDevice(dev_);
+        cudaStreamSynchronize(stream_);
+        cudaStreamDestroy(stream_);
+    }
+}
+
+int Solver::fail(int code, const std::string &msg)
+{
+    last_error = msg;
+    return code;
+}
+
+int Solver::check(cudaError_t e, const char *what)
+{
+    if (e == cudaSuccess) return 0;
+    char buf[256];
+    snprintf(buf, sizeof buf, "%s: %s", what, cudaGetErrorString(e));
+    last_error = buf;
+    return e == cudaErrorMemoryAllocation ? 8 : 4;
+}
+
+int Solver::sync(const char *what)
+{
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+    return check(e, what);
+}
+
+static void deltas(const std::vector<double> &d, std::vector<double> &del)
+{
+    const size_t n = d.size();
+    del.assign(n + 1, 0.0);
+    del[0] = d[0];
+    for (size_t i = 1; i < n; i++) del[i] = d[i - 1] + d[i];
+    del[n] = d[n - 1];
+    for (auto &v : del) v = v / 2.0;
+}
+
+int Solver::create(int dev, int nx_, int ny_, int nz_, int nzAir_, const double *dx, const double *dy, const double *dz)
+{
+    if (nx_ < 2 || ny_ < 2 || nz_ < 2 || nzAir_ < 0 || nzAir_ >= nz_ || !dx || !dy || !dz)
+        return fail(5, "mt3d_create: invalid grid dimensions or null spacing arrays");
+    nx = nx_; ny = ny_; nz = nz_; nzAir = nzAir_;
+    const int64_t nX = (int64_t)nx * (ny + 1) * (nz + 1), nY = (int64_t)(nx + 1) * ny * (nz + 1),
+                  nZ = (int64_t)(nx + 1) * (ny + 1) * nz;
+    nE = nX + nY + nZ;
+    nN = (int64_t)(nx + 1) * (ny + 1) * (nz + 1);
+    nEi = (int64_t)nx * (ny - 1) * (nz - 1) + (int64_t)(nx - 1) * ny * (nz - 1) + (int64_t)(nx - 1) * (ny - 1) * nz;
+    if (nE >= (int64_t)1 << 31) return fail(5, "mt3d_create: grid too large (edge count must fit in int32)");
+    for (int i = 0; i < nx; i++) if (!(dx[i] > 0)) return fail(5, "mt3d_create: dx must be positive");
+    for (int i = 0; i < ny; i++) if (!(dy[i] > 0)) return fail(5, "mt3d_create: dy must be positive");
+    for (int i = 0; i < nz; i++) if (!(dz[i] > 0)) return fail(5, "mt3d_create: dz must be positive");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(7, "mt3d_create: no CUDA device available");
+    }
+    if (dev < 0 || dev >= ndev) return fail(5, "mt3d_create: device id out of range");
+    dev_ = dev;
+    int rc;
+    if ((rc = check(cudaSetDevice(dev_), "cudaSetDevice"))) return rc;
+    if ((rc = check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate"))) return rc;
+
+    dx_.assign(dx, dx + nx); dy_.assign(dy, dy + ny); dz_.assign(dz, dz + nz);
+    deltas(dx_, delX_); deltas(dy_, delY_); deltas(dz_, delZ_);
+    // tables: dx dy dz delX delY delZ rdx rdy rdz
+    std::vector<double> t;
+    auto app = [&](const std::vector<double> &v) { t.insert(t.end(), v.begin(), v.end()); };
+    std::vector<double> rdx(nx), rdy(ny), rdz(nz);
+    for (int i = 0; i < nx; i++) rdx[i] = 1.0 / dx_[i];
+    for (int i = 0; i < ny; i++) rdy[i] = 1.0 / dy_[i];
+    for (int i = 0; i < nz; i++) rdz[i] = 1.0 / dz_[i];
+    app(dx_); app(dy_); app(dz_); app(delX_); app(delY_); app(delZ_); app(rdx); app(rdy); app(rdz);
+    std::vector<float> tf(t.begin(), t.end());
+    if (tab64_.alloc(t.size() * sizeof(double)) || tab32_.alloc(tf.size() * sizeof(float)))
+        return fail(8, "mt3d_create: out of device memory");
+    if ((rc = check(cudaMemcpy(tab64_.as<void>(), t.data(), t.size() * sizeof(double), cudaMemcpyHostToDevice), "copy tables")))
+        return rc;
+    if ((rc = check(cudaMemcpy(tab32_.as<void>(), tf.data(), tf.size() * sizeof(float), cudaMemcpyHostToDevice), "copy tables")))
+        return rc;
+    size_t o[10];
+    o[0] = 0; o[1] = o[0] + nx; o[2] = o[1] + ny; o[3] = o[2] + nz; o[4] = o[3] + nx + 1; o[5] = o[4] + ny + 1;
+    o[6] = o[5] + nz + 1; o[7] = o[6] + nx; o[8] = o[7] + ny; o[9] = o[8] + nz;
+    auto fill = [&](auto &g, auto *base) {
+        g.nx = nx; g.ny = ny; g.nz = nz; g.nzAir = nzAir;
+        g.nXe = (int)nX; g.nYe = (int)nY; g.nZe = (int)nZ; g.nE = (int)nE; g.nN = (int)nN;
+        g.dx = base + o[0]; g.dy = base + o[1]; g.dz = base + o[2];
+        g.delX = base + o[3]; g.delY = base + o[4]; g.delZ = base + o[5];
+        g.rdx = base + o[6]; g.rdy = base + o[7]; g.rdz = base + o[8];
+    };
+    fill(g64_, tab64_.as<double>());
+    fill(g32_, tab32_.as<float>());
+
+    // interior edge list (boundaryIndex, vecTranslate.f90:436-526), 0-based
+    edgei.clear();
+    edgei.reserve(nEi);
+    for (int k = 0; k <= nz; k++)
+        for (int j = 0; j <= ny; j++)
+            for (int i = 0; i < nx; i++)
+                if (j >= 1 && j <= ny - 1 && k >= 1 && k <= nz - 1) edgei.push_back(i + nx * (j + (ny + 1) * k));
+    for (int k = 0; k <= nz; k++)
+        for (int j = 0; j < ny; j++)
+            for (int i = 0; i <= nx; i++)
+                if (i >= 1 && i <= nx - 1 && k >= 1 && k <= nz - 1)
+                    edgei.push_back((int)nX + i + (nx + 1) * (j + ny * k));
+    for (int k = 0; k < nz; k++)
+        for (int j = 0; j <= ny; j++)
+            for (int i = 0; i <= nx; i++)
+                if (i >= 1 && i <= nx - 1 && j >= 1 && j <= ny - 1)
+                    edgei.push_back((int)(nX + nY) + i + (nx + 1) * (j + (ny + 1) * k));
+    if ((int64_t)edgei.size() != nEi) return fail(5, "internal: interior edge count mismatch");
+    if (edgei_d_.alloc(edgei.size() * sizeof(int32_t))) return fail(8, "mt3d_create: out of device memory");
+    if ((rc = check(cudaMemcpy(edgei_d_.as<void>(), edgei.data(), edgei.size() * sizeof(int32_t), cudaMemcpyHostToDevice),
+                    "copy edge list")))
+        return rc;
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// UpdateCond: ModelParamToEdge (LOGE, f90/3D_MT/modelParam/ModelMap.inc:88-188)
+// and DivCorrSetUp (f90/3D_MT/FWD/modelOperator3D.f90:1538-1672)
+// ---------------------------------------------------------------------------
+int Solver::update_cond(const double *m_earth, double airCond)
+{
+    if (!m_earth) return fail(5, "mt3d_update_cond: null model");
+    const int nzE = nz - nzAir;
+    const int64_t nC = (int64_t)nx * ny * nz;
+    for (int64_t c = 0; c < (int64_t)nx * ny * nzE; c++)
+        if (!std::isfinite(m_earth[c])) return fail(3, "mt3d_update_cond: NaN/Inf in the model parameter");
+    if (!std::isfinite(airCond)) return fail(3, "mt3d_update_cond: NaN/Inf air conductivity");
+    auto cl = [&](int i, int j, int k) { return (int64_t)i + (int64_t)nx * (j + (int64_t)ny * k); };
+    std::vector<double> VC(nC), CT(nC);
+    for (int k = 0; k < nz; k++)
+        for (int j = 0; j < ny; j++)
+            for (int i = 0; i < nx; i++) {
+                const int64_t c = cl(i, j, k);
+                VC[c] = dx_[i] * dy_[j] * dz_[k];
+                const double s = (k < nzAir) ? std::exp(airCond) : std::exp(m_earth[c - (int64_t)nx * ny * nzAir]);
+                CT[c] = VC[c] * s;
+            }
+    const int64_t nX = (int64_t)nx * (ny + 1) * (nz + 1), nY = (int64_t)(nx + 1) * ny * (nz + 1);
+    std::vector<double> sig(nE);
+    // Cell2Edge of V_C*sigma over Cell2Edge of V_C, summing the adjacent cells in
+    // the reference's order (a-1,b-1), (a,b-1), (a-1,b), (a,b)
+    auto avg = [&](int comp, int i, int j, int k) {
+        double num = 0.0, den = 0.0;
+        int n = 0;
+        for (int q = 0; q < 4; q++) {
+            const int da = (q & 1) ? 0 : -1, db = (q & 2) ? 0 : -1;
+            int ci = i, cj = j, ck = k;
+            if (comp == 0) { cj = j + da; ck = k + db; }
+            if (comp == 1) { ci = i + da; ck = k + db; }
+            if (comp == 2) { cj = j + da; ci = i + db; }
+            if (ci < 0 || ci >= nx || cj < 0 || cj >= ny || ck < 0 || ck >= nz) continue;
+            num += CT[cl(ci, cj, ck)];
+            den += VC[cl(ci, cj, ck)];
+            n++;
+        }
+        return (num / n) / (den / n);
+    };
+    for (int k = 0; k <= nz; k++)
+        for (int j = 0; j <= ny; j++)
+            for (int i = 0; i < nx; i++) sig[i + nx * (j + (int64_t)(ny + 1) * k)] = avg(0, i, j, k);
+    for (int k = 0; k <= nz; k++)
+        for (int j = 0; j < ny; j++)
+            for (int i = 0; i <= nx; i++) sig[nX + i + (nx + 1) * (j + (int64_t)ny * k)] = avg(1, i, j, k);
+    for (int k = 0; k < nz; k++)
+        for (int j = 0; j <= ny; j++)
+            for (int i = 0; i <= nx; i++) sig[nX + nY + i + (nx + 1) * (j + (int64_t)(ny + 1) * k)] = avg(2, i, j, k);
+    auto ex = [&](int i, int j, int k) { return (int64_t)i + nx * (j + (int64_t)(ny + 1) * k); };
+    auto ey = [&](int i, int j, int k) { return nX + i + (nx + 1) * (j + (int64_t)ny * k); };
+    auto ez = [&](int i, int j, int k) { return nX + nY + i + (nx + 1) * (j + (int64_t)(ny + 1) * k); };
+    auto nd = [&](int i, int j, int k) { return (int64_t)i + (nx + 1) * (j + (int64_t)(ny + 1) * k); };
+    // DivCorrSetUp: air cells (1-based iz <= nzAir, ix <= nx, iy <= ny) at SIGMA_AIR
+    for (int k = 0; k < nzAir; k++)
+        for (int j = 0; j < ny; j++)
+            for (int i = 0; i < nx; i++) sig[ex(i, j, k)] = sig[ey(i, j, k)] = sig[ez(i, j, k)] = kSigmaAir;
+    std::vector<double> coef(7 * (size_t)nN, 0.0);
+    double *db1x = &coef[0], *db2x = &coef[nN], *db1y = &coef[2 * nN], *db2y = &coef[3 * nN], *db1z = &coef[4 * nN],
+           *db2z = &coef[5 * nN], *cc = &coef[6 * nN];
+    for (int k = 1; k < nz; k++)
+        for (int j = 1; j < ny; j++)
+            for (int i = 1; i < nx; i++) {
+                const int64_t n = nd(i, j, k);
+                db1x[n] = sig[ex(i - 1, j, k)] / (dx_[i - 1] * delX_[i]);
+                db2x[n] = sig[ex(i, j, k)] / (dx_[i] * delX_[i]);
+                db1y[n] = sig[ey(i, j - 1, k)] / (dy_[j - 1] * delY_[j]);
+                db2y[n] = sig[ey(i, j, k)] / (dy_[j] * delY_[j]);
+                db1z[n] = sig[ez(i, j, k - 1)] / (dz_[k - 1] * delZ_[k]);
+                db2z[n] = sig[ez(i, j, k)] / (dz_[k] * delZ_[k]);
+                cc[n] = -(db1x[n] + db2x[n] + db1y[n] + db2y[n] + db1z[n] + db2z[n]);
+            }
+    for (int k = 0; k < nzAir; k++)
+        for (int j = 0; j < ny; j++)
+            for (int i = 0; i < nx; i++) sig[ex(i, j, k)] = sig[ey(i, j, k)] = sig[ez(i, j, k)] = 0.0;
+    for (int k = 1; k < nz; k++)
+        for (int j = 1; j < ny; j++)
+            for (int i = 1; i < nx; i++) {
+                const int64_t n = nd(i, j, k);
+                const double v = delX_[i] * delY_[j] * delZ_[k];
+                db1x[n] *= v; db1y[n] *= v; db1z[n] *= v;
+                db2x[n] *= v; db2y[n] *= v; db2z[n] *= v;
+                cc[n] = cc[n] * v;
+            }
+    // coefficients that multiply boundary nodes are zero (phi = 0 on the boundary)
+    for (int k = 0; k <= nz; k++)
+        for (int j = 0; j <= ny; j++)
+            for (int i = 0; i <= nx; i++) {
+                const int64_t n = nd(i, j, k);
+                if (i == 1) db1x[n] = 0.0;
+                if (i == nx - 1) db2x[n] = 0.0;
+                if (j == 1) db1y[n] = 0.0;
+                if (j == ny - 1) db2y[n] = 0.0;
+                if (k == 1) db1z[n] = 0.0;
+                if (k == nz - 1) db2z[n] = 0.0;
+            }
+    std::vector<float> sigf(sig.begin(), sig.end());
+    int rc;
+    if (sig64_.alloc(nE * sizeof(double)) || sig32_.alloc(nE * sizeof(float)) || coef_.alloc(coef.size() * sizeof(double)))
+        return fail(8, "mt3d_update_cond: out of device memory");
+    if ((rc = check(cudaMemcpyAsync(sig64_.as<void>(), sig.data(), nE * sizeof(double), cudaMemcpyHostToDevice, stream_), "copy sigma")))
+        return rc;
+    if ((rc = check(cudaMemcpyAsync(sig32_.as<void>(), sigf.data(), nE * sizeof(float), cudaMemcpyHostToDevice, stream_), "copy sigma")))
+        return rc;
+    if ((rc = check(cudaMemcpyAsync(coef_.as<void>(), coef.data(), coef.size() * sizeof(double), cudaMemcpyHostToDevice, stream_),
+                    "copy div-corr coefficients")))
+        return rc;
+    if ((rc = sync("mt3d_update_cond"))) return rc;
+    cond_set = true;
+    return 0;
+}
+
+int Solver::update_freq(double w)
+{
+    if (!(w > 0.0) || !std::isfinite(w)) return fail(5, "mt3d_update_freq: omega must be positive and finite");
+    omega = w;
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// workspace and argument blocks
+// ---------------------------------------------------------------------------
+static int blocks_for(int64_t n, int nrhs, int &chunk)
+{
+    // contiguous chunks of >= 4 sweeps of the block; about 8 resident blocks
+    // per SM over the whole batch
+    const int64_t target = std::max<int64_t>(1, (148LL * 8) / std::max(1, nrhs));
+    int64_t per = (n + target - 1) / target;
+    per = std::max<int64_t>(per, 4 * kThreads);
+    per = (per + kThreads - 1) / kThreads * kThreads;
+    chunk = (int)per;
+    return (int)((n + per - 1) / per);
+}
+
+int Solver::ensure_workspace(int nrhs, int precision)
+{
+    const int rlen = std::max(ctl.IterPerDivCor, 1) + 1, dlen = std::max(ctl.MaxIterDivCor, 1) + 1;
+    if (ws_.nrhs >= nrhs && ws_.precision == precision && ws_.rlen == rlen && ws_.dlen == dlen) return 0;
+    Workspace &w = ws_;
+    const size_t e64 = (size_t)nrhs * nE * sizeof(double2), e32 = (size_t)nrhs * nE * sizeof(float2);
+    const size_t n64 = (size_t)nrhs * nN * sizeof(double2);
+    // release everything first so a precision change does not hold both sets
+    DevBuf *all[] = {&w.b, &w.X, &w.x1, &w.r, &w.rt, &w.p, &w.v, &w.ph, &w.s, &w.sh, &w.t, &w.bc, &w.tmp,
+                     &w.f_b, &w.f_x0, &w.f_x1, &w.f_r, &w.f_rt, &w.f_p, &w.f_v, &w.f_ph, &w.f_s, &w.f_sh, &w.f_t,
+                     &w.px, &w.pr, &w.pp, &w.pq, &w.phi0};
+    for (DevBuf *d : all) d->release();
+    int err = 0;
+    err |= w.b.alloc(e64) | w.X.alloc(e64) | w.bc.alloc(e64) | w.tmp.alloc(e64);
+    if (precision == 0) {
+        DevBuf *v64[] = {&w.x1, &w.r, &w.rt, &w.p, &w.v, &w.ph, &w.s, &w.sh, &w.t};
+        for (DevBuf *d : v64) err |= d->alloc(e64);
+    } else {
+        DevBuf *v32[] = {&w.f_b, &w.f_x0, &w.f_x1, &w.f_r, &w.f_rt, &w.f_p, &w.f_v, &w.f_ph, &w.f_s, &w.f_sh, &w.f_t};
+        for (DevBuf *d : v32) err |= d->alloc(e32);
+    }
+    DevBuf *nv[] = {&w.px, &w.pr, &w.pp, &w.pq, &w.phi0};
+    for (DevBuf *d : nv) err |= d->alloc(n64);
+    int c;
+    const int nb = std::max(blocks_for(nE, nrhs, c), blocks_for(nN, nrhs, c));
+    err |= w.bst.alloc(nrhs * sizeof(BicgState)) | w.pst.alloc(nrhs * sizeof(PcgState)) |
+           w.ost.alloc(nrhs * sizeof(OuterState));
+    err |= w.parts.alloc((size_t)nrhs * nb * kMaxParts * sizeof(double)) | w.cnt.alloc(nrhs * sizeof(unsigned));
+    err |= w.rerr.alloc((size_t)nrhs * rlen * sizeof(double));
+    err |= w.dcrerr.alloc((size_t)nrhs * dlen * sizeof(double));
+    if (err) {
+        for (DevBuf *d : all) d->release();
+        w.nrhs = 0;
+        w.precision = -1;
+        cudaGetLastError();
+        return fail(8, "out of device memory for the solver workspace");
+    }
+    cudaMemsetAsync(w.cnt.as<void>(), 0, nrhs * sizeof(unsigned), stream_);
+    w.nrhs = nrhs;
+    w.precision = precision;
+    w.rlen = rlen;
+    w.dlen = dlen;
+    return 0;
+}
+
+template <> KArgs<double> Solver::kargs<double>(int nrhs, int)
+{
+    KArgs<double> a{};
+    Workspace &w = ws_;
+    a.g = g64_;
+    a.sigma = sig64_.as<double>();
+    a.ost = w.ost.as<OuterState>();
+    a.st = w.bst.as<BicgState>();
+    a.r = w.r.as<double2>(); a.rt = w.rt.as<double2>(); a.p = w.p.as<double2>(); a.v = w.v.as<double2>();
+    a.ph = w.ph.as<double2>(); a.s = w.s.as<double2>(); a.sh = w.sh.as<double2>(); a.t = w.t.as<double2>();
+    a.x0 = w.X.as<double2>(); a.x1 = w.x1.as<double2>();
+    a.b = w.b.as<double2>();
+    a.parts = w.parts.as<double>();
+    a.cnt = w.cnt.as<unsigned>();
+    a.rerr = w.rerr.as<double>();
+    a.rerr_stride = ctl.IterPerDivCor + 1;
+    a.stride = nE;
+    a.nblk = blocks_for(nE, nrhs, a.chunk);
+    a.maxit = ctl.IterPerDivCor;
+    a.inner = 0;
+    a.dsgn = -1.0;
+    return a;
+}
+template <> KArgs<float> Solver::kargs<float>(int nrhs, int)
+{
+    KArgs<float> a{};
+    Workspace &w = ws_;
+    a.g = g32_;
+    a.sigma = sig32_.as<float>();
+    a.ost = w.ost.as<OuterState>();
+    a.st = w.bst.as<BicgState>();
+    a.r = w.f_r.as<float2>(); a.rt = w.f_rt.as<float2>(); a.p = w.f_p.as<float2>(); a.v = w.f_v.as<float2>();
+    a.ph = w.f_ph.as<float2>(); a.s = w.f_s.as<float2>(); a.sh = w.f_sh.as<float2>(); a.t = w.f_t.as<float2>();
+    a.x0 = w.f_x0.as<float2>(); a.x1 = w.f_x1.as<float2>();
+    a.b = w.f_b.as<float2>();
+    a.parts = w.parts.as<double>();
+    a.cnt = w.cnt.as<unsigned>();
+    a.rerr = w.rerr.as<double>();
+    a.rerr_stride = ctl.IterPerDivCor + 1;
+    a.stride = nE;
+    a.nblk = blocks_for(nE, nrhs, a.chunk);
+    a.maxit = ctl.IterPerDivCor;
+    a.inner = 1;
+    a.dsgn = -1.0;
+    return a;
+}
+
+DArgs Solver::dargs(int nrhs)
+{
+    DArgs a{};
+    Workspace &w = ws_;
+    a.g = g64_;
+    a.sigma = sig64_.as<double>();
+    a.coef = coef_.as<double>();
+    a.ost = w.ost.as<OuterState>();
+    a.pst = w.pst.as<PcgState>();
+    a.E = w.X.as<double2>();
+    a.phi0 = w.phi0.as<double2>();
+    a.px = w.px.as<double2>(); a.pr = w.pr.as<double2>(); a.pp = w.pp.as<double2>(); a.pq = w.pq.as<double2>();
+    a.parts = w.parts.as<double>();
+    a.cnt = w.cnt.as<unsigned>();
+    a.rerr = w.dcrerr.as<double>();
+    a.rerr_stride = ctl.MaxIterDivCor + 1;
+    a.stride = nN;
+    a.estride = nE;
+    a.nblk = blocks_for(nN, nrhs, a.chunk);
+    a.enblk = blocks_for(nE, nrhs, a.echunk);
+    a.maxit = ctl.MaxIterDivCor;
+    a.tol = ctl.tolDivCor;
+    return a;
+}
+
+int Solver::run_bicg(int nrhs, int precision, int maxit)
+{
+    if (precision == 0) {
+        KArgs<double> a = kargs<double>(nrhs, 0);
+        a.maxit = maxit;
+        launch_bicg_init(a, nrhs, stream_);
+        for (int it = 0; it < maxit; it++) launch_bicg_iter(a, nrhs, stream_);
+        launch_bicg_finish(a, nrhs, stream_);
+    } else {
+        KArgs<float> a = kargs<float>(nrhs, 1);
+        a.maxit = maxit;
+        launch_bicg_init(a, nrhs, stream_);
+        for (int it = 0; it < maxit; it++) launch_bicg_iter(a, nrhs, stream_);
+        launch_bicg_finish(a, nrhs, stream_);
+    }
+    return check(cudaGetLastError(), "BiCG launch");
+}
+
+int Solver::run_divcorr(int nrhs)
+{
+    DArgs a = dargs(nrhs);
+    launch_divcorr_start(a, nrhs, stream_);
+    for (int it = 1; it < ctl.MaxIterDivCor; it++) launch_divcorr_iter(a, nrhs, stream_);
+    launch_divcorr_finish(a, nrhs, stream_);
+    return check(cudaGetLastError(), "divergence correction launch");
+}
+
+// ---------------------------------------------------------------------------
+// y = A x on interior vectors
+// ---------------------------------------------------------------------------
+int Solver::mult_aii(int adjt, const double *x, double *y)
+{
+    if (!cond_set) return fail(5, "mt3d_mult_aii: conductivity not set (call mt3d_update_cond)");
+    if (!(omega > 0)) return fail(5, "mt3d_mult_aii: frequency not set (call mt3d_update_freq)");
+    if (!x || !y) return fail(5, "mt3d_mult_aii: null vector");
+    int rc;
+    if ((rc = ensure_workspace(1, ws_.precision < 0 ? 0 : ws_.precision))) return rc;
+    OuterState os{};
+    os.omega = omega;
+    os.active = 1;
+    if ((rc = check(cudaMemcpyAsync(ws_.ost.as<void>(), &os, sizeof os, cudaMemcpyHostToDevice, stream_), "copy state"))) return rc;
+    double2 *xf = ws_.bc.as<double2>(), *yf = ws_.tmp.as<double2>(), *xi = ws_.b.as<double2>();
+    cudaMemsetAsync(xf, 0, nE * sizeof(double2), stream_);
+    cudaMemcpyAsync(xi, x, nEi * sizeof(double2), cudaMemcpyHostToDevice, stream_);
+    launch_scatter_interior((int)nEi, edgei_d_.as<int>(), xi, xf, stream_);
+    KArgs<double> a = kargs<double>(1, 0);
+    a.dsgn = adjt ? 1.0 : -1.0;
+    launch_apply(a, xf, yf, 0, 1, stream_);
+    launch_gather_interior((int)nEi, edgei_d_.as<int>(), yf, xi, stream_);
+    cudaMemcpyAsync(y, xi, nEi * sizeof(double2), cudaMemcpyDeviceToHost, stream_);
+    return sync("mt3d_mult_aii");
+}
+
+// ---------------------------------------------------------------------------
+// one Krylov call on interior vectors (BICG / cuBiCG)
+// ---------------------------------------------------------------------------
+int Solver::bicg(const double *b, double *x, int maxit, double tol, int *niter, double *rerr, int *failed)
+{
+    if (!cond_set) return fail(5, "mt3d_bicg: conductivity not set (call mt3d_update_cond)");
+    if (!(omega > 0)) return fail(5, "mt3d_bicg: frequency not set (call mt3d_update_freq)");
+    if (!b || !x || maxit < 1 || !(tol > 0)) return fail(5, "mt3d_bicg: invalid arguments");
+    const int keep = ctl.IterPerDivCor;
+    ctl.IterPerDivCor = maxit;  // rerr rows of maxit+1 entries
+    int rc = ensure_workspace(1, 0);
+    ctl.IterPerDivCor = keep;
+    if (rc) return rc;
+    OuterState os{};
+    os.omega = omega;
+    os.tol = tol;
+    os.active = 1;
+    cudaMemcpyAsync(ws_.ost.as<void>(), &os, sizeof os, cudaMemcpyHostToDevice, stream_);
+    double2 *xi = ws_.tmp.as<double2>();
+    cudaMemsetAsync(ws_.b.as<void>(), 0, nE * sizeof(double2), stream_);
+    cudaMemsetAsync(ws_.X.as<void>(), 0, nE * sizeof(double2), stream_);
+    cudaMemcpyAsync(xi, b, nEi * sizeof(double2), cudaMemcpyHostToDevice, stream_);
+    launch_scatter_interior((int)nEi, edgei_d_.as<int>(), xi, ws_.b.as<double2>(), stream_);
+    cudaMemcpyAsync(xi, x, nEi * sizeof(double2), cudaMemcpyHostToDevice, stream_);
+    launch_scatter_interior((int)nEi, edgei_d_.as<int>(), xi, ws_.X.as<double2>(), stream_);
+    {
+        KArgs<double> a = kargs<double>(1, 0);
+        a.maxit = maxit;
+        a.rerr_stride = maxit + 1;
+        launch_bicg_init(a, 1, stream_);
+        for (int it = 0; it < maxit; it++) launch_bicg_iter(a, 1, stream_);
+        launch_bicg_finish(a, 1, stream_);
+    }
+    launch_gather_interior((int)nEi, edgei_d_.as<int>(), ws_.X.as<double2>(), xi, stream_);
+    cudaMemcpyAsync(x, xi, nEi * sizeof(double2), cudaMemcpyDeviceToHost, stream_);
+    BicgState st;
+    cudaMemcpyAsync(&st, ws_.bst.as<void>(), sizeof st, cudaMemcpyDeviceToHost, stream_);
+    std::vector<double> h(maxit + 1);
+    cudaMemcpyAsync(h.data(), ws_.rerr.as<void>(), (maxit + 1) * sizeof(double), cudaMemcpyDeviceToHost, stream_);
+    if ((rc = sync("mt3d_bicg"))) return rc;
+    const bool conv = st.status == KS_CONVERGED;
+    const int n = conv ? st.iter : maxit;
+    if (!conv && st.imin > 0) h[maxit - 1] = h[st.imin - 1];
+    if (!conv && st.imin == 0) h[maxit - 1] = h[0];
+    if (niter) *niter = n;
+    if (failed) *failed = (st.status == KS_BREAKDOWN || st.status == KS_NAN) ? 1 : 0;
+    if (rerr) std::memcpy(rerr, h.data(), maxit * sizeof(double));
+    if (st.status == KS_NAN) return fail(3, "mt3d_bicg: NaN in the right-hand side or iterates");
+    if (st.status == KS_BREAKDOWN) return fail(2, "mt3d_bicg: BiCGStab breakdown");
+    return conv ? 0 : 1;
+}
+
+// ---------------------------------------------------------------------------
+// FWDsolve3D over a batch of right-hand sides
+// ---------------------------------------------------------------------------
+int Solver::solve(int nrhs, const double *omegas, const int *trans, const double *bc, const double *src, double *e,
+                  int *status)
+{
+    if (!cond_set) return fail(5, "fwdsolve: conductivity not set (call mt3d_update_cond)");
+    if (nrhs < 1 || !omegas || !e) return fail(5, "fwdsolve: invalid arguments");
+    for (int r = 0; r < nrhs; r++)
+        if (!(omegas[r] > 0) || !std::isfinite(omegas[r])) return fail(5, "fwdsolve: omega must be positive and finite");
+    const int prec = ctl.precision;
+    int rc;
+    if ((rc = ensure_workspace(nrhs, prec))) return rc;
+    Workspace &w = ws_;
+    const size_t ebytes = nE * sizeof(double2);
+    // per right-hand side flags
+    std::vector<OuterState> os(nrhs);
+    for (int r = 0; r < nrhs; r++) {
+        OuterState &o = os[r];
+        o = OuterState{};
+        o.omega = omegas[r];
+        o.trans = trans ? (trans[r] != 0) : 0;
+        o.has_bc = 0;
+        o.has_src = 0;
+        if (bc) {
+            const double *v = bc + (size_t)r * nE * 2;
+            for (int64_t q = 0; q < 2 * nE && !o.has_bc; q++) o.has_bc = v[q] != 0.0;
+        }
+        if (src) {
+            const double *v = src + (size_t)r * nE * 2;
+            for (int64_t q = 0; q < 2 * nE && !o.has_src; q++) o.has_src = v[q] != 0.0;
+        }
+        o.tol = o.trans ? ctl.tolEMadj : (o.has_bc ? ctl.tolEMfwd : ctl.tolEMadj);
+        o.active = 1;
+    }
+    cudaMemcpyAsync(w.ost.as<void>(), os.data(), nrhs * sizeof(OuterState), cudaMemcpyHostToDevice, stream_);
+    double2 *B = w.b.as<double2>(), *X = w.X.as<double2>(), *BC = w.bc.as<double2>(), *TMP = w.tmp.as<double2>();
+    // boundary data (kept for the post-processing) and initial guess
+    cudaMemsetAsync(BC, 0, nrhs * ebytes, stream_);
+    if (bc) cudaMemcpyAsync(BC, bc, nrhs * ebytes, cudaMemcpyHostToDevice, stream_);
+    cudaMemcpyAsync(X, e, nrhs * ebytes, cudaMemcpyHostToDevice, stream_);
+    launch_keep_interior(g64_, X, nE, nrhs, stream_);
+    // forward right-hand side: b = -V_E A_IB bc (FWDsolve3D, f90/3D_MT/FWD/EMsolve3D.f90:186-200)
+    cudaMemcpyAsync(TMP, BC, nrhs * ebytes, cudaMemcpyDeviceToDevice, stream_);
+    for (int r = 0; r < nrhs; r++)
+        if (os[r].trans) cudaMemsetAsync(TMP + (size_t)r * nE, 0, ebytes, stream_);
+    launch_keep_boundary(g64_, TMP, nE, nrhs, stream_);
+    {
+        KArgs<double> a = kargs<double>(nrhs, 0);
+        launch_apply(a, TMP, B, 1, nrhs, stream_);
+    }
+    // sources: b += V_E src (forward) or b = src (transposed); phi0
+    bool any_src = false;
+    for (auto &o : os) any_src = any_src || o.has_src;
+    if (any_src) {
+        cudaMemcpyAsync(TMP, src, nrhs * ebytes, cudaMemcpyHostToDevice, stream_);
+        launch_keep_interior(g64_, TMP, nE, nrhs, stream_);
+        launch_add_src(g64_, B, TMP, nE, w.ost.as<OuterState>(), nrhs, stream_);
+        launch_phi0(g64_, TMP, nE, w.phi0.as<double2>(), nN, w.ost.as<OuterState>(), nrhs, stream_);
+    }
+    {
+        KArgs<double> a = kargs<double>(nrhs, 0);
+        launch_norm_b(a, nrhs, stream_);
+    }
+    // transposed problem without a source: zero solution (plus boundary data)
+    for (int r = 0; r < nrhs; r++)
+        if (os[r].trans && !os[r].has_src) {
+            os[r].active = 0;
+            os[r].converged = 1;
+        }
+    diag = Diag{};
+    std::vector<Diag> dg(nrhs);
+    auto push_state = [&]() {
+        cudaMemcpyAsync(w.ost.as<void>(), os.data(), nrhs * sizeof(OuterState), cudaMemcpyHostToDevice, stream_);
+    };
+    auto pull_state = [&]() -> int {
+        // only the device-written fields are taken over
+        std::vector<OuterState> dv(nrhs);
+        cudaMemcpyAsync(dv.data(), w.ost.as<void>(), nrhs * sizeof(OuterState), cudaMemcpyDeviceToHost, stream_);
+        int rc2 = sync("fwdsolve");
+        if (rc2) return rc2;
+        for (int r = 0; r < nrhs; r++) {
+            os[r].bnorm64 = dv[r].bnorm64;
+            os[r].relres = dv[r].relres;
+            os[r].scale = dv[r].scale;
+            os[r].divJ[0] = dv[r].divJ[0];
+            os[r].divJ[1] = dv[r].divJ[1];
+        }
+        return 0;
+    };
+    if ((rc = pull_state())) return rc;
+    for (int r = 0; r < nrhs; r++)
+        if (!std::isfinite(os[r].bnorm64)) {
+            os[r].active = 0;
+            os[r].failed = 3;
+        }
+    // initial divergence correction for a source term (EMsolve3D.f90:298-303)
+    bool any_dc = false;
+    for (int r = 0; r < nrhs; r++) {
+        os[r].dc_run = os[r].active && os[r].has_src;
+        if (os[r].dc_run) { os[r].nDivCor = 1; any_dc = true; }
+    }
+    push_state();
+    if (any_dc) {
+        if ((rc = run_divcorr(nrhs))) return rc;
+        if ((rc = pull_state())) return rc;
+        for (int r = 0; r < nrhs; r++)
+            if (os[r].dc_run) { dg[r].divJ.push_back(os[r].divJ[0]); dg[r].divJ.push_back(os[r].divJ[1]); }
+    }
+    std::vector<BicgState> bs(nrhs);
+    std::vector<double> rerr((size_t)nrhs * (ctl.IterPerDivCor + 1));
+    auto any_active = [&]() {
+        for (auto &o : os) if (o.active) return true;
+        return false;
+    };
+    while (any_active()) {
+        if (prec == 1) {
+            // true FP64 residual r64 = b - A X (into tmp); converged right-hand
+            // sides leave the loop, the others get an FP32 correction solve
+            for (auto &o : os) o.dc_run = 0;
+            push_state();
+            {
+                KArgs<double> a = kargs<double>(nrhs, 0);
+                a.r = w.tmp.as<double2>();
+                launch_res64(a, nrhs, stream_);
+            }
+            if ((rc = pull_state())) return rc;
+            bool work = false;
+            for (int r = 0; r < nrhs; r++) {
+                OuterState &o = os[r];
+                if (!o.active) continue;
+                if (!std::isfinite(o.relres)) { o.active = 0; o.failed = 3; continue; }
+                if (o.relres <= o.tol) { o.active = 0; o.converged = 1; continue; }
+                if (o.nDivCor >= ctl.MaxDivCor) { o.active = 0; o.failed = 1; continue; }
+                o.tol_inner = o.tol * o.bnorm64 * o.scale;  // tol*||b|| relative to ||r64||
+                work = true;
+            }
+            if (!work) break;
+            push_state();
+            launch_cast(w.ost.as<OuterState>(), (int)nE, nE, w.tmp.as<double2>(), w.f_b.as<float2>(),
+                        w.f_x0.as<float2>(), nrhs, stream_);
+        }
+        // Krylov call: FP64 on (b, X), or FP32 on the normalised residual
+        if ((rc = run_bicg(nrhs, prec, ctl.IterPerDivCor))) return rc;
+        if (prec == 1)
+            launch_update(w.ost.as<OuterState>(), (int)nE, nE, w.f_x0.as<float2>(), X, nrhs, stream_);
+        cudaMemcpyAsync(bs.data(), w.bst.as<void>(), nrhs * sizeof(BicgState), cudaMemcpyDeviceToHost, stream_);
+        cudaMemcpyAsync(rerr.data(), w.rerr.as<void>(), rerr.size() * sizeof(double), cudaMemcpyDeviceToHost, stream_);
+        if ((rc = sync("fwdsolve Krylov cycle"))) return rc;
+        for (int r = 0; r < nrhs; r++) {
+            OuterState &o = os[r];
+            o.dc_run = 0;
+            if (!o.active) continue;
+            const BicgState &st = bs[r];
+            const int maxit = ctl.IterPerDivCor;
+            const bool conv = st.status == KS_CONVERGED;
+            const int niter = conv ? st.iter : maxit;
+            double *h = &rerr[(size_t)r * (maxit + 1)];
+            if (!conv) h[maxit - 1] = st.imin > 0 ? h[st.imin - 1] : h[0];
+            for (int k = 0; k < niter; k++) dg[r].EMrelErr.push_back(h[k]);
+            o.nIterTotal += niter;
+            if (prec == 0) {
+                if (conv) o.converged = 1;
+                if (st.status == KS_BREAKDOWN || st.status == KS_NAN) o.failed = (st.status == KS_NAN) ? 3 : 2;
+            } else if (st.status == KS_NAN) {
+                o.failed = 3;
+            }
+            o.nDivCor += 1;
+            if (o.nDivCor < ctl.MaxDivCor) {
+                o.dc_run = 1;
+            } else if (prec == 0) {
+                if (!o.failed) o.failed = 1;
+            }
+        }
+        push_state();
+        bool dc = false;
+        for (auto &o : os) dc = dc || o.dc_run;
+        if (dc) {
+            if ((rc = run_divcorr(nrhs))) return rc;
+            if ((rc = pull_state())) return rc;
+            for (int r = 0; r < nrhs; r++)
+                if (os[r].dc_run) { dg[r].divJ.push_back(os[r].divJ[0]); dg[r].divJ.push_back(os[r].divJ[1]); }
+        }
+        for (int r = 0; r < nrhs; r++) {
+            OuterState &o = os[r];
+            o.dc_run = 0;
+            if (!o.active) continue;
+            if (prec == 0) {
+                if (o.converged || o.failed) o.active = 0;
+            } else if (o.failed == 3) {
+                o.active = 0;
+            }
+        }
+    }
+    // true relative residual of the returned interior field (all right-hand sides)
+    for (auto &o : os) { o.active = 1; o.dc_run = 0; }
+    push_state();
+    {
+        KArgs<double> a = kargs<double>(nrhs, 0);
+        if (prec == 1) a.r = w.tmp.as<double2>();
+        launch_res64(a, nrhs, stream_);
+    }
+    if ((rc = pull_state())) return rc;
+    // post-processing and copy back
+    launch_post(g64_, X, BC, nE, w.ost.as<OuterState>(), nrhs, stream_);
+    cudaMemcpyAsync(e, X, nrhs * ebytes, cudaMemcpyDeviceToHost, stream_);
+    if ((rc = sync("fwdsolve copy back"))) return rc;
+    int worst = 0;
+    for (int r = 0; r < nrhs; r++) {
+        OuterState &o = os[r];
+        int s = 0;
+        if (o.failed == 3) s = 3;
+        else if (o.failed == 2) s = 2;
+        else if (!o.converged) s = 1;
+        if (status) status[r] = s;
+        worst = std::max(worst, s);
+        dg[r].nIterTotal = o.nIterTotal;
+        dg[r].nDivCor = o.nDivCor;
+        dg[r].failed = s != 0;
+        dg[r].final_relres = o.relres;
+    }
+    diag = dg[0];
+    if (worst == 3) return fail(3, "fwdsolve: NaN/Inf in the right-hand side or iterates");
+    if (worst == 2) return fail(2, "fwdsolve: BiCGStab breakdown");
+    return worst;
+}
+
+int Solver::pmult_t(int npol, const double *e0, const double *eadj, const double *m0, double *dm)
+{
+    if (npol < 1 || !e0 || !eadj || !m0 || !dm) return fail(5, "mt3d_pmult_t: invalid arguments");
+    if (!(omega > 0)) return fail(5, "mt3d_pmult_t: frequency not set (call mt3d_update_freq)");
+    const size_t eb = (size_t)npol * nE * sizeof(double2);
+    const int64_t nEarth = (int64_t)nx * ny * (nz - nzAir);
+    DevBuf a, b, m, d;
+    if (a.alloc(eb) || b.alloc(eb) || m.alloc(nEarth * sizeof(double)) || d.alloc(nEarth * sizeof(double)))
+        return fail(8, "mt3d_pmult_t: out of device memory");
+    cudaMemcpyAsync(a.as<void>(), e0, eb, cudaMemcpyHostToDevice, stream_);
+    cudaMemcpyAsync(b.as<void>(), eadj, eb, cudaMemcpyHostToDevice, stream_);
+    cudaMemcpyAsync(m.as<void>(), m0, nEarth * sizeof(double), cudaMemcpyHostToDevice, stream_);
+    launch_pmult_t(g64_, npol, a.as<double2>(), b.as<double2>(), omega, m.as<double>(), d.as<double>(), stream_);
+    cudaMemcpyAsync(dm, d.as<void>(), nEarth * sizeof(double), cudaMemcpyDeviceToHost, stream_);
+    return sync("mt3d_pmult_t");
+}
+
+}  // namespace mt3d

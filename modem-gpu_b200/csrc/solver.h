@@ -1,0 +1,98 @@
+// solver.h -- host-side solver object behind the C ABI.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "kernels.h"
+
+namespace mt3d {
+
+struct Control {
+    int IterPerDivCor = 40;  // f90/3D_MT/FWD/EMsolve3D.f90:58-68 defaults
+    int MaxDivCor = 20;
+    int MaxIterDivCor = 100;
+    double tolEMfwd = 1e-7;
+    double tolEMadj = 1e-7;
+    double tolDivCor = 1e-5;
+    int solver = 1;     // BICG
+    int precision = 0;  // 0 FP64, 1 mixed
+};
+
+struct Diag {
+    int nIterTotal = 0, nDivCor = 0, failed = 0;
+    std::vector<double> EMrelErr;
+    std::vector<double> divJ;  // pairs
+    double final_relres = 0.0;
+};
+
+class DevBuf {
+  public:
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { release(); }
+    int alloc(size_t bytes);
+    void release();
+    template <typename T> T *as() const { return reinterpret_cast<T *>(ptr_); }
+    size_t bytes() const { return bytes_; }
+
+  private:
+    void *ptr_ = nullptr;
+    size_t bytes_ = 0;
+};
+
+struct Workspace {
+    int nrhs = 0;
+    int precision = -1;
+    int rlen = 0, dlen = 0;  // rerr row lengths the buffers were sized for
+    // FP64 edge vectors [nrhs][nE]
+    DevBuf b, X, x1, r, rt, p, v, ph, s, sh, t, bc, tmp;
+    // FP32 edge vectors (mixed)
+    DevBuf f_b, f_x0, f_x1, f_r, f_rt, f_p, f_v, f_ph, f_s, f_sh, f_t;
+    // FP64 node vectors [nrhs][nN]
+    DevBuf px, pr, pp, pq, phi0;
+    DevBuf bst, pst, ost, parts, cnt, rerr, dcrerr;
+};
+
+class Solver {
+  public:
+    ~Solver();
+    int create(int dev, int nx, int ny, int nz, int nzAir, const double *dx, const double *dy, const double *dz);
+    int update_cond(const double *m_earth, double airCond);
+    int update_freq(double omega);
+    int mult_aii(int adjt, const double *x, double *y);
+    int bicg(const double *b, double *x, int maxit, double tol, int *niter, double *rerr, int *failed);
+    int solve(int nrhs, const double *omegas, const int *trans, const double *bc, const double *src, double *e,
+              int *status);
+    int pmult_t(int npol, const double *e0, const double *eadj, const double *m0, double *dm);
+
+    int fail(int code, const std::string &msg);
+    std::string last_error;
+    Control ctl;
+    Diag diag;
+    int nx = 0, ny = 0, nz = 0, nzAir = 0;
+    int64_t nE = 0, nEi = 0, nN = 0;
+    std::vector<int32_t> edgei;  // 0-based interior edge list
+    double omega = 0.0;
+    bool cond_set = false;
+
+  private:
+    int ensure_workspace(int nrhs, int precision);
+    int run_bicg(int nrhs, int precision, int maxit);
+    int run_divcorr(int nrhs);
+    template <typename T> KArgs<T> kargs(int nrhs, int precision_ws);
+    DArgs dargs(int nrhs);
+    int check(cudaError_t e, const char *what);
+    int sync(const char *what);
+
+    int dev_ = 0;
+    cudaStream_t stream_ = nullptr;
+    Geo<double> g64_{};
+    Geo<float> g32_{};
+    DevBuf tab64_, tab32_, sig64_, sig32_, coef_, edgei_d_;
+    Workspace ws_;
+    std::vector<double> dx_, dy_, dz_, delX_, delY_, delZ_;
+};
+
+}  // namespace mt3d

@@ -1,0 +1,194 @@
+"""ctypes binding of libmt3d.so (include/mt3d.h).
+
+This mirrors, in Python, the calls a ModEM host makes around its forward
+solver: ``ModelDataInit`` (Solver(...)), ``UpdateCond``, ``UpdateFreq``,
+``Mult_Aii``, ``BICG`` and ``FWDsolve3D`` (f90/3D_MT/FWD/modelOperator3D.f90,
+f90/3D_MT/FWD/EMsolve3D.f90, f90/3D_MT/FWD_SP2/solver.f90).  There is no CPU
+fallback: if the library or a CUDA device is missing, calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libmt3d.so")
+
+STATUS = {0: "MT3D_OK", 1: "MT3D_NOT_CONVERGED", 2: "MT3D_BREAKDOWN", 3: "MT3D_NAN_INPUT", 4: "MT3D_CUDA_ERROR",
+          5: "MT3D_INVALID_ARGUMENT", 6: "MT3D_DEVICE_TIMEOUT", 7: "MT3D_NO_DEVICE", 8: "MT3D_OUT_OF_MEMORY"}
+SOLVER_BICG = 1
+PREC_FP64, PREC_MIXED = 0, 1
+
+#: every symbol include/mt3d.h declares
+EXPORTS = ["mt3d_version", "mt3d_device_count", "mt3d_create", "mt3d_destroy", "mt3d_set_control", "mt3d_update_cond",
+           "mt3d_update_freq", "mt3d_sizes", "mt3d_interior_index", "mt3d_mult_aii", "mt3d_bicg", "mt3d_fwdsolve",
+           "mt3d_fwdsolve_batch", "mt3d_get_diag", "mt3d_pmult_t", "mt3d_last_error"]
+
+_lib = None
+
+
+class MT3DError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+def load(path: str = LIB_PATH):
+    """Load libmt3d.so; raises if it is missing (build it with build.py)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} not found: build the CUDA library first (python modem-gpu_b200/build.py)")
+    L = C.CDLL(path)
+    P = C.c_void_p
+    D = C.POINTER(C.c_double)
+    I = C.c_int
+    IP = C.POINTER(C.c_int)
+    L.mt3d_version.restype = C.c_char_p
+    L.mt3d_device_count.restype = I
+    L.mt3d_create.argtypes = [I, I, I, I, I, D, D, D, C.POINTER(P)]
+    L.mt3d_destroy.argtypes = [P]
+    L.mt3d_set_control.argtypes = [P, I, I, I, C.c_double, C.c_double, C.c_double, I, I]
+    L.mt3d_update_cond.argtypes = [P, D, C.c_double]
+    L.mt3d_update_freq.argtypes = [P, C.c_double]
+    L.mt3d_sizes.argtypes = [P, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    L.mt3d_interior_index.argtypes = [P, C.POINTER(C.c_int32)]
+    L.mt3d_mult_aii.argtypes = [P, I, D, D]
+    L.mt3d_bicg.argtypes = [P, D, D, I, C.c_double, IP, D, IP]
+    L.mt3d_fwdsolve.argtypes = [P, I, D, D, D]
+    L.mt3d_fwdsolve_batch.argtypes = [P, I, D, IP, D, D, D, IP]
+    L.mt3d_get_diag.argtypes = [P, IP, IP, IP, D, I, D, I, D]
+    L.mt3d_pmult_t.argtypes = [P, I, D, D, D, D]
+    L.mt3d_last_error.argtypes = [P, C.c_char_p, I]
+    for name in EXPORTS:
+        getattr(L, name).restype = getattr(L, name).restype or I
+    L.mt3d_version.restype = C.c_char_p
+    _lib = L
+    return L
+
+
+def _d(a):
+    if a is None:
+        return None
+    assert a.flags.c_contiguous and a.dtype in (np.float64, np.complex128)
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class Solver:
+    """One solver handle: a grid, its conductivity model and a frequency."""
+
+    def __init__(self, grid, device: int = 0):
+        self.L = load()
+        self.grid = grid
+        self.h = C.c_void_p()
+        dx = np.ascontiguousarray(grid.dx, np.float64)
+        dy = np.ascontiguousarray(grid.dy, np.float64)
+        dz = np.ascontiguousarray(grid.dz, np.float64)
+        rc = self.L.mt3d_create(device, grid.nx, grid.ny, grid.nz, grid.nzAir, _d(dx), _d(dy), _d(dz),
+                                C.byref(self.h))
+        if rc:
+            raise MT3DError(rc, self._err(None))
+        nE, nEi, nN = C.c_int64(), C.c_int64(), C.c_int64()
+        self.L.mt3d_sizes(self.h, C.byref(nE), C.byref(nEi), C.byref(nN))
+        self.nE, self.nEi, self.nN = nE.value, nEi.value, nN.value
+
+    def _err(self, h):
+        buf = C.create_string_buffer(512)
+        self.L.mt3d_last_error(h, buf, 512)
+        return buf.value.decode()
+
+    def _check(self, rc, allow=(0,)):
+        if rc not in allow:
+            raise MT3DError(rc, self._err(self.h))
+        return rc
+
+    def close(self):
+        if self.h:
+            self.L.mt3d_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_control(self, IterPerDivCor=40, MaxDivCor=20, MaxIterDivCor=100, tolEMfwd=1e-7, tolEMadj=1e-7,
+                    tolDivCor=1e-5, solver=SOLVER_BICG, precision=PREC_FP64):
+        self._check(self.L.mt3d_set_control(self.h, IterPerDivCor, MaxDivCor, MaxIterDivCor, tolEMfwd, tolEMadj,
+                                            tolDivCor, solver, precision))
+
+    def update_cond(self, m_earth, air_cond):
+        m = np.ascontiguousarray(m_earth, np.float64)
+        self._check(self.L.mt3d_update_cond(self.h, _d(m), float(air_cond)))
+
+    def update_freq(self, omega):
+        self._check(self.L.mt3d_update_freq(self.h, float(omega)))
+
+    def interior_index(self):
+        out = np.zeros(self.nEi, np.int32)
+        self._check(self.L.mt3d_interior_index(self.h, out.ctypes.data_as(C.POINTER(C.c_int32))))
+        return out
+
+    def mult_aii(self, x, adjt=False):
+        x = np.ascontiguousarray(x, np.complex128)
+        y = np.zeros(self.nEi, np.complex128)
+        self._check(self.L.mt3d_mult_aii(self.h, int(adjt), _d(x), _d(y)))
+        return y
+
+    def bicg(self, b, x0, maxit, tol):
+        b = np.ascontiguousarray(b, np.complex128)
+        x = np.array(x0, np.complex128)
+        rerr = np.zeros(maxit)
+        n, f = C.c_int(), C.c_int()
+        rc = self._check(self.L.mt3d_bicg(self.h, _d(b), _d(x), int(maxit), float(tol), C.byref(n), _d(rerr),
+                                          C.byref(f)), allow=(0, 1, 2, 3))
+        return x, n.value, rerr, f.value, rc
+
+    def fwdsolve(self, trans=False, bc=None, src=None, e0=None):
+        e = np.zeros(self.nE, np.complex128) if e0 is None else np.array(e0, np.complex128)
+        bcp = None if bc is None else np.ascontiguousarray(bc, np.complex128)
+        srcp = None if src is None else np.ascontiguousarray(src, np.complex128)
+        rc = self._check(self.L.mt3d_fwdsolve(self.h, int(trans), _d(bcp), _d(srcp), _d(e)), allow=(0, 1, 2, 3))
+        return e, rc
+
+    def fwdsolve_batch(self, omegas, trans=None, bc=None, src=None, e0=None):
+        omegas = np.ascontiguousarray(omegas, np.float64)
+        n = omegas.size
+        tr = np.zeros(n, np.int32) if trans is None else np.ascontiguousarray(trans, np.int32)
+        e = np.zeros((n, self.nE), np.complex128) if e0 is None else np.array(e0, np.complex128)
+        bcp = None if bc is None else np.ascontiguousarray(bc, np.complex128)
+        srcp = None if src is None else np.ascontiguousarray(src, np.complex128)
+        st = np.zeros(n, np.int32)
+        rc = self._check(self.L.mt3d_fwdsolve_batch(self.h, n, _d(omegas), tr.ctypes.data_as(C.POINTER(C.c_int)),
+                                                    _d(bcp), _d(srcp), _d(e), st.ctypes.data_as(C.POINTER(C.c_int))),
+                         allow=(0, 1, 2, 3))
+        return e, st, rc
+
+    def diagnostics(self, maxlen=4000, maxdc=200):
+        nit, ndc, fl = C.c_int(), C.c_int(), C.c_int()
+        rel = np.zeros(maxlen)
+        dj = np.zeros(2 * maxdc)
+        fr = C.c_double()
+        self._check(self.L.mt3d_get_diag(self.h, C.byref(nit), C.byref(ndc), C.byref(fl), _d(rel), maxlen, _d(dj),
+                                         maxdc, C.byref(fr)))
+        return dict(nIterTotal=nit.value, nDivCor=ndc.value, failed=bool(fl.value),
+                    EMrelErr=rel[: min(nit.value, maxlen)].copy(), divJ=dj.reshape(-1, 2)[: ndc.value].copy(),
+                    final_relres=fr.value)
+
+    def pmult_t(self, e0, eadj, m0_earth):
+        e0 = np.ascontiguousarray(e0, np.complex128)
+        ea = np.ascontiguousarray(eadj, np.complex128)
+        npol = e0.shape[0] if e0.ndim == 2 else 1
+        m0 = np.ascontiguousarray(m0_earth, np.float64)
+        g = self.grid
+        out = np.zeros(g.nx * g.ny * g.nzEarth)
+        self._check(self.L.mt3d_pmult_t(self.h, npol, _d(e0), _d(ea), _d(m0), _d(out)))
+        return out
+
+
+def device_count() -> int:
+    return int(load().mt3d_device_count())

@@ -1,0 +1,225 @@
+"""GPU parity: the CUDA path (through the C ABI, libmt3d.so) against the oracle.
+
+Tolerances (FP64 unless stated):
+  * operator apply: relative 2-norm difference <= 1e-13 (summation order only);
+  * BiCGStab residual history: <= 1e-8 relative over the first iterations;
+  * solutions of the full divergence-corrected solve: <= 1e-5 relative on the
+    edges where the field is unique (sigma > 0), both solves at tol 1e-7 or
+    tighter; the air edges carry a gauge (gradient) part that only the
+    divergence correction pins;
+  * mixed precision (FP32 inner iterations, FP64 refinement) against FP64:
+    the same 1e-5 bound, and a true FP64 relative residual <= the tolerance.
+"""
+import numpy as np
+import pytest
+
+from helpers import earth_mask, random_model, relerr, small_grid
+from mt3d import bc as mbc
+from mt3d import capi, models
+from oracle.oracle import BICG, PC_JACOBI, Oracle, interior_edge_mask
+
+pytestmark = pytest.mark.gpu
+
+
+def make_pair(g, m, omega, **ctl):
+    o = Oracle(g)
+    o.update_cond(m.m_earth, m.air_cond)
+    o.update_freq(omega)
+    o.set_control(solver=BICG, precond=PC_JACOBI, **ctl)
+    s = capi.Solver(g)
+    s.update_cond(m.m_earth, m.air_cond)
+    s.update_freq(omega)
+    s.set_control(**ctl)
+    return o, s
+
+
+@pytest.fixture(scope="module")
+def prob(cuda):
+    g = small_grid()
+    m = random_model(g, seed=3)
+    omega = 2 * np.pi * 0.5
+    o, s = make_pair(g, m, omega)
+    return g, m, omega, o, s
+
+
+def test_interior_index(prob):
+    g, m, omega, o, s = prob
+    idx = s.interior_index() - 1
+    assert np.array_equal(np.flatnonzero(interior_edge_mask(g)), idx)
+
+
+def test_mult_aii_matches_oracle(prob):
+    g, m, omega, o, s = prob
+    mask = interior_edge_mask(g)
+    rng = np.random.default_rng(0)
+    xi = rng.standard_normal(s.nEi) + 1j * rng.standard_normal(s.nEi)
+    x = np.zeros(g.n_edges, complex)
+    x[mask] = xi
+    for adjt in (False, True):
+        y = s.mult_aii(xi, adjt=adjt)
+        yref = o.multA(x, adjt=adjt)[mask]
+        assert relerr(y, yref) < 1e-13
+
+
+def test_bicg_history_matches_oracle(prob):
+    g, m, omega, o, s = prob
+    mask = interior_edge_mask(g)
+    bcv = mbc.boundary_1d(m, omega, 2)
+    b = -o.multA(np.where(mask, 0, bcv))
+    x0 = np.zeros(g.n_edges, complex)
+    xo, no, ro, fo = o.krylov(b, x0, 40, 1e-7)
+    xg, ng, rg, fg, rc = s.bicg(b[mask], np.zeros(s.nEi, complex), 40, 1e-7)
+    assert fo == fg == 0
+    k = min(12, ng, no)
+    assert np.max(np.abs(rg[:k] - ro[:k]) / ro[:k]) < 1e-8
+    if no == ng:
+        assert relerr(xg, xo[mask]) < 1e-6
+
+
+@pytest.mark.parametrize("mode", [1, 2])
+def test_fwdsolve_fp64_matches_oracle(prob, mode):
+    g, m, omega, o, s = prob
+    bcv = mbc.boundary_1d(m, omega, mode)
+    s.set_control(precision=capi.PREC_FP64)
+    eg, rc = s.fwdsolve(bc=bcv)
+    eo, rco = o.fwdsolve(bc=bcv)
+    assert rc == 0 and rco == 0
+    em = earth_mask(g, m)
+    assert relerr(eg[em], eo[em]) < 1e-5
+    bmask = ~interior_edge_mask(g)
+    assert np.array_equal(eg[bmask], bcv[bmask])
+    dg, do = s.diagnostics(), o.diagnostics()
+    assert dg["nDivCor"] >= 1
+    assert abs(dg["nIterTotal"] - do["nIterTotal"]) <= max(3, 0.1 * do["nIterTotal"])
+    assert dg["final_relres"] < 5e-7
+
+
+def test_fwdsolve_mixed_matches_fp64(prob):
+    g, m, omega, o, s = prob
+    bcv = mbc.boundary_1d(m, omega, 1)
+    s.set_control(precision=capi.PREC_FP64)
+    e64, rc64 = s.fwdsolve(bc=bcv)
+    s.set_control(precision=capi.PREC_MIXED)
+    emx, rcm = s.fwdsolve(bc=bcv)
+    d = s.diagnostics()
+    s.set_control(precision=capi.PREC_FP64)
+    assert rc64 == 0 and rcm == 0
+    assert d["final_relres"] <= 1e-7
+    em = earth_mask(g, m)
+    assert relerr(emx[em], e64[em]) < 1e-5
+
+
+def test_layered_closed_form_gpu(cuda):
+    g = small_grid()
+    m = models.halfspace_model(g, 30.0)
+    omega = 2 * np.pi * 0.1
+    s = capi.Solver(g)
+    s.update_cond(m.m_earth, m.air_cond)
+    s.update_freq(omega)
+    for prec in (capi.PREC_FP64, capi.PREC_MIXED):
+        s.set_control(tolEMfwd=1e-9, precision=prec)
+        for mode in (1, 2):
+            e, rc = s.fwdsolve(bc=mbc.boundary_1d(m, omega, mode))
+            assert rc == 0
+            assert relerr(e, mbc.layered_solution(m, omega, mode)) < 1e-6
+
+
+def test_batch_matches_single(prob):
+    g, m, omega, o, s = prob
+    oms = np.array([omega, omega, 2 * np.pi * 0.05, 2 * np.pi * 0.05])
+    modes = [1, 2, 1, 2]
+    bcs = np.stack([mbc.boundary_1d(m, w, md) for w, md in zip(oms, modes)])
+    for prec in (capi.PREC_FP64, capi.PREC_MIXED):
+        s.set_control(precision=prec)
+        eb, st, rc = s.fwdsolve_batch(oms, bc=bcs)
+        assert rc == 0 and np.all(st == 0)
+        for r in range(4):
+            s.update_freq(oms[r])
+            e1, rc1 = s.fwdsolve(bc=bcs[r])
+            assert rc1 == 0
+            assert relerr(eb[r], e1) < 1e-12
+    s.update_freq(omega)
+    s.set_control(precision=capi.PREC_FP64)
+
+
+def test_transposed_solve_matches_oracle(prob):
+    g, m, omega, o, s = prob
+    mask = interior_edge_mask(g)
+    em = mask & earth_mask(g, m)
+    rng = np.random.default_rng(4)
+    src = np.where(em, rng.standard_normal(g.n_edges) + 1j * rng.standard_normal(g.n_edges), 0)
+    src = src * o.VE
+    eg, rc = s.fwdsolve(trans=True, src=src)
+    eo, rco = o.fwdsolve(trans=True, src=src)
+    assert rc == 0 and rco == 0
+    emask = earth_mask(g, m)
+    assert relerr(eg[emask], eo[emask]) < 1e-5
+    # boundary values from AdjtBC of the V_E-weighted interior solution
+    bm = ~mask
+    assert relerr(eg[bm], o.adjt_bc(np.where(mask, eg, 0))[bm] * -1) < 1e-10
+
+
+def test_forward_source_matches_oracle(prob):
+    g, m, omega, o, s = prob
+    mask = interior_edge_mask(g)
+    em = mask & earth_mask(g, m)
+    rng = np.random.default_rng(9)
+    src = np.where(em, rng.standard_normal(g.n_edges) + 1j * rng.standard_normal(g.n_edges), 0)
+    eg, rc = s.fwdsolve(trans=False, src=src)
+    eo, rco = o.fwdsolve(trans=False, src=src)
+    assert rc == 0 and rco == 0
+    emask = earth_mask(g, m)
+    assert relerr(eg[emask], eo[emask]) < 1e-5
+
+
+def test_pmult_t_matches_oracle(prob):
+    g, m, omega, o, s = prob
+    rng = np.random.default_rng(2)
+    e0 = rng.standard_normal((2, g.n_edges)) + 1j * rng.standard_normal((2, g.n_edges))
+    ea = rng.standard_normal((2, g.n_edges)) + 1j * rng.standard_normal((2, g.n_edges))
+    assert relerr(s.pmult_t(e0, ea, m.m_earth), o.pmult_t(e0, ea, m.m_earth)) < 1e-13
+
+
+def test_config_small_forward_matches_oracle(cuda):
+    """The 24x24x24 forward configuration (100 ohm-m halfspace with a 1 ohm-m
+    block, 0.1 Hz, both polarisations) through the batch entry point."""
+    m, freqs = models.config_small_forward()
+    g = m.grid
+    omega = 2 * np.pi * freqs[0]
+    o, s = make_pair(g, m, omega)
+    bcs = np.stack([mbc.boundary_1d(m, omega, md) for md in (1, 2)])
+    em = earth_mask(g, m)
+    for prec in (capi.PREC_FP64, capi.PREC_MIXED):
+        s.set_control(precision=prec)
+        eb, st, rc = s.fwdsolve_batch(np.array([omega, omega]), bc=bcs)
+        assert rc == 0
+        for r, md in enumerate((1, 2)):
+            eo, rco = o.fwdsolve(bc=bcs[r])
+            assert rco == 0
+            assert relerr(eb[r][em], eo[em]) < 1e-5
+
+
+def test_error_paths(cuda):
+    g = small_grid()
+    s = capi.Solver(g)
+    m = random_model(g)
+    bad = m.m_earth.copy()
+    bad[3] = np.nan
+    with pytest.raises(capi.MT3DError) as ei:
+        s.update_cond(bad, m.air_cond)
+    assert ei.value.code == 3
+    with pytest.raises(capi.MT3DError) as ei:
+        s.fwdsolve(bc=np.zeros(s.nE, complex))
+    assert ei.value.code == 5  # conductivity not set
+    s.update_cond(m.m_earth, m.air_cond)
+    with pytest.raises(capi.MT3DError) as ei:
+        s.update_freq(-1.0)
+    assert ei.value.code == 5
+    with pytest.raises(capi.MT3DError) as ei:
+        s.set_control(precision=7)
+    assert ei.value.code == 5
+    s.update_freq(1.0)
+    bcv = np.zeros(s.nE, complex)
+    bcv[0] = np.nan
+    e, rc = s.fwdsolve(bc=bcv)
+    assert rc == 3

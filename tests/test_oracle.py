@@ -1,0 +1,171 @@
+"""CPU tests of the oracle (the checker of the CUDA path).
+
+The oracle restates ModEM's matrix-free operator and solver.  These tests pin
+it independently of its own code: against the SP2 sparse-matrix construction
+of the same operator, against direct sparse solves, against the closed-form
+solution of a layered model, and against the reference's own identities
+(symmetry of the operator; AdjtBC = A_IB^T; PmultT = transpose of Pmult,
+the Stest-style check of f90/SENS/SymmetryTest.f90:205-272).
+"""
+import numpy as np
+import pytest
+import scipy.sparse.linalg as spla
+
+from helpers import assemble_A, assemble_cc, direct_solve, earth_mask, edge_volumes, random_model, relerr, small_grid
+from mt3d import bc as mbc
+from mt3d import models
+from oracle.oracle import BICG, PC_DILU, PC_JACOBI, QMR, Oracle, interior_edge_mask
+
+
+@pytest.fixture(scope="module")
+def setup():
+    g = small_grid()
+    m = random_model(g, seed=3)
+    o = Oracle(g)
+    o.update_cond(m.m_earth, m.air_cond)
+    omega = 2 * np.pi * 0.5
+    o.update_freq(omega)
+    return g, m, o, omega
+
+
+def test_edge_conductivity_matches_numpy(setup):
+    g, m, o, _ = setup
+    assert np.allclose(o.sigE, mbc.edge_conductivity(m), rtol=1e-14, atol=0)
+
+
+def test_edge_volume(setup):
+    g, m, o, _ = setup
+    assert np.allclose(o.VE, edge_volumes(g), rtol=1e-15)
+
+
+def test_stencil_matches_sparse_assembly(setup):
+    g, m, o, omega = setup
+    A = assemble_A(g, m, omega)
+    mask = interior_edge_mask(g)
+    rng = np.random.default_rng(0)
+    x = rng.standard_normal(g.n_edges) + 1j * rng.standard_normal(g.n_edges)
+    y = o.multA(x)
+    yref = A @ x
+    assert relerr(y[mask], yref[mask]) < 1e-13
+    assert np.all(y[~mask] == 0)
+
+
+def test_operator_complex_symmetric_and_adjoint(setup):
+    g, m, o, _ = setup
+    mask = interior_edge_mask(g)
+    rng = np.random.default_rng(1)
+    x = np.where(mask, rng.standard_normal(g.n_edges) + 1j * rng.standard_normal(g.n_edges), 0)
+    y = np.where(mask, rng.standard_normal(g.n_edges) + 1j * rng.standard_normal(g.n_edges), 0)
+    # A^T = A on the interior system
+    assert abs(y @ o.multA(x) - x @ o.multA(y)) < 1e-12 * abs(y @ o.multA(x))
+    # conjugate transpose: <y, A x> = <A^H y, x>
+    lhs = np.vdot(y, o.multA(x))
+    rhs = np.vdot(o.multA(y, adjt=True), x)
+    assert abs(lhs - rhs) < 1e-12 * abs(lhs)
+
+
+def test_layered_model_closed_form():
+    g = small_grid()
+    m = models.halfspace_model(g, 30.0)
+    o = Oracle(g)
+    o.update_cond(m.m_earth, m.air_cond)
+    omega = 2 * np.pi * 0.1
+    o.update_freq(omega)
+    o.set_control(solver=BICG, precond=PC_JACOBI, tolEMfwd=1e-10)
+    for mode in (1, 2):
+        e, rc = o.fwdsolve(bc=mbc.boundary_1d(m, omega, mode))
+        assert rc == 0
+        ref = mbc.layered_solution(m, omega, mode)
+        assert relerr(e, ref) < 1e-7
+
+
+@pytest.mark.parametrize("solver,pc", [(QMR, PC_DILU), (BICG, PC_DILU), (BICG, PC_JACOBI)])
+def test_fwdsolve_matches_direct_solve(setup, solver, pc):
+    g, m, o, omega = setup
+    bcv = mbc.boundary_1d(m, omega, 2)
+    edir, _ = direct_solve(g, m, omega, bcv)
+    o.set_control(solver=solver, precond=pc, tolEMfwd=1e-9)
+    e, rc = o.fwdsolve(bc=bcv)
+    assert rc == 0
+    em = earth_mask(g, m)
+    assert relerr(e[em], edir[em]) < 1e-6
+    d = o.diagnostics()
+    assert d["nDivCor"] >= 1 and d["EMrelErr"][-1] < 1e-9
+
+
+def test_bicg_rhs_equals_minus_aib_bc(setup):
+    g, m, o, omega = setup
+    bcv = mbc.boundary_1d(m, omega, 1)
+    mask = interior_edge_mask(g)
+    A = assemble_A(g, m, omega)
+    b_ref = -(A[mask][:, ~mask] @ bcv[~mask])
+    b = -o.multA(np.where(mask, 0, bcv))[mask]
+    assert relerr(b, b_ref) < 1e-13
+
+
+def test_adjt_bc_is_transpose_of_aib(setup):
+    """AdjtBC(e) computes A_IB^T e for the curl-curl part (AdjtBC comment,
+    f90/3D_MT/FWD/modelOperator3D.f90:920-943); only boundary edges that are
+    not shared by two faces are well defined through the face arrays."""
+    g, m, o, omega = setup
+    mask = interior_edge_mask(g)
+    cc = assemble_cc(g)
+    VE = edge_volumes(g)
+    rng = np.random.default_rng(5)
+    e = np.where(mask, rng.standard_normal(g.n_edges) + 1j * rng.standard_normal(g.n_edges), 0)
+    # AdjtBC works on the unsymmetric Maxwell coefficients: its input in the
+    # reference is V_E*e, and (V_E^-1 CC)_IB^T V_E e = CC_BI e
+    got = o.adjt_bc(VE * e)
+    ref = cc[~mask][:, mask] @ e[mask]
+    gb = got[~mask]
+    # edges on face intersections are forced to zero by the reference
+    sel = gb != 0
+    assert sel.sum() > 0.5 * gb.size
+    assert relerr(gb[sel], ref[sel]) < 1e-12
+
+
+def test_transpose_solve_identity(setup):
+    """Stest-style identity (f90/SENS/SymmetryTest.f90:205-272): for the
+    interior system S = A_II^-1, b2^T S b1 = b1^T S^T b2 with S^T from the
+    transposed solve (FWDsolve3D with TRN)."""
+    g, m, o, omega = setup
+    mask = interior_edge_mask(g)
+    VE = o.VE
+    rng = np.random.default_rng(11)
+    # sources on earth edges only: the air part of A_II^-1 is fixed only up to
+    # gradients, which such sources do not see
+    em = mask & earth_mask(g, m)
+    s1 = np.where(em, rng.standard_normal(g.n_edges) + 1j * rng.standard_normal(g.n_edges), 0)
+    s2 = np.where(em, rng.standard_normal(g.n_edges) + 1j * rng.standard_normal(g.n_edges), 0)
+    o.set_control(solver=QMR, precond=PC_DILU, tolEMfwd=1e-9, tolEMadj=1e-9, tolDivCor=1e-8)
+    # forward solve with interior source s1 (b = V_E s1), transposed solve with source V_E s2
+    e1, rc1 = o.fwdsolve(trans=False, src=s1)
+    e2, rc2 = o.fwdsolve(trans=True, src=VE * s2)
+    assert rc1 == 0 and rc2 == 0
+    # transposed solution is V_E-weighted on output (EMsolve3D.f90:356-359)
+    lhs = (VE * s2)[mask] @ e1[mask]
+    rhs = (VE * s1)[mask] @ (e2[mask] / VE[mask])
+    assert abs(lhs - rhs) < 1e-6 * abs(lhs)
+
+
+def test_pmult_t_is_transpose_of_linearised_map(setup):
+    """<dm, PmultT(e0, ea)> = Re sum(ea * (i mu0 w dsigma_E(dm)) * e0): the
+    sigma gradient is the transpose of the linearised ModelParamToEdge
+    (ModelMap.inc:88-188 with m0) scaled by i*omega*mu0 (SolverSens.f90:63-116)."""
+    g, m, o, omega = setup
+    rng = np.random.default_rng(7)
+    e0 = rng.standard_normal((2, g.n_edges)) + 1j * rng.standard_normal((2, g.n_edges))
+    ea = rng.standard_normal((2, g.n_edges)) + 1j * rng.standard_normal((2, g.n_edges))
+    dm = rng.standard_normal(g.nx * g.ny * g.nzEarth)
+    grad = o.pmult_t(e0, ea, m.m_earth)
+    dsig = o.model_to_edge(dm, m.air_cond, m0_earth=m.m_earth)
+    lin = np.real(np.sum(ea * (1j * models.MU_0 * omega * dsig) * e0))
+    assert abs(grad @ dm - lin) < 1e-10 * abs(lin)
+
+
+def test_divcorr_reduces_divergence(setup):
+    g, m, o, omega = setup
+    o.set_control(solver=BICG, precond=PC_JACOBI, tolEMfwd=1e-7)
+    e, rc = o.fwdsolve(bc=mbc.boundary_1d(m, omega, 1))
+    d = o.diagnostics()
+    assert np.all(d["divJ"][:, 1] <= d["divJ"][:, 0])
