@@ -141,6 +141,24 @@ MT3D_API int mt3d_fwdsolve(mt3d_handle h, int trans, const double *bc, const dou
 MT3D_API int mt3d_fwdsolve_batch(mt3d_handle h, int nrhs, const double *omegas, const int *trans, const double *bc,
                         const double *src, double *e, int *status);
 
+/* As mt3d_fwdsolve_batch, with bc, src and e in device memory of the
+ * handle's device (no host copies; for callers that keep the fields resident
+ * in HBM).  bc / src may be NULL. */
+MT3D_API int mt3d_fwdsolve_batch_device(mt3d_handle h, int nrhs, const double *omegas, const int *trans,
+                                        const double *bc_dev, const double *src_dev, double *e_dev, int *status);
+
+/* Run the handle's work on a caller-owned CUDA stream (a cudaStream_t passed
+ * as void*); NULL restores the handle's own stream. */
+MT3D_API int mt3d_set_stream(mt3d_handle h, void *stream);
+
+/* Kernel timing: with enable != 0 every launch of the BiCGStab stencil
+ * kernels (v = A ph with the fused dot product) is bracketed by CUDA events
+ * on the solver stream.  mt3d_kernel_time returns the number of timed
+ * launches and their summed device time in milliseconds since the last
+ * enable, and the precision (0 FP64, 1 FP32) of the last timed launch. */
+MT3D_API int mt3d_profile(mt3d_handle h, int enable);
+MT3D_API int mt3d_kernel_time(mt3d_handle h, int *launches, double *ms, int *precision);
+
 /* Solver diagnostics of the last mt3d_fwdsolve (getEMsolveDiag,
  * f90/3D_MT/FWD/EMsolve3D.f90:866-876): total Krylov iterations, number of
  * divergence corrections, failure flag, the relative residual history
@@ -148,6 +166,11 @@ MT3D_API int mt3d_fwdsolve_batch(mt3d_handle h, int nrhs, const double *omegas, 
  * to lenDivJ pairs) and the relative residual of the returned field. */
 MT3D_API int mt3d_get_diag(mt3d_handle h, int *nIterTotal, int *nDivCor, int *failed, double *EMrelErr, int len,
                   double *divJ, int lenDivJ, double *final_relres);
+
+/* Per right-hand-side diagnostics of the last solve (batched or not): the
+ * total Krylov iterations and the true relative residual ||b - A e|| / ||b||
+ * of each returned interior field; arrays of at least nrhs entries. */
+MT3D_API int mt3d_get_batch_diag(mt3d_handle h, int nrhs, int *niter, double *relres);
 
 /* Gradient with respect to ln(sigma) of the earth cells from background
  * fields e0 and adjoint fields eadj of npol polarisations (npol full edge
@@ -157,6 +180,9 @@ MT3D_API int mt3d_get_diag(mt3d_handle h, int *nIterTotal, int *nDivCor, int *fa
  * values. */
 MT3D_API int mt3d_pmult_t(mt3d_handle h, int npol, const double *e0, const double *eadj, const double *m0_earth,
                  double *dm);
+
+/* Number of kernels the library has launched in this process (all handles). */
+MT3D_API int64_t mt3d_launch_counter(void);
 
 /* Message of the last error on the handle (NUL-terminated, truncated to len). */
 MT3D_API int mt3d_last_error(mt3d_handle h, char *buf, int len);

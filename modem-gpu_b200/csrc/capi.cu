@@ -1,12 +1,17 @@
 // capi.cu -- extern "C" entry points of libmt3d.so (declared in include/mt3d.h).
 // Each call validates its arguments, runs on the handle's device and
 // returns an mt3d_status; exceptions never cross the boundary.
+#include <atomic>
 #include <cstring>
 #include <new>
 #include <string>
 
 #include "../../include/mt3d.h"
 #include "solver.h"
+
+namespace mt3d {
+extern std::atomic<long long> g_launch_count;
+}
 
 struct mt3d_solver {
     mt3d::Solver s;
@@ -176,6 +181,27 @@ int mt3d_fwdsolve_batch(mt3d_handle h, int nrhs, const double *omegas, const int
     return wrap(h, [&] { return h->s.solve(nrhs, omegas, trans, bc, src, e, status); });
 }
 
+int mt3d_fwdsolve_batch_device(mt3d_handle h, int nrhs, const double *omegas, const int *trans, const double *bc_dev,
+                               const double *src_dev, double *e_dev, int *status)
+{
+    return wrap(h, [&] { return h->s.solve(nrhs, omegas, trans, bc_dev, src_dev, e_dev, status, true); });
+}
+
+int mt3d_set_stream(mt3d_handle h, void *stream)
+{
+    return wrap(h, [&] { return h->s.set_stream(stream); });
+}
+
+int mt3d_profile(mt3d_handle h, int enable)
+{
+    return wrap(h, [&] { return h->s.profile(enable); });
+}
+
+int mt3d_kernel_time(mt3d_handle h, int *launches, double *ms, int *precision)
+{
+    return wrap(h, [&] { return h->s.kernel_time(launches, ms, precision); });
+}
+
 int mt3d_get_diag(mt3d_handle h, int *nIterTotal, int *nDivCor, int *failed, double *EMrelErr, int len, double *divJ,
                   int lenDivJ, double *final_relres)
 {
@@ -198,10 +224,23 @@ int mt3d_get_diag(mt3d_handle h, int *nIterTotal, int *nDivCor, int *failed, dou
     return MT3D_OK;
 }
 
+int mt3d_get_batch_diag(mt3d_handle h, int nrhs, int *niter, double *relres)
+{
+    if (!h || nrhs < 0) return MT3D_INVALID_ARGUMENT;
+    const int n = std::min<int>(nrhs, (int)h->s.batch_niter.size());
+    for (int r = 0; r < nrhs; r++) {
+        if (niter) niter[r] = r < n ? h->s.batch_niter[r] : 0;
+        if (relres) relres[r] = r < n ? h->s.batch_relres[r] : 0.0;
+    }
+    return MT3D_OK;
+}
+
 int mt3d_pmult_t(mt3d_handle h, int npol, const double *e0, const double *eadj, const double *m0_earth, double *dm)
 {
     return wrap(h, [&] { return h->s.pmult_t(npol, e0, eadj, m0_earth, dm); });
 }
+
+int64_t mt3d_launch_counter(void) { return mt3d::g_launch_count.load(); }
 
 int mt3d_last_error(mt3d_handle h, char *buf, int len)
 {

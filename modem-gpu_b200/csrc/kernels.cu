@@ -7,10 +7,15 @@
 // and updates the scalars, so an iteration needs no host synchronisation and
 // is bitwise reproducible.  A right-hand side whose state is not RUNNING is
 // skipped by every block.
+#include <atomic>
+
 #include "common.cuh"
 #include "kernels.h"
 
 namespace mt3d {
+
+std::atomic<long long> g_launch_count{0};
+static inline void counted(int n) { g_launch_count.fetch_add(n, std::memory_order_relaxed); }
 
 __device__ __forceinline__ int chunk_begin(int chunk) { return blockIdx.x * chunk + threadIdx.x; }
 
@@ -372,7 +377,7 @@ __global__ void __launch_bounds__(kThreads) kd_rhs(DArgs a)
         double2 b = make_double2(0, 0);
         if (node_interior(g, i, j, k)) {
             double2 d = divc_node(a, a.E + eoff, i, j, k);
-            if (a.phi0) {
+            if (a.phi0 && a.ost[r].has_src) {
                 double2 p0 = a.phi0[off + n];
                 d.x -= p0.x;
                 d.y -= p0.y;
@@ -549,7 +554,7 @@ __global__ void __launch_bounds__(kThreads) kd_divj(DArgs a)
         node_decode(g, n, i, j, k);
         if (!node_interior(g, i, j, k)) continue;
         double2 d = divc_node(a, a.E + eoff, i, j, k);
-        if (a.phi0) {
+        if (a.phi0 && a.ost[r].has_src) {
             d.x -= a.phi0[off + n].x;
             d.y -= a.phi0[off + n].y;
         }
@@ -904,6 +909,18 @@ __global__ void __launch_bounds__(kThreads) k_pmult_t(Geo<double> g, int npol, c
     }
 }
 
+// flags[r] |= 1 when vector r has a non-zero (or NaN) entry
+__global__ void __launch_bounds__(kThreads) k_nonzero(const double2 *v, size_t stride, int n, int *flags)
+{
+    const int r = blockIdx.y;
+    bool nz = false;
+    for (int e = blockIdx.x * kThreads + threadIdx.x; e < n; e += gridDim.x * kThreads) {
+        const double2 a = v[(size_t)r * stride + e];
+        nz = nz || (a.x != 0.0) || (a.y != 0.0);
+    }
+    if (__syncthreads_or(nz) && threadIdx.x == 0) atomicOr(&flags[r], 1);
+}
+
 // ---------------------------------------------------------------------------
 // gather / scatter between interior vectors (EDGEi order) and full vectors
 // ---------------------------------------------------------------------------
@@ -921,58 +938,72 @@ __global__ void __launch_bounds__(kThreads) k_gather_interior(int nEi, const int
 // ---------------------------------------------------------------------------
 template <typename T> void launch_apply(const KArgs<T> &a, const C2<T> *x, C2<T> *y, int neg, int nrhs, cudaStream_t s)
 {
+    counted(1);
     k_apply<T><<<dim3(a.nblk, nrhs), kThreads, 0, s>>>(a, x, y, neg);
 }
 template <typename T> void launch_bicg_init(const KArgs<T> &a, int nrhs, cudaStream_t s)
 {
+    counted(1);
     kb_init<T><<<dim3(a.nblk, nrhs), kThreads, 0, s>>>(a);
 }
-template <typename T> void launch_bicg_iter(const KArgs<T> &a, int nrhs, cudaStream_t s)
+template <typename T> void launch_bicg_iter(const KArgs<T> &a, int nrhs, cudaStream_t s, cudaEvent_t *ev)
 {
+    counted(5);
     dim3 grid(a.nblk, nrhs);
     kb_p<T><<<grid, kThreads, 0, s>>>(a);
+    if (ev) cudaEventRecord(ev[0], s);
     kb_v<T><<<grid, kThreads, 0, s>>>(a);
+    if (ev) cudaEventRecord(ev[1], s);
     kb_s<T><<<grid, kThreads, 0, s>>>(a);
+    if (ev) cudaEventRecord(ev[2], s);
     kb_t<T><<<grid, kThreads, 0, s>>>(a);
+    if (ev) cudaEventRecord(ev[3], s);
     kb_xr<T><<<grid, kThreads, 0, s>>>(a);
 }
 template <typename T> void launch_bicg_finish(const KArgs<T> &a, int nrhs, cudaStream_t s)
 {
+    counted(1);
     kb_finish<T><<<dim3(a.nblk, nrhs), kThreads, 0, s>>>(a);
 }
 template void launch_apply<double>(const KArgs<double> &, const double2 *, double2 *, int, int, cudaStream_t);
 template void launch_apply<float>(const KArgs<float> &, const float2 *, float2 *, int, int, cudaStream_t);
 template void launch_bicg_init<double>(const KArgs<double> &, int, cudaStream_t);
 template void launch_bicg_init<float>(const KArgs<float> &, int, cudaStream_t);
-template void launch_bicg_iter<double>(const KArgs<double> &, int, cudaStream_t);
-template void launch_bicg_iter<float>(const KArgs<float> &, int, cudaStream_t);
+template void launch_bicg_iter<double>(const KArgs<double> &, int, cudaStream_t, cudaEvent_t *);
+template void launch_bicg_iter<float>(const KArgs<float> &, int, cudaStream_t, cudaEvent_t *);
 template void launch_bicg_finish<double>(const KArgs<double> &, int, cudaStream_t);
 template void launch_bicg_finish<float>(const KArgs<float> &, int, cudaStream_t);
 
 void launch_norm_b(const KArgs<double> &a, int nrhs, cudaStream_t s)
 {
+    counted(1);
     k_norm_b<<<dim3(a.nblk, nrhs), kThreads, 0, s>>>(a);
 }
 void launch_res64(const KArgs<double> &a, int nrhs, cudaStream_t s)
 {
+    counted(1);
     km_res64<<<dim3(a.nblk, nrhs), kThreads, 0, s>>>(a, 0.0);
 }
 static int grid_for(long n) { return (int)std::min<long>((n + kThreads - 1) / kThreads, 148L * 16); }
 void launch_cast(const OuterState *ost, int nE, size_t stride, const double2 *r64, float2 *b32, float2 *x32, int nrhs,
                  cudaStream_t s)
 {
+    counted(1);
     km_cast<<<dim3(grid_for(nE), nrhs), kThreads, 0, s>>>(ost, nE, stride, r64, b32, x32);
 }
 void launch_update(const OuterState *ost, int nE, size_t stride, const float2 *d32, double2 *X, int nrhs, cudaStream_t s)
 {
+    counted(1);
     km_update<<<dim3(grid_for(nE), nrhs), kThreads, 0, s>>>(ost, nE, stride, d32, X);
 }
 void launch_divcorr_start(const DArgs &a, int nrhs, cudaStream_t s)
 {
+    counted(1);
     kd_rhs<<<dim3(a.nblk, nrhs), kThreads, 0, s>>>(a);
 }
 void launch_divcorr_iter(const DArgs &a, int nrhs, cudaStream_t s)
 {
+    counted(3);
     dim3 grid(a.nblk, nrhs);
     kd_p<<<grid, kThreads, 0, s>>>(a);
     kd_q<<<grid, kThreads, 0, s>>>(a);
@@ -980,45 +1011,59 @@ void launch_divcorr_iter(const DArgs &a, int nrhs, cudaStream_t s)
 }
 void launch_divcorr_finish(const DArgs &a, int nrhs, cudaStream_t s)
 {
+    counted(2);
     kd_grad<<<dim3(a.enblk, nrhs), kThreads, 0, s>>>(a);
     kd_divj<<<dim3(a.nblk, nrhs), kThreads, 0, s>>>(a);
 }
 void launch_keep_boundary(const Geo<double> &g, double2 *v, size_t stride, int nrhs, cudaStream_t s)
 {
+    counted(1);
     k_keep_boundary<<<dim3(grid_for(g.nE), nrhs), kThreads, 0, s>>>(g, v, stride);
 }
 void launch_keep_interior(const Geo<double> &g, double2 *v, size_t stride, int nrhs, cudaStream_t s)
 {
+    counted(1);
     k_keep_interior<<<dim3(grid_for(g.nE), nrhs), kThreads, 0, s>>>(g, v, stride);
 }
 void launch_add_src(const Geo<double> &g, double2 *b, const double2 *src, size_t stride, const OuterState *ost, int nrhs,
                     cudaStream_t s)
 {
+    counted(1);
     k_add_src<<<dim3(grid_for(g.nE), nrhs), kThreads, 0, s>>>(g, b, src, stride, ost);
 }
 void launch_phi0(const Geo<double> &g, const double2 *src, size_t estride, double2 *phi0, size_t nstride,
                  const OuterState *ost, int nrhs, cudaStream_t s)
 {
+    counted(1);
     k_phi0<<<dim3(grid_for(g.nN), nrhs), kThreads, 0, s>>>(g, src, estride, phi0, nstride, ost);
 }
 void launch_post(const Geo<double> &g, double2 *E, const double2 *bc, size_t stride, const OuterState *ost, int nrhs,
                  cudaStream_t s)
 {
+    counted(2);
     k_post_scale<<<dim3(grid_for(g.nE), nrhs), kThreads, 0, s>>>(g, E, stride, ost);
     k_post_boundary<<<dim3(grid_for(g.nE), nrhs), kThreads, 0, s>>>(g, E, bc, stride, ost);
 }
 void launch_pmult_t(const Geo<double> &g, int npol, const double2 *e0, const double2 *ea, double omega, const double *m0,
                     double *dm, cudaStream_t s)
 {
+    counted(1);
     const int nEarth = g.nx * g.ny * (g.nz - g.nzAir);
     k_pmult_t<<<grid_for(nEarth), kThreads, 0, s>>>(g, npol, e0, ea, omega, m0, dm);
 }
+void launch_nonzero(const double2 *v, size_t stride, int n, int *flags, int nrhs, cudaStream_t s)
+{
+    counted(1);
+    k_nonzero<<<dim3(grid_for(n), nrhs), kThreads, 0, s>>>(v, stride, n, flags);
+}
 void launch_scatter_interior(int nEi, const int *edgei, const double2 *vi, double2 *vf, cudaStream_t s)
 {
+    counted(1);
     k_scatter_interior<<<grid_for(nEi), kThreads, 0, s>>>(nEi, edgei, vi, vf);
 }
 void launch_gather_interior(int nEi, const int *edgei, const double2 *vf, double2 *vi, cudaStream_t s)
 {
+    counted(1);
     k_gather_interior<<<grid_for(nEi), kThreads, 0, s>>>(nEi, edgei, vf, vi);
 }
 

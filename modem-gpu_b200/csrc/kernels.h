@@ -47,7 +47,7 @@ struct DArgs {
 
 template <typename T> void launch_apply(const KArgs<T> &a, const C2<T> *x, C2<T> *y, int neg, int nrhs, cudaStream_t s);
 template <typename T> void launch_bicg_init(const KArgs<T> &a, int nrhs, cudaStream_t s);
-template <typename T> void launch_bicg_iter(const KArgs<T> &a, int nrhs, cudaStream_t s);
+template <typename T> void launch_bicg_iter(const KArgs<T> &a, int nrhs, cudaStream_t s, cudaEvent_t *ev = nullptr);
 template <typename T> void launch_bicg_finish(const KArgs<T> &a, int nrhs, cudaStream_t s);
 void launch_norm_b(const KArgs<double> &a, int nrhs, cudaStream_t s);
 void launch_res64(const KArgs<double> &a, int nrhs, cudaStream_t s);
@@ -67,6 +67,7 @@ void launch_post(const Geo<double> &g, double2 *E, const double2 *bc, size_t str
                  cudaStream_t s);
 void launch_pmult_t(const Geo<double> &g, int npol, const double2 *e0, const double2 *ea, double omega, const double *m0,
                     double *dm, cudaStream_t s);
+void launch_nonzero(const double2 *v, size_t stride, int n, int *flags, int nrhs, cudaStream_t s);
 void launch_scatter_interior(int nEi, const int *edgei, const double2 *vi, double2 *vf, cudaStream_t s);
 void launch_gather_interior(int nEi, const int *edgei, const double2 *vf, double2 *vi, cudaStream_t s);
 

@@ -35,11 +35,66 @@ void DevBuf::release()
 
 Solver::~Solver()
 {
-    if (stream_) {
-        cudaSetDevice(dev_);
-        cudaStreamSynchronize(stream_);
-        cudaStreamDestroy(stream_);
+    cudaSetDevice(dev_);
+    if (stream_) cudaStreamSynchronize(stream_);
+    for (cudaEvent_t e : ev_) cudaEventDestroy(e);
+    if (own_stream_) cudaStreamDestroy(own_stream_);
+}
+
+int Solver::set_stream(void *s)
+{
+    if (stream_) cudaStreamSynchronize(stream_);
+    stream_ = s ? (cudaStream_t)s : own_stream_;
+    return 0;
+}
+
+int Solver::profile(int enable)
+{
+    if (stream_) cudaStreamSynchronize(stream_);
+    prof_ = enable != 0;
+    prof_launches_ = 0;
+    prof_ms_ = 0.0;
+    ev_used_ = 0;
+    return 0;
+}
+
+cudaEvent_t *Solver::next_events(int n)
+{
+    if (!prof_) return nullptr;
+    while (ev_.size() < ev_used_ + n) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) { cudaGetLastError(); return nullptr; }
+        ev_.push_back(e);
     }
+    cudaEvent_t *p = &ev_[ev_used_];
+    ev_used_ += n;
+    return p;
+}
+
+// sum the elapsed time of the recorded (start, stop) pairs; the stream must
+// have been synchronised
+void Solver::collect_events()
+{
+    for (size_t i = 0; i + 1 < ev_used_; i += 2) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, ev_[i], ev_[i + 1]) == cudaSuccess) {
+            prof_ms_ += ms;
+            prof_launches_ += 1;
+        } else {
+            cudaGetLastError();
+        }
+    }
+    ev_used_ = 0;
+}
+
+int Solver::kernel_time(int *launches, double *ms, int *precision)
+{
+    if (stream_) cudaStreamSynchronize(stream_);
+    collect_events();
+    if (launches) *launches = prof_launches_;
+    if (ms) *ms = prof_ms_;
+    if (precision) *precision = prof_prec_;
+    return 0;
 }
 
 int Solver::fail(int code, const std::string &msg)
@@ -97,7 +152,8 @@ int Solver::create(int dev, int nx_, int ny_, int nz_, int nzAir_, const double 
     dev_ = dev;
     int rc;
     if ((rc = check(cudaSetDevice(dev_), "cudaSetDevice"))) return rc;
-    if ((rc = check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate"))) return rc;
+    if ((rc = check(cudaStreamCreateWithFlags(&own_stream_, cudaStreamNonBlocking), "cudaStreamCreate"))) return rc;
+    stream_ = own_stream_;
 
     dx_.assign(dx, dx + nx); dy_.assign(dy, dy + ny); dz_.assign(dz, dz + nz);
     deltas(dx_, delX_); deltas(dy_, delY_); deltas(dz_, delZ_);
@@ -317,7 +373,7 @@ int Solver::ensure_workspace(int nrhs, int precision)
     const int nb = std::max(blocks_for(nE, nrhs, c), blocks_for(nN, nrhs, c));
     err |= w.bst.alloc(nrhs * sizeof(BicgState)) | w.pst.alloc(nrhs * sizeof(PcgState)) |
            w.ost.alloc(nrhs * sizeof(OuterState));
-    err |= w.parts.alloc((size_t)nrhs * nb * kMaxParts * sizeof(double)) | w.cnt.alloc(nrhs * sizeof(unsigned));
+    err |= w.parts.alloc((size_t)nrhs * nb * kMaxParts * sizeof(double)) | w.cnt.alloc(3 * nrhs * sizeof(unsigned));
     err |= w.rerr.alloc((size_t)nrhs * rlen * sizeof(double));
     err |= w.dcrerr.alloc((size_t)nrhs * dlen * sizeof(double));
     if (err) {
@@ -409,17 +465,18 @@ DArgs Solver::dargs(int nrhs)
 
 int Solver::run_bicg(int nrhs, int precision, int maxit)
 {
+    if (prof_) prof_prec_ = precision;
     if (precision == 0) {
         KArgs<double> a = kargs<double>(nrhs, 0);
         a.maxit = maxit;
         launch_bicg_init(a, nrhs, stream_);
-        for (int it = 0; it < maxit; it++) launch_bicg_iter(a, nrhs, stream_);
+        for (int it = 0; it < maxit; it++) launch_bicg_iter(a, nrhs, stream_, next_events(4));
         launch_bicg_finish(a, nrhs, stream_);
     } else {
         KArgs<float> a = kargs<float>(nrhs, 1);
         a.maxit = maxit;
         launch_bicg_init(a, nrhs, stream_);
-        for (int it = 0; it < maxit; it++) launch_bicg_iter(a, nrhs, stream_);
+        for (int it = 0; it < maxit; it++) launch_bicg_iter(a, nrhs, stream_, next_events(4));
         launch_bicg_finish(a, nrhs, stream_);
     }
     return check(cudaGetLastError(), "BiCG launch");
@@ -516,7 +573,7 @@ int Solver::bicg(const double *b, double *x, int maxit, double tol, int *niter, 
 // FWDsolve3D over a batch of right-hand sides
 // ---------------------------------------------------------------------------
 int Solver::solve(int nrhs, const double *omegas, const int *trans, const double *bc, const double *src, double *e,
-                  int *status)
+                  int *status, bool device)
 {
     if (!cond_set) return fail(5, "fwdsolve: conductivity not set (call mt3d_update_cond)");
     if (nrhs < 1 || !omegas || !e) return fail(5, "fwdsolve: invalid arguments");
@@ -527,32 +584,22 @@ int Solver::solve(int nrhs, const double *omegas, const int *trans, const double
     if ((rc = ensure_workspace(nrhs, prec))) return rc;
     Workspace &w = ws_;
     const size_t ebytes = nE * sizeof(double2);
-    // per right-hand side flags
-    std::vector<OuterState> os(nrhs);
-    for (int r = 0; r < nrhs; r++) {
-        OuterState &o = os[r];
-        o = OuterState{};
-        o.omega = omegas[r];
-        o.trans = trans ? (trans[r] != 0) : 0;
-        o.has_bc = 0;
-        o.has_src = 0;
-        if (bc) {
-            const double *v = bc + (size_t)r * nE * 2;
-            for (int64_t q = 0; q < 2 * nE && !o.has_bc; q++) o.has_bc = v[q] != 0.0;
-        }
-        if (src) {
-            const double *v = src + (size_t)r * nE * 2;
-            for (int64_t q = 0; q < 2 * nE && !o.has_src; q++) o.has_src = v[q] != 0.0;
-        }
-        o.tol = o.trans ? ctl.tolEMadj : (o.has_bc ? ctl.tolEMfwd : ctl.tolEMadj);
-        o.active = 1;
-    }
-    cudaMemcpyAsync(w.ost.as<void>(), os.data(), nrhs * sizeof(OuterState), cudaMemcpyHostToDevice, stream_);
+    const cudaMemcpyKind in_kind = device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    const cudaMemcpyKind out_kind = device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    if (prof_) collect_events();
     double2 *B = w.b.as<double2>(), *X = w.X.as<double2>(), *BC = w.bc.as<double2>(), *TMP = w.tmp.as<double2>();
     // boundary data (kept for the post-processing) and initial guess
+    std::vector<OuterState> os(nrhs);
+    for (int r = 0; r < nrhs; r++) {
+        os[r] = OuterState{};
+        os[r].omega = omegas[r];
+        os[r].trans = trans ? (trans[r] != 0) : 0;
+        os[r].active = 1;
+    }
+    cudaMemcpyAsync(w.ost.as<void>(), os.data(), nrhs * sizeof(OuterState), cudaMemcpyHostToDevice, stream_);
     cudaMemsetAsync(BC, 0, nrhs * ebytes, stream_);
-    if (bc) cudaMemcpyAsync(BC, bc, nrhs * ebytes, cudaMemcpyHostToDevice, stream_);
-    cudaMemcpyAsync(X, e, nrhs * ebytes, cudaMemcpyHostToDevice, stream_);
+    if (bc) cudaMemcpyAsync(BC, bc, nrhs * ebytes, in_kind, stream_);
+    cudaMemcpyAsync(X, e, nrhs * ebytes, in_kind, stream_);
     launch_keep_interior(g64_, X, nE, nrhs, stream_);
     // forward right-hand side: b = -V_E A_IB bc (FWDsolve3D, f90/3D_MT/FWD/EMsolve3D.f90:186-200)
     cudaMemcpyAsync(TMP, BC, nrhs * ebytes, cudaMemcpyDeviceToDevice, stream_);
@@ -563,12 +610,30 @@ int Solver::solve(int nrhs, const double *omegas, const int *trans, const double
         KArgs<double> a = kargs<double>(nrhs, 0);
         launch_apply(a, TMP, B, 1, nrhs, stream_);
     }
-    // sources: b += V_E src (forward) or b = src (transposed); phi0
-    bool any_src = false;
-    for (auto &o : os) any_src = any_src || o.has_src;
-    if (any_src) {
-        cudaMemcpyAsync(TMP, src, nrhs * ebytes, cudaMemcpyHostToDevice, stream_);
+    // which right-hand sides carry non-zero boundary data / sources (found on
+    // the device); the sources stay in TMP
+    std::vector<int> flags(2 * nrhs, 0);
+    int *dflags = w.cnt.as<int>() + nrhs;  // scratch after the reduction counters
+    cudaMemsetAsync(dflags, 0, 2 * nrhs * sizeof(int), stream_);
+    launch_nonzero(BC, nE, (int)nE, dflags, nrhs, stream_);
+    if (src) {
+        cudaMemcpyAsync(TMP, src, nrhs * ebytes, in_kind, stream_);
         launch_keep_interior(g64_, TMP, nE, nrhs, stream_);
+        launch_nonzero(TMP, nE, (int)nE, dflags + nrhs, nrhs, stream_);
+    }
+    cudaMemcpyAsync(flags.data(), dflags, 2 * nrhs * sizeof(int), cudaMemcpyDeviceToHost, stream_);
+    if ((rc = sync("fwdsolve input"))) return rc;
+    bool any_src = false;
+    for (int r = 0; r < nrhs; r++) {
+        OuterState &o = os[r];
+        o.has_bc = flags[r] != 0;
+        o.has_src = flags[nrhs + r] != 0;
+        o.tol = o.trans ? ctl.tolEMadj : (o.has_bc ? ctl.tolEMfwd : ctl.tolEMadj);
+        any_src = any_src || o.has_src;
+    }
+    cudaMemcpyAsync(w.ost.as<void>(), os.data(), nrhs * sizeof(OuterState), cudaMemcpyHostToDevice, stream_);
+    // sources: b += V_E src (forward) or b = src (transposed); phi0
+    if (any_src) {
         launch_add_src(g64_, B, TMP, nE, w.ost.as<OuterState>(), nrhs, stream_);
         launch_phi0(g64_, TMP, nE, w.phi0.as<double2>(), nN, w.ost.as<OuterState>(), nrhs, stream_);
     }
@@ -661,6 +726,7 @@ int Solver::solve(int nrhs, const double *omegas, const int *trans, const double
         cudaMemcpyAsync(bs.data(), w.bst.as<void>(), nrhs * sizeof(BicgState), cudaMemcpyDeviceToHost, stream_);
         cudaMemcpyAsync(rerr.data(), w.rerr.as<void>(), rerr.size() * sizeof(double), cudaMemcpyDeviceToHost, stream_);
         if ((rc = sync("fwdsolve Krylov cycle"))) return rc;
+        if (prof_) collect_events();
         for (int r = 0; r < nrhs; r++) {
             OuterState &o = os[r];
             o.dc_run = 0;
@@ -717,8 +783,9 @@ int Solver::solve(int nrhs, const double *omegas, const int *trans, const double
     if ((rc = pull_state())) return rc;
     // post-processing and copy back
     launch_post(g64_, X, BC, nE, w.ost.as<OuterState>(), nrhs, stream_);
-    cudaMemcpyAsync(e, X, nrhs * ebytes, cudaMemcpyDeviceToHost, stream_);
+    cudaMemcpyAsync(e, X, nrhs * ebytes, out_kind, stream_);
     if ((rc = sync("fwdsolve copy back"))) return rc;
+    if (prof_) collect_events();
     int worst = 0;
     for (int r = 0; r < nrhs; r++) {
         OuterState &o = os[r];
@@ -734,6 +801,12 @@ int Solver::solve(int nrhs, const double *omegas, const int *trans, const double
         dg[r].final_relres = o.relres;
     }
     diag = dg[0];
+    batch_niter.assign(nrhs, 0);
+    batch_relres.assign(nrhs, 0.0);
+    for (int r = 0; r < nrhs; r++) {
+        batch_niter[r] = os[r].nIterTotal;
+        batch_relres[r] = os[r].relres;
+    }
     if (worst == 3) return fail(3, "fwdsolve: NaN/Inf in the right-hand side or iterates");
     if (worst == 2) return fail(2, "fwdsolve: BiCGStab breakdown");
     return worst;

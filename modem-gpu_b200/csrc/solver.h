@@ -64,13 +64,18 @@ class Solver {
     int mult_aii(int adjt, const double *x, double *y);
     int bicg(const double *b, double *x, int maxit, double tol, int *niter, double *rerr, int *failed);
     int solve(int nrhs, const double *omegas, const int *trans, const double *bc, const double *src, double *e,
-              int *status);
+              int *status, bool device = false);
+    int set_stream(void *s);
+    int profile(int enable);
+    int kernel_time(int *launches, double *ms, int *precision);
     int pmult_t(int npol, const double *e0, const double *eadj, const double *m0, double *dm);
 
     int fail(int code, const std::string &msg);
     std::string last_error;
     Control ctl;
     Diag diag;
+    std::vector<int> batch_niter;
+    std::vector<double> batch_relres;
     int nx = 0, ny = 0, nz = 0, nzAir = 0;
     int64_t nE = 0, nEi = 0, nN = 0;
     std::vector<int32_t> edgei;  // 0-based interior edge list
@@ -87,7 +92,16 @@ class Solver {
     int sync(const char *what);
 
     int dev_ = 0;
-    cudaStream_t stream_ = nullptr;
+    cudaStream_t stream_ = nullptr;      // active stream (own or caller's)
+    cudaStream_t own_stream_ = nullptr;  // created with the handle
+    // kernel timing: pairs of events around the stencil launches
+    bool prof_ = false;
+    std::vector<cudaEvent_t> ev_;
+    size_t ev_used_ = 0;
+    int prof_launches_ = 0, prof_prec_ = 0;
+    double prof_ms_ = 0.0;
+    cudaEvent_t *next_events(int n);
+    void collect_events();
     Geo<double> g64_{};
     Geo<float> g32_{};
     DevBuf tab64_, tab32_, sig64_, sig32_, coef_, edgei_d_;

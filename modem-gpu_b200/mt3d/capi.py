@@ -24,7 +24,8 @@ PREC_FP64, PREC_MIXED = 0, 1
 #: every symbol include/mt3d.h declares
 EXPORTS = ["mt3d_version", "mt3d_device_count", "mt3d_create", "mt3d_destroy", "mt3d_set_control", "mt3d_update_cond",
            "mt3d_update_freq", "mt3d_sizes", "mt3d_interior_index", "mt3d_mult_aii", "mt3d_bicg", "mt3d_fwdsolve",
-           "mt3d_fwdsolve_batch", "mt3d_get_diag", "mt3d_pmult_t", "mt3d_last_error"]
+           "mt3d_fwdsolve_batch", "mt3d_fwdsolve_batch_device", "mt3d_set_stream", "mt3d_profile",
+           "mt3d_kernel_time", "mt3d_get_diag", "mt3d_get_batch_diag", "mt3d_pmult_t", "mt3d_launch_counter", "mt3d_last_error"]
 
 _lib = None
 
@@ -60,12 +61,19 @@ def load(path: str = LIB_PATH):
     L.mt3d_bicg.argtypes = [P, D, D, I, C.c_double, IP, D, IP]
     L.mt3d_fwdsolve.argtypes = [P, I, D, D, D]
     L.mt3d_fwdsolve_batch.argtypes = [P, I, D, IP, D, D, D, IP]
+    L.mt3d_fwdsolve_batch_device.argtypes = [P, I, D, IP, C.c_void_p, C.c_void_p, C.c_void_p, IP]
+    L.mt3d_set_stream.argtypes = [P, C.c_void_p]
+    L.mt3d_profile.argtypes = [P, I]
+    L.mt3d_kernel_time.argtypes = [P, IP, D, IP]
     L.mt3d_get_diag.argtypes = [P, IP, IP, IP, D, I, D, I, D]
+    L.mt3d_get_batch_diag.argtypes = [P, I, IP, D]
     L.mt3d_pmult_t.argtypes = [P, I, D, D, D, D]
     L.mt3d_last_error.argtypes = [P, C.c_char_p, I]
+    L.mt3d_launch_counter.restype = C.c_int64
+    L.mt3d_launch_counter.argtypes = []
     for name in EXPORTS:
-        getattr(L, name).restype = getattr(L, name).restype or I
-    L.mt3d_version.restype = C.c_char_p
+        if name not in ("mt3d_version", "mt3d_launch_counter"):
+            getattr(L, name).restype = I
     _lib = L
     return L
 
@@ -168,6 +176,30 @@ class Solver:
                          allow=(0, 1, 2, 3))
         return e, st, rc
 
+    def fwdsolve_batch_device(self, omegas, e_ptr, bc_ptr=None, src_ptr=None, trans=None):
+        """Batched solve on device-resident fields: e_ptr, bc_ptr, src_ptr are
+        device addresses (e.g. torch tensor data_ptr()) of nrhs full edge
+        vectors each (complex128)."""
+        omegas = np.ascontiguousarray(omegas, np.float64)
+        n = omegas.size
+        tr = np.zeros(n, np.int32) if trans is None else np.ascontiguousarray(trans, np.int32)
+        st = np.zeros(n, np.int32)
+        rc = self._check(self.L.mt3d_fwdsolve_batch_device(self.h, n, _d(omegas), tr.ctypes.data_as(C.POINTER(C.c_int)),
+                                                           bc_ptr, src_ptr, e_ptr,
+                                                           st.ctypes.data_as(C.POINTER(C.c_int))), allow=(0, 1, 2, 3))
+        return st, rc
+
+    def set_stream(self, stream_handle):
+        self._check(self.L.mt3d_set_stream(self.h, stream_handle))
+
+    def profile(self, enable=True):
+        self._check(self.L.mt3d_profile(self.h, int(enable)))
+
+    def kernel_time(self):
+        n, ms, prec = C.c_int(), C.c_double(), C.c_int()
+        self._check(self.L.mt3d_kernel_time(self.h, C.byref(n), C.byref(ms), C.byref(prec)))
+        return n.value, ms.value, prec.value
+
     def diagnostics(self, maxlen=4000, maxdc=200):
         nit, ndc, fl = C.c_int(), C.c_int(), C.c_int()
         rel = np.zeros(maxlen)
@@ -178,6 +210,12 @@ class Solver:
         return dict(nIterTotal=nit.value, nDivCor=ndc.value, failed=bool(fl.value),
                     EMrelErr=rel[: min(nit.value, maxlen)].copy(), divJ=dj.reshape(-1, 2)[: ndc.value].copy(),
                     final_relres=fr.value)
+
+    def batch_diagnostics(self, nrhs):
+        it = np.zeros(nrhs, np.int32)
+        rr = np.zeros(nrhs)
+        self._check(self.L.mt3d_get_batch_diag(self.h, nrhs, it.ctypes.data_as(C.POINTER(C.c_int)), _d(rr)))
+        return it, rr
 
     def pmult_t(self, e0, eadj, m0_earth):
         e0 = np.ascontiguousarray(e0, np.complex128)

@@ -35,8 +35,8 @@ static const double MU_0 = ORC_PI * 0.0000004;
 static const double SIGMA_AIR = (double)1.0e-10f;
 #define ISIGN (-1)
 
-enum { ORC_QMR = 0, ORC_BICG = 1 };
-enum { ORC_PC_DILU = 0, ORC_PC_JACOBI = 1 };
+enum { ORC_QMR = 0, ORC_BICG = 1, ORC_COCG = 2 };
+enum { ORC_PC_DILU = 0, ORC_PC_JACOBI = 1, ORC_PC_RBDILU = 2, ORC_PC_DILU_SWEEP = 3, ORC_PC_ZLINE = 4 };
 
 typedef struct orc {
     int nx, ny, nz, nzAir;
@@ -58,6 +58,8 @@ typedef struct orc {
     int IterPerDivCor, MaxDivCor, MaxIterDivCor;
     double tolEMfwd, tolEMadj, tolDivCor;
     int solver, precond;
+    int nsweep;      /* Jacobi sweeps per triangular solve (ORC_PC_DILU_SWEEP) */
+    cplx *Drb;       /* 1/D of the red-black ordered D-ILU */
     /* diagnostics (emsolve_diag) */
     int nIterTotal, nDivCor, failed;
     double *EMrelErr;     /* MaxDivCor*IterPerDivCor */
@@ -87,6 +89,7 @@ static void *xcalloc(size_t n, size_t s)
 /* EdgeVolume/NodeVolume/CellVolume (f90/3D_MT/GridCalc.f90:44-200)          */
 /* ------------------------------------------------------------------------ */
 static void curlcurl_setup(orc_t *o);
+static void rbdilu_setup(orc_t *o, int adjt);
 
 orc_t *orc_create(int nx, int ny, int nz, int nzAir, const double *dx, const double *dy, const double *dz)
 {
@@ -183,7 +186,7 @@ void orc_destroy(orc_t *o)
                       o->zZX1, o->zZX2, o->zZY1, o->zZY2, o->zX, o->zY, o->zZO, o->VE, o->VN, o->VC,
                       o->sigE, o->sigC, o->db1, o->db2, o->c, o->d, o->EMrelErr, o->divJ, o->DivCorRelErr};
     for (size_t i = 0; i < sizeof(bufs) / sizeof(bufs[0]); i++) free(bufs[i]);
-    free(o->Adiag); free(o->Dilu); free(o->DivCorIters);
+    free(o->Adiag); free(o->Dilu); free(o->DivCorIters); free(o->Drb);
     free(o);
 }
 
@@ -197,7 +200,9 @@ void orc_set_control(orc_t *o, int IterPerDivCor, int MaxDivCor, int MaxIterDivC
     o->tolEMadj = tolEMadj;
     o->tolDivCor = tolDivCor;
     o->solver = solver;
-    o->precond = precond;
+    o->precond = precond % 16;
+    o->nsweep = precond / 16;
+    if (o->precond == ORC_PC_RBDILU && o->omega > 0) rbdilu_setup(o, 0);
     free(o->EMrelErr); free(o->divJ); free(o->DivCorRelErr); free(o->DivCorIters);
     o->EMrelErr = xcalloc((size_t)MaxDivCor * IterPerDivCor, sizeof(double));
     o->divJ = xcalloc(2 * (size_t)MaxDivCor, sizeof(double));
@@ -636,6 +641,7 @@ void orc_update_freq(orc_t *o, double omega)
                          - o->zZY1[iy] * o->zZY2[iy - 1] * D[IEZ(o, ix, iy - 1, iz)];
                 D[e] = 1.0 / v;
             }
+    if (o->precond == ORC_PC_RBDILU) rbdilu_setup(o, 0);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -797,6 +803,186 @@ static void m2solve(const orc_t *o, const cplx *in, int adjt, cplx *out)
                              - out[IEZ(o, ix, iy - 1, iz)] * o->zZY2[iy - 1] * conj(D[IEZ(o, ix, iy - 1, iz)]);
                 }
     }
+}
+
+/* Plane-wise D-ILU variants used to evaluate GPU-parallel alternatives to the
+ * natural-ordering recurrence of DiluSetUp/M1solve/M2solve.  Each edge
+ * component couples, within the preconditioner, only to its same-component
+ * neighbours in the two transverse directions (5-point structure per plane),
+ * as in the reference.  For a component the helper returns, for interior edge
+ * e, the neighbour indices (-1 if not interior) and the couplings
+ *   lo_a = a(e, e-a) (lower, direction a), up_a = a(e, e+a), lo_b, up_b
+ * and the plane coordinates (pa, pb) used for the colouring. */
+typedef struct { long nb[4]; double cf[4]; int pa, pb; double diagr; } nbrs_t;
+static int edge_nbrs(const orc_t *o, long e, nbrs_t *q)
+{
+    int nx = o->nx, ny = o->ny, nz = o->nz;
+    if (!orc_is_interior_edge(o, e)) return 0;
+    if (e < o->nXe) {
+        int ix = (int)(e % nx) + 1, iy = (int)((e / nx) % (ny + 1)) + 1, iz = (int)(e / ((long)nx * (ny + 1))) + 1;
+        q->pa = iy; q->pb = iz;
+        q->nb[0] = iy > 2 ? IEX(o, ix, iy - 1, iz) : -1; q->cf[0] = o->xXY1[iy];
+        q->nb[1] = iy < ny ? IEX(o, ix, iy + 1, iz) : -1; q->cf[1] = o->xXY2[iy];
+        q->nb[2] = iz > 2 ? IEX(o, ix, iy, iz - 1) : -1; q->cf[2] = o->xXZ1[iz];
+        q->nb[3] = iz < nz ? IEX(o, ix, iy, iz + 1) : -1; q->cf[3] = o->xXZ2[iz];
+        q->diagr = TY(xXO, iy, iz);
+    } else if (e < o->nXe + o->nYe) {
+        long f = e - o->nXe;
+        int ix = (int)(f % (nx + 1)) + 1, iy = (int)((f / (nx + 1)) % ny) + 1, iz = (int)(f / ((long)(nx + 1) * ny)) + 1;
+        q->pa = ix; q->pb = iz;
+        q->nb[0] = ix > 2 ? IEY(o, ix - 1, iy, iz) : -1; q->cf[0] = o->yYX1[ix];
+        q->nb[1] = ix < nx ? IEY(o, ix + 1, iy, iz) : -1; q->cf[1] = o->yYX2[ix];
+        q->nb[2] = iz > 2 ? IEY(o, ix, iy, iz - 1) : -1; q->cf[2] = o->yYZ1[iz];
+        q->nb[3] = iz < nz ? IEY(o, ix, iy, iz + 1) : -1; q->cf[3] = o->yYZ2[iz];
+        q->diagr = TX(yYO, ix, iz);
+    } else {
+        long f = e - o->nXe - o->nYe;
+        int ix = (int)(f % (nx + 1)) + 1, iy = (int)((f / (nx + 1)) % (ny + 1)) + 1, iz = (int)(f / ((long)(nx + 1) * (ny + 1))) + 1;
+        q->pa = ix; q->pb = iy;
+        q->nb[0] = ix > 2 ? IEZ(o, ix - 1, iy, iz) : -1; q->cf[0] = o->zZX1[ix];
+        q->nb[1] = ix < nx ? IEZ(o, ix + 1, iy, iz) : -1; q->cf[1] = o->zZX2[ix];
+        q->nb[2] = iy > 2 ? IEZ(o, ix, iy - 1, iz) : -1; q->cf[2] = o->zZY1[iy];
+        q->nb[3] = iy < ny ? IEZ(o, ix, iy + 1, iz) : -1; q->cf[3] = o->zZY2[iy];
+        q->diagr = TX(zZO, ix, iy);
+    }
+    return 1;
+}
+/* coupling from neighbour k back to e: the transpose entry a(nb, e) */
+static double back_coef(const orc_t *o, long nbidx, int k)
+{
+    nbrs_t r;
+    edge_nbrs(o, nbidx, &r);
+    return r.cf[k ^ 1];  /* lower <-> upper of the same direction */
+}
+static void rbdilu_setup(orc_t *o, int adjt)
+{
+    if (!o->Drb) o->Drb = xcalloc(o->nE, sizeof(cplx));
+    double ds = adjt ? -1.0 * ISIGN : (double)ISIGN;
+    /* red: (pa+pb) even -> D = a_ee; black: D = a_ee - sum a_ej a_je / a_jj */
+    for (long e = 0; e < o->nE; e++) {
+        nbrs_t q;
+        if (!edge_nbrs(o, e, &q)) { o->Drb[e] = 1.0; continue; }
+        cplx aee = q.diagr + ds * o->Adiag[e];
+        if (((q.pa + q.pb) & 1) == 0) { o->Drb[e] = 1.0 / aee; continue; }
+        cplx d = aee;
+        for (int k = 0; k < 4; k++) {
+            if (q.nb[k] < 0) continue;
+            nbrs_t r;
+            edge_nbrs(o, q.nb[k], &r);
+            cplx ajj = r.diagr + ds * o->Adiag[q.nb[k]];
+            d -= q.cf[k] * back_coef(o, q.nb[k], k) / ajj;
+        }
+        o->Drb[e] = 1.0 / d;
+    }
+}
+/* M^-1 v for M = (D+L) D^-1 (D+U) in red-black order, applied to V_E^-1 v */
+static void rbdilu_apply(orc_t *o, const cplx *in, cplx *out)
+{
+    long n = o->nE;
+    cplx *w = xcalloc(n, sizeof(cplx));
+    for (long e = 0; e < n; e++) {
+        nbrs_t q;
+        if (!edge_nbrs(o, e, &q)) continue;
+        if (((q.pa + q.pb) & 1) == 0) w[e] = in[e] / o->VE[e] * o->Drb[e];
+    }
+    for (long e = 0; e < n; e++) {
+        nbrs_t q;
+        if (!edge_nbrs(o, e, &q)) continue;
+        if (((q.pa + q.pb) & 1) == 0) continue;
+        cplx s = in[e] / o->VE[e];
+        for (int k = 0; k < 4; k++) if (q.nb[k] >= 0) s -= q.cf[k] * w[q.nb[k]];
+        w[e] = s * o->Drb[e];
+    }
+    for (long e = 0; e < n; e++) out[e] = 0.0;
+    for (long e = 0; e < n; e++) {
+        nbrs_t q;
+        if (!edge_nbrs(o, e, &q)) continue;
+        if (((q.pa + q.pb) & 1) == 1) { out[e] = w[e]; continue; }
+        cplx s = 0.0;
+        for (int k = 0; k < 4; k++) if (q.nb[k] >= 0) s += q.cf[k] * w[q.nb[k]];
+        out[e] = w[e] - s * o->Drb[e];
+    }
+    free(w);
+}
+/* natural-order D-ILU with each triangular solve replaced by nsweep Jacobi
+ * sweeps on the triangular system (x <- D^-1 (v - L x)) */
+static void dilu_sweep_apply(orc_t *o, const cplx *in, cplx *out)
+{
+    long n = o->nE;
+    cplx *w = xcalloc(n, sizeof(cplx)), *t = xcalloc(n, sizeof(cplx)), *v = xcalloc(n, sizeof(cplx));
+    for (long e = 0; e < n; e++) { nbrs_t q; if (edge_nbrs(o, e, &q)) v[e] = in[e] / o->VE[e]; }
+    for (long e = 0; e < n; e++) w[e] = v[e] * o->Dilu[e];
+    for (int s = 0; s < o->nsweep; s++) {
+        for (long e = 0; e < n; e++) {
+            nbrs_t q;
+            if (!edge_nbrs(o, e, &q)) { t[e] = 0.0; continue; }
+            cplx acc = v[e];
+            if (q.nb[0] >= 0) acc -= q.cf[0] * w[q.nb[0]];
+            if (q.nb[2] >= 0) acc -= q.cf[2] * w[q.nb[2]];
+            t[e] = acc * o->Dilu[e];
+        }
+        memcpy(w, t, n * sizeof(cplx));
+    }
+    /* (I + D^-1 U) x = w */
+    memcpy(out, w, n * sizeof(cplx));
+    for (int s = 0; s < o->nsweep; s++) {
+        for (long e = 0; e < n; e++) {
+            nbrs_t q;
+            if (!edge_nbrs(o, e, &q)) { t[e] = 0.0; continue; }
+            cplx acc = 0.0;
+            if (q.nb[1] >= 0) acc += q.cf[1] * out[q.nb[1]];
+            if (q.nb[3] >= 0) acc += q.cf[3] * out[q.nb[3]];
+            t[e] = w[e] - acc * o->Dilu[e];
+        }
+        memcpy(out, t, n * sizeof(cplx));
+    }
+    free(w); free(t); free(v);
+}
+
+/* z-line block-Jacobi preconditioner: for Ex and Ey an exact tridiagonal
+ * solve along each vertical line of interior edges (the xXZ / yYZ couplings
+ * with the full diagonal), for Ez the diagonal.  M approximates Maxwell;
+ * applied to V_E^-1 v.  Not in the reference: a candidate GPU preconditioner
+ * (independent lines, coalesced across x). */
+static void zline_apply(const orc_t *o, const cplx *in, int adjt, cplx *out)
+{
+    int nx = o->nx, ny = o->ny, nz = o->nz;
+    double ds = adjt ? -1.0 * ISIGN : (double)ISIGN;
+    cplx *cp = xcalloc(nz + 2, sizeof(cplx)), *dp = xcalloc(nz + 2, sizeof(cplx));
+    for (long i = 0; i < o->nE; i++) out[i] = 0.0;
+    for (int comp = 0; comp < 2; comp++) {
+        int ilo = comp == 0 ? 1 : 2, ihi = nx, jlo = comp == 0 ? 2 : 1, jhi = comp == 0 ? ny : ny;
+        for (int iy = jlo; iy <= jhi; iy++)
+            for (int ix = ilo; ix <= ihi; ix++) {
+                /* unknowns iz = 2..nz */
+                for (int iz = 2; iz <= nz; iz++) {
+                    long e = comp == 0 ? IEX(o, ix, iy, iz) : IEY(o, ix, iy, iz);
+                    double lo = comp == 0 ? o->xXZ1[iz] : o->yYZ1[iz];
+                    double up = comp == 0 ? o->xXZ2[iz] : o->yYZ2[iz];
+                    cplx dg = (comp == 0 ? TY(xXO, iy, iz) : TX(yYO, ix, iz)) + ds * o->Adiag[e];
+                    cplx rhs = in[e] / o->VE[e];
+                    if (iz == 2) { cp[iz] = up / dg; dp[iz] = rhs / dg; }
+                    else {
+                        cplx den = dg - lo * cp[iz - 1];
+                        cp[iz] = up / den;
+                        dp[iz] = (rhs - lo * dp[iz - 1]) / den;
+                    }
+                }
+                cplx xn = dp[nz];
+                out[comp == 0 ? IEX(o, ix, iy, nz) : IEY(o, ix, iy, nz)] = xn;
+                for (int iz = nz - 1; iz >= 2; iz--) {
+                    xn = dp[iz] - cp[iz] * xn;
+                    out[comp == 0 ? IEX(o, ix, iy, iz) : IEY(o, ix, iy, iz)] = xn;
+                }
+            }
+    }
+    for (int iz = 1; iz <= nz; iz++)
+        for (int iy = 2; iy <= ny; iy++)
+            for (int ix = 2; ix <= nx; ix++) {
+                long e = IEZ(o, ix, iy, iz);
+                out[e] = in[e] / ((TX(zZO, ix, iy) + ds * o->Adiag[e]) * o->VE[e]);
+            }
+    free(cp); free(dp);
 }
 
 /* Jacobi (diagonal) preconditioner: out = in / diag(V_E * Maxwell) on the
@@ -1010,6 +1196,9 @@ static void pcg(const orc_t *o, const cplx *b, cplx *x, kss_t *it)
 static void precond_L(const orc_t *o, const cplx *in, int adjt, cplx *out)
 {
     if (o->precond == ORC_PC_DILU) m1solve(o, in, adjt, out);
+    else if (o->precond == ORC_PC_RBDILU) rbdilu_apply((orc_t *)o, in, out);
+    else if (o->precond == ORC_PC_DILU_SWEEP) dilu_sweep_apply((orc_t *)o, in, out);
+    else if (o->precond == ORC_PC_ZLINE) zline_apply(o, in, adjt, out);
     else jacobi_apply(o, in, adjt, out);
 }
 static void precond_U(const orc_t *o, const cplx *in, int adjt, cplx *out)
@@ -1191,6 +1380,68 @@ done:
     free(xhalf); free(xmin);
 }
 
+/* Bi-CG for the complex-symmetric system (A^T = A) with the shadow residual
+ * conj(r0), which reduces to the conjugate-orthogonal CG (COCG, van der Vorst &
+ * Melissen 1990): one operator application per iteration; bilinear (not
+ * conjugated) products.  Preconditioned with the (complex-symmetric) diagonal
+ * or D-ILU preconditioner applied as z = M^-1 r.  Returns like bicg(): the
+ * best iterate when not converged. */
+static cplx dotu(const cplx *a, const cplx *b, long n)
+{
+    cplx s = 0.0;
+    for (long i = 0; i < n; i++) s += a[i] * b[i];
+    return s;
+}
+static void cocg(const orc_t *o, const cplx *b, cplx *x, kss_t *it)
+{
+    long n = o->nE;
+    double bnorm = nrm(b, n);
+    if (isnan(bnorm)) { it->failed = 1; it->niter = 0; return; }
+    if (bnorm == 0.0) {
+        memcpy(x, b, n * sizeof(cplx));
+        it->niter = 1; it->failed = 0;
+        for (int i = 0; i < it->maxIt; i++) it->rerr[i] = 0.0;
+        return;
+    }
+    cplx *R = xcalloc(n, sizeof(cplx)), *Z = xcalloc(n, sizeof(cplx)), *P = xcalloc(n, sizeof(cplx));
+    cplx *Q = xcalloc(n, sizeof(cplx)), *T = xcalloc(n, sizeof(cplx)), *xmin = xcalloc(n, sizeof(cplx));
+    multA_N(o, x, 0, R);
+    for (long i = 0; i < n; i++) R[i] = b[i] - R[i];
+    double rnorm = nrm(R, n), btol = it->tol * bnorm, rnormin = rnorm;
+    it->rerr[0] = rnorm / bnorm;
+    memcpy(xmin, x, n * sizeof(cplx));
+    int converged = 0, imin = 0;
+    if (rnorm <= btol) { it->niter = 1; it->failed = 0; goto done; }
+    precond_L(o, R, 0, T);
+    precond_U(o, T, 0, Z);
+    memcpy(P, Z, n * sizeof(cplx));
+    cplx rho = dotu(R, Z, n);
+    for (int iter = 1; iter <= it->maxIt; iter++) {
+        multA_N(o, P, 0, Q);
+        cplx mu = dotu(P, Q, n);
+        if (mu == 0.0 || rho == 0.0) { it->failed = 1; break; }
+        cplx alpha = rho / mu;
+        for (long i = 0; i < n; i++) { x[i] += alpha * P[i]; R[i] -= alpha * Q[i]; }
+        rnorm = nrm(R, n);
+        it->rerr[iter - 1] = rnorm / bnorm;
+        if (rnorm < btol) { it->niter = iter; converged = 1; break; }
+        if (rnorm < rnormin) { rnormin = rnorm; memcpy(xmin, x, n * sizeof(cplx)); imin = iter; }
+        precond_L(o, R, 0, T);
+        precond_U(o, T, 0, Z);
+        cplx rho_new = dotu(R, Z, n);
+        cplx beta = rho_new / rho;
+        rho = rho_new;
+        for (long i = 0; i < n; i++) P[i] = Z[i] + beta * P[i];
+    }
+    if (!converged) {
+        memcpy(x, xmin, n * sizeof(cplx));
+        it->niter = it->maxIt;
+        it->rerr[it->maxIt - 1] = imin > 0 ? it->rerr[imin - 1] : it->rerr[0];
+    }
+done:
+    free(R); free(Z); free(P); free(Q); free(T); free(xmin);
+}
+
 /* ------------------------------------------------------------------------ */
 /* divergence correction and the solve driver                                */
 /* ------------------------------------------------------------------------ */
@@ -1356,6 +1607,7 @@ int orc_fwdsolve(orc_t *o, int trans, const cplx *bc, const cplx *src, cplx *e)
         it.niter = 0; it.failed = 0;
         memset(it.rerr, 0, sizeof(double) * it.maxIt);
         if (o->solver == ORC_QMR) qmr(o, b, e, &it);
+        else if (o->solver == ORC_COCG) cocg(o, b, e, &it);
         else bicg(o, b, e, &it);
         converged = it.niter < it.maxIt;
         failed = failed || it.failed;
@@ -1390,6 +1642,7 @@ int orc_krylov(orc_t *o, const cplx *b, cplx *x, int maxit, double tol, double *
     it.maxIt = maxit; it.tol = tol;
     it.rerr = xcalloc(maxit, sizeof(double));
     if (o->solver == ORC_QMR) qmr(o, b, x, &it);
+    else if (o->solver == ORC_COCG) cocg(o, b, x, &it);
     else bicg(o, b, x, &it);
     if (rerr) memcpy(rerr, it.rerr, sizeof(double) * maxit);
     if (failed) *failed = it.failed;

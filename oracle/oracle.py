@@ -22,7 +22,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "liboracle.so")
 
-QMR, BICG = 0, 1
+QMR, BICG, COCG = 0, 1, 2
 PC_DILU, PC_JACOBI = 0, 1
 
 _lib = None

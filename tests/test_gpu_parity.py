@@ -130,7 +130,7 @@ def test_batch_matches_single(prob):
     modes = [1, 2, 1, 2]
     bcs = np.stack([mbc.boundary_1d(m, w, md) for w, md in zip(oms, modes)])
     for prec in (capi.PREC_FP64, capi.PREC_MIXED):
-        s.set_control(precision=prec)
+        s.set_control(precision=prec, MaxDivCor=100)
         eb, st, rc = s.fwdsolve_batch(oms, bc=bcs)
         assert rc == 0 and np.all(st == 0)
         for r in range(4):
@@ -220,6 +220,7 @@ def test_error_paths(cuda):
     assert ei.value.code == 5
     s.update_freq(1.0)
     bcv = np.zeros(s.nE, complex)
-    bcv[0] = np.nan
+    # Ex(i=1, j=0, k=1): a boundary edge that the interior equations read
+    bcv[1 + g.nx * (g.ny + 1)] = np.nan
     e, rc = s.fwdsolve(bc=bcv)
     assert rc == 3
