@@ -55,7 +55,12 @@ typedef enum {
 } mt3d_status;
 
 /* Krylov solver and precision choices */
-enum { MT3D_SOLVER_BICG = 1 };
+/* MT3D_SOLVER_BICG: BiCGStab as in the reference's BICG with the diagonal
+ * preconditioner.  MT3D_SOLVER_COCG: Bi-CG specialised to the complex-
+ * symmetric operator (conjugate-orthogonal CG, one operator application per
+ * iteration) with the vertical-line (z-line) tridiagonal preconditioner.
+ * MT3D_SOLVER_BICG_ZLINE: BiCGStab with the z-line preconditioner. */
+enum { MT3D_SOLVER_BICG = 1, MT3D_SOLVER_COCG = 2, MT3D_SOLVER_BICG_ZLINE = 3 };
 enum { MT3D_PREC_FP64 = 0, MT3D_PREC_MIXED = 1 };
 
 /* Library version string. */
@@ -84,6 +89,18 @@ MT3D_API int mt3d_destroy(mt3d_handle h);
  * FP32 inner iterations wrapped in FP64 iterative refinement). */
 MT3D_API int mt3d_set_control(mt3d_handle h, int IterPerDivCor, int MaxDivCor, int MaxIterDivCor, double tolEMfwd,
                      double tolEMadj, double tolDivCor, int solver, int precision);
+
+/* Discretised system.  MT3D_FORM_CCDC: the curl-curl operator of the
+ * matrix-free solver (f90/3D_MT/FWD/modelOperator3D.f90) with the divergence
+ * correction SdivCorr every IterPerDivCor iterations (FWDsolve3D of
+ * f90/3D_MT/FWD/EMsolve3D.f90).  MT3D_FORM_CCGD: curl-curl plus the grad-div
+ * term of GradDivSetup2 (f90/3D_MT/FWD_SP2/modelOperator3D.f90:916-1008), no
+ * divergence correction, BiCGStab restarted every 120 iterations and checked
+ * against the true residual (FWDsolve3D + cuBiCG of f90/3D_MT/FWD_SP2); there
+ * IterPerDivCor x MaxDivCor bounds the total iterations.  Both have the same
+ * discrete solution. */
+enum { MT3D_FORM_CCDC = 0, MT3D_FORM_CCGD = 1 };
+MT3D_API int mt3d_set_formulation(mt3d_handle h, int formulation);
 
 /* Set the conductivity model (UpdateCond, f90/3D_MT/FWD/modelOperator3D.f90:
  * 211-232): ModelParamToEdge (LOGE, ModelMap.inc:88-188) and DivCorrSetUp. */

@@ -102,8 +102,8 @@ int mt3d_set_control(mt3d_handle h, int IterPerDivCor, int MaxDivCor, int MaxIte
         h->s.last_error = "mt3d_set_control: iteration counts must be >= 1 and tolerances > 0";
         return MT3D_INVALID_ARGUMENT;
     }
-    if (solver != MT3D_SOLVER_BICG) {
-        h->s.last_error = "mt3d_set_control: only the BICG solver is implemented on the device";
+    if (solver != MT3D_SOLVER_BICG && solver != MT3D_SOLVER_COCG && solver != MT3D_SOLVER_BICG_ZLINE) {
+        h->s.last_error = "mt3d_set_control: unknown solver";
         return MT3D_INVALID_ARGUMENT;
     }
     if (precision != MT3D_PREC_FP64 && precision != MT3D_PREC_MIXED) {
@@ -119,6 +119,17 @@ int mt3d_set_control(mt3d_handle h, int IterPerDivCor, int MaxDivCor, int MaxIte
     c.tolDivCor = tolDivCor;
     c.solver = solver;
     c.precision = precision;
+    return MT3D_OK;
+}
+
+int mt3d_set_formulation(mt3d_handle h, int formulation)
+{
+    if (!h) return MT3D_INVALID_ARGUMENT;
+    if (formulation != MT3D_FORM_CCDC && formulation != MT3D_FORM_CCGD) {
+        h->s.last_error = "mt3d_set_formulation: unknown formulation";
+        return MT3D_INVALID_ARGUMENT;
+    }
+    h->s.ctl.formulation = formulation;
     return MT3D_OK;
 }
 

@@ -24,10 +24,11 @@ template <typename T> __device__ __forceinline__ T dterm_of(const Geo<T> &g, con
     return wmu * sig * edge_volume(g, q);
 }
 
-// ph = v / d, d = V_E*ccdiag + i*dterm (diagonal of A)
-template <typename T> __device__ __forceinline__ C2<T> jacobi(const Geo<T> &g, const EdgeIdx &q, T dterm, C2<T> v)
+// ph = v / d, d = V_E*ccdiag (+ GD_ee) + i*dterm (diagonal of A)
+template <typename T>
+__device__ __forceinline__ C2<T> jacobi(const Geo<T> &g, const EdgeIdx &q, T dterm, C2<T> v, T gdd = T(0))
 {
-    const T dr = cc_diag(g, q), di = dterm;
+    const T dr = cc_diag(g, q) + gdd, di = dterm;
     const T inv = T(1) / (dr * dr + di * di);
     return mk<T>((v.x * dr + v.y * di) * inv, (v.y * dr - v.x * di) * inv);
 }
@@ -38,10 +39,111 @@ template <typename T> __device__ __forceinline__ T rhs_wmu(const KArgs<T> &a, in
 }
 
 // ---------------------------------------------------------------------------
+// grad-div term of the SP2 operator (GradDivSetup2,
+// f90/3D_MT/FWD_SP2/modelOperator3D.f90:916-1008):
+//   GD x = DFA . G phi,  phi_n = w_n sum_e G_en c_en DFA_e x_e
+// with DFA the dual face area of an edge, G the edge-node incidence (-1 at
+// the start node, +1 at the end node), c_en = sigma_e at earth nodes and 1 at
+// air nodes, w_n = 1/(sigma_n V_n) (earth) or 1/V_n (air), 0 on the boundary.
+// ---------------------------------------------------------------------------
+template <typename T> __device__ __forceinline__ T dual_face_area(const Geo<T> &g, const EdgeIdx &q)
+{
+    if (q.c == 0) return g.delY[q.j] * g.delZ[q.k];
+    if (q.c == 1) return g.delX[q.i] * g.delZ[q.k];
+    return g.delX[q.i] * g.delY[q.j];
+}
+template <typename T> __device__ __forceinline__ void edge_nodes(const Geo<T> &g, const EdgeIdx &q, int &ns, int &ne)
+{
+    ns = iN(g, q.i, q.j, q.k);
+    ne = q.c == 0 ? iN(g, q.i + 1, q.j, q.k) : q.c == 1 ? iN(g, q.i, q.j + 1, q.k) : iN(g, q.i, q.j, q.k + 1);
+}
+// (GD x)_e from the node potentials phi of x
+template <typename T>
+__device__ __forceinline__ C2<T> gd_edge(const Geo<T> &g, const EdgeIdx &q, const C2<T> *__restrict__ phi)
+{
+    int ns, ne;
+    edge_nodes(g, q, ns, ne);
+    return cscale(csub(phi[ne], phi[ns]), dual_face_area(g, q));
+}
+// GD_ee (diagonal of the grad-div term)
+template <typename T>
+__device__ __forceinline__ T gd_diag(const KArgs<T> &a, const EdgeIdx &q, T sig_e)
+{
+    int ns, ne;
+    edge_nodes(a.g, q, ns, ne);
+    const T dfa = dual_face_area(a.g, q);
+    const T cs = a.gde[ns] ? sig_e : T(1), ce = a.gde[ne] ? sig_e : T(1);
+    return dfa * dfa * (a.gdw[ns] * cs + a.gdw[ne] * ce);
+}
+
+// phi = W G^T (C DFA x) on interior nodes (mode 0: operator; mode 1: the
+// source-correction operator V_E GD2 of GradDivSetup2, earth nodes only and
+// c = 1).  For mode 1 the input is the source scaled per right-hand side by
+// 1 / (i ISIGN omega mu0), divided by V_E for transposed problems.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_gd_phi(KArgs<T> a, const C2<T> *x, C2<T> *phi, int mode)
+{
+    const int r = blockIdx.y;
+    if (!a.ost[r].active && mode == 0) return;
+    const Geo<T> &g = a.g;
+    const size_t eo = (size_t)r * a.stride, no = (size_t)r * g.nN;
+    C2<T> scl = mk<T>(1, 0);
+    bool dv = false;
+    if (mode == 1) {
+        if (!a.ost[r].has_src) return;
+        // 1/(i*ISIGN*omega*mu0) = i/(omega*mu0) for ISIGN = -1
+        scl = mk<T>(0, (T)(1.0 / (a.ost[r].omega * kMu0)));
+        dv = a.ost[r].trans != 0;
+    }
+    for (int n = blockIdx.x * kThreads + threadIdx.x; n < g.nN; n += gridDim.x * kThreads) {
+        const int i = n % (g.nx + 1), t = n / (g.nx + 1), j = t % (g.ny + 1), k = t / (g.ny + 1);
+        C2<T> out = mk<T>(0, 0);
+        const bool earth = a.gde[n];
+        if (i >= 1 && i <= g.nx - 1 && j >= 1 && j <= g.ny - 1 && k >= 1 && k <= g.nz - 1 && (mode == 0 || earth)) {
+            const int e[6] = {iX(g, i - 1, j, k), iX(g, i, j, k), iY(g, i, j - 1, k),
+                              iY(g, i, j, k), iZ(g, i, j, k - 1), iZ(g, i, j, k)};
+            const T dfa[3] = {g.delY[j] * g.delZ[k], g.delX[i] * g.delZ[k], g.delX[i] * g.delY[j]};
+            C2<T> acc = mk<T>(0, 0);
+#pragma unroll
+            for (int q = 0; q < 6; q++) {
+                C2<T> v = x[eo + e[q]];
+                T c = dfa[q >> 1];
+                if (mode == 0 && earth) c *= a.sigma[e[q]];
+                if (dv) {
+                    const EdgeIdx qq = {q >> 1, (q == 0) ? i - 1 : i, (q == 2) ? j - 1 : j, (q == 4) ? k - 1 : k};
+                    c /= edge_volume(g, qq);
+                }
+                v = cscale(v, c);
+                acc = (q & 1) ? csub(acc, v) : cadd(acc, v);  // end node of the first, start of the second
+            }
+            out = cscale(acc, a.gdw[n]);
+            if (mode == 1) out = cmul(out, scl);
+        }
+        phi[no + n] = out;
+    }
+}
+
+// b += DFA G phi on interior edges (source correction of the SP2 right-hand side)
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_gd_add(KArgs<T> a, C2<T> *b, const C2<T> *phi)
+{
+    const int r = blockIdx.y;
+    if (!a.ost[r].has_src) return;
+    const Geo<T> &g = a.g;
+    const size_t eo = (size_t)r * a.stride, no = (size_t)r * g.nN;
+    for (int e = blockIdx.x * kThreads + threadIdx.x; e < g.nE; e += gridDim.x * kThreads) {
+        EdgeIdx q = edge_decode(g, e);
+        if (!edge_interior(g, q)) continue;
+        b[eo + e] = cadd(b[eo + e], gd_edge(g, q, phi + no));
+    }
+}
+
+// ---------------------------------------------------------------------------
 // operator apply: y = A x (interior; boundary of y set to zero).  Optional
 // mode 1: y = b - A x with reduction of |y|^2 into parts (no finalisation).
 // ---------------------------------------------------------------------------
-template <typename T> __global__ void __launch_bounds__(kThreads) k_apply(KArgs<T> a, const C2<T> *x, C2<T> *y, int neg)
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_apply(KArgs<T> a, const C2<T> *x, C2<T> *y, int neg, int use_gd)
 {
     const int r = blockIdx.y;
     const size_t off = (size_t)r * a.stride;
@@ -53,6 +155,7 @@ template <typename T> __global__ void __launch_bounds__(kThreads) k_apply(KArgs<
         C2<T> out = mk<T>(0, 0);
         if (edge_interior(g, q)) {
             out = stencil(g, x + off, q, dterm_of(g, q, wmu, a.sigma[e]));
+            if (use_gd) out = cadd(out, gd_edge(g, q, a.phi + (size_t)r * g.nN));
             if (neg) { out.x = -out.x; out.y = -out.y; }
         }
         y[off + e] = out;
@@ -81,6 +184,7 @@ template <typename T> __global__ void __launch_bounds__(kThreads) kb_init(KArgs<
         C2<T> res = mk<T>(0, 0);
         if (edge_interior(g, q)) {
             C2<T> ax = stencil(g, x, q, dterm_of(g, q, wmu, a.sigma[e]));
+            if (a.gd) ax = cadd(ax, gd_edge(g, q, a.phi + (size_t)r * g.nN));
             C2<T> bb = a.b[off + e];
             res = csub(bb, ax);
             v[0] += (double)bb.x * bb.x + (double)bb.y * bb.y;
@@ -99,6 +203,7 @@ template <typename T> __global__ void __launch_bounds__(kThreads) kb_init(KArgs<
         st.xbest = 0;
         st.imin = 0;
         st.first = 1;
+        st.pad = 0;
         st.bnorm = bnorm;
         st.rnorm = rnorm;
         st.rnormin = rnorm;
@@ -135,7 +240,7 @@ template <typename T> __global__ void __launch_bounds__(kThreads) kb_p(KArgs<T> 
     const size_t off = (size_t)r * a.stride;
     const Geo<T> &g = a.g;
     const T wmu = rhs_wmu(a, r);
-    const bool first = st.first;
+    const bool first = st.first, reset_rt = st.first && st.pad;
     const C2<T> beta = mk<T>((T)st.beta.re, (T)st.beta.im);
     const C2<T> om = mk<T>((T)st.omega.re, (T)st.omega.im);
     const int end = min((blockIdx.x + 1) * a.chunk, g.nE);
@@ -144,14 +249,19 @@ template <typename T> __global__ void __launch_bounds__(kThreads) kb_p(KArgs<T> 
         C2<T> p;
         if (first) {
             p = rr;
+            if (reset_rt) a.rt[off + e] = rr;
         } else {
             C2<T> pv = csub(a.p[off + e], cmul(om, a.v[off + e]));
             p = cadd(rr, cmul(beta, pv));
         }
         a.p[off + e] = p;
+        if (a.pc_ext) continue;
         EdgeIdx q = edge_decode(g, e);
         C2<T> ph = mk<T>(0, 0);
-        if (edge_interior(g, q)) ph = jacobi(g, q, dterm_of(g, q, wmu, a.sigma[e]), p);
+        if (edge_interior(g, q)) {
+            const T sg = a.sigma[e];
+            ph = jacobi(g, q, dterm_of(g, q, wmu, sg), p, a.gd ? gd_diag(a, q, sg) : T(0));
+        }
         a.ph[off + e] = ph;
     }
 }
@@ -172,6 +282,7 @@ template <typename T> __global__ void __launch_bounds__(kThreads) kb_v(KArgs<T> 
         C2<T> out = mk<T>(0, 0);
         if (edge_interior(g, q)) {
             out = stencil(g, a.ph + off, q, dterm_of(g, q, wmu, a.sigma[e]));
+            if (a.gd) out = cadd(out, gd_edge(g, q, a.phi + (size_t)r * g.nN));
             C2<T> t = a.rt[off + e];
             v[0] += (double)t.x * out.x + (double)t.y * out.y;  // conj(rt)*v
             v[1] += (double)t.x * out.y - (double)t.y * out.x;
@@ -202,9 +313,13 @@ template <typename T> __global__ void __launch_bounds__(kThreads) kb_s(KArgs<T> 
     for (int e = chunk_begin(a.chunk); e < end; e += kThreads) {
         C2<T> s = csub(a.r[off + e], cmul(al, a.v[off + e]));
         a.s[off + e] = s;
+        if (a.pc_ext) continue;
         EdgeIdx q = edge_decode(g, e);
         C2<T> sh = mk<T>(0, 0);
-        if (edge_interior(g, q)) sh = jacobi(g, q, dterm_of(g, q, wmu, a.sigma[e]), s);
+        if (edge_interior(g, q)) {
+            const T sg = a.sigma[e];
+            sh = jacobi(g, q, dterm_of(g, q, wmu, sg), s, a.gd ? gd_diag(a, q, sg) : T(0));
+        }
         a.sh[off + e] = sh;
     }
 }
@@ -225,6 +340,7 @@ template <typename T> __global__ void __launch_bounds__(kThreads) kb_t(KArgs<T> 
         C2<T> out = mk<T>(0, 0);
         if (edge_interior(g, q)) {
             out = stencil(g, a.sh + off, q, dterm_of(g, q, wmu, a.sigma[e]));
+            if (a.gd) out = cadd(out, gd_edge(g, q, a.phi + (size_t)r * g.nN));
             C2<T> s = a.s[off + e];
             v[0] += (double)out.x * s.x + (double)out.y * s.y;  // conj(t)*s
             v[1] += (double)out.x * s.y - (double)out.y * s.x;
@@ -276,6 +392,7 @@ template <typename T> __global__ void __launch_bounds__(kThreads) kb_xr(KArgs<T>
         st.iter += 1;
         st.xcur = dst;
         st.first = 0;
+        st.pad = 0;
         st.rnorm = rnorm;
         rerr[st.iter - 1] = rnorm / st.bnorm;
         if (!isfinite(rnorm)) { st.status = KS_NAN; return; }
@@ -291,6 +408,15 @@ template <typename T> __global__ void __launch_bounds__(kThreads) kb_xr(KArgs<T>
         }
         if (st.iter >= st.maxit) {
             st.status = KS_MAXIT;
+            return;
+        }
+        if (a.restart > 0 && st.iter % a.restart == 0) {
+            // restart towards steepest descent (cuBiCG, f90/3D_MT/FWD_SP2/solver.f90:1545-1573):
+            // rt = r, rho = rt . r, p = r, omega = 1
+            st.first = 1;
+            st.pad = 1;
+            st.rho = {tot[0], 0.0};
+            st.omega = {1.0, 0.0};
             return;
         }
         cd rho_new = {tot[1], tot[2]};
@@ -667,7 +793,9 @@ __global__ void __launch_bounds__(kThreads) km_res64(KArgs<double> a, double tol
         EdgeIdx q = edge_decode(g, e);
         double2 res = make_double2(0, 0);
         if (edge_interior(g, q)) {
-            res = csub(a.b[off + e], stencil(g, a.x0 + off, q, dterm_of(g, q, wmu, a.sigma[e])));
+            double2 ax = stencil(g, a.x0 + off, q, dterm_of(g, q, wmu, a.sigma[e]));
+            if (a.gd) ax = cadd(ax, gd_edge(g, q, a.phi + (size_t)r * g.nN));
+            res = csub(a.b[off + e], ax);
             v[0] += res.x * res.x + res.y * res.y;
         }
         a.r[off + e] = res;
@@ -936,25 +1064,48 @@ __global__ void __launch_bounds__(kThreads) k_gather_interior(int nEi, const int
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
-template <typename T> void launch_apply(const KArgs<T> &a, const C2<T> *x, C2<T> *y, int neg, int nrhs, cudaStream_t s)
+template <typename T>
+void launch_apply(const KArgs<T> &a, const C2<T> *x, C2<T> *y, int neg, int nrhs, cudaStream_t s, int use_gd)
 {
     counted(1);
-    k_apply<T><<<dim3(a.nblk, nrhs), kThreads, 0, s>>>(a, x, y, neg);
+    if (use_gd) launch_gd_phi(a, x, a.phi, 0, nrhs, s);
+    k_apply<T><<<dim3(a.nblk, nrhs), kThreads, 0, s>>>(a, x, y, neg, use_gd);
 }
+template <typename T> void launch_gd_phi(const KArgs<T> &a, const C2<T> *x, C2<T> *phi, int mode, int nrhs, cudaStream_t s)
+{
+    counted(1);
+    const int gn = (int)std::min<long>((a.g.nN + kThreads - 1) / kThreads, 148L * 16);
+    k_gd_phi<T><<<dim3(gn, nrhs), kThreads, 0, s>>>(a, x, phi, mode);
+}
+template <typename T> void launch_gd_add(const KArgs<T> &a, C2<T> *b, const C2<T> *phi, int nrhs, cudaStream_t s)
+{
+    counted(1);
+    const int ge = (int)std::min<long>((a.g.nE + kThreads - 1) / kThreads, 148L * 16);
+    k_gd_add<T><<<dim3(ge, nrhs), kThreads, 0, s>>>(a, b, phi);
+}
+template void launch_gd_phi<double>(const KArgs<double> &, const double2 *, double2 *, int, int, cudaStream_t);
+template void launch_gd_phi<float>(const KArgs<float> &, const float2 *, float2 *, int, int, cudaStream_t);
+template void launch_gd_add<double>(const KArgs<double> &, double2 *, const double2 *, int, cudaStream_t);
 template <typename T> void launch_bicg_init(const KArgs<T> &a, int nrhs, cudaStream_t s)
 {
     counted(1);
+    if (a.gd) launch_gd_phi(a, a.x0, a.phi, 0, nrhs, s);
     kb_init<T><<<dim3(a.nblk, nrhs), kThreads, 0, s>>>(a);
 }
-template <typename T> void launch_bicg_iter(const KArgs<T> &a, int nrhs, cudaStream_t s, cudaEvent_t *ev)
+template <typename T>
+void launch_bicg_iter(const KArgs<T> &a, int nrhs, cudaStream_t s, cudaEvent_t *ev, const ColArgs<T> *pc)
 {
     counted(5);
     dim3 grid(a.nblk, nrhs);
     kb_p<T><<<grid, kThreads, 0, s>>>(a);
+    if (pc) launch_col_prec(*pc, a.p, a.ph, nrhs, s);
+    if (a.gd) launch_gd_phi(a, a.ph, a.phi, 0, nrhs, s);
     if (ev) cudaEventRecord(ev[0], s);
     kb_v<T><<<grid, kThreads, 0, s>>>(a);
     if (ev) cudaEventRecord(ev[1], s);
     kb_s<T><<<grid, kThreads, 0, s>>>(a);
+    if (pc) launch_col_prec(*pc, a.s, a.sh, nrhs, s);
+    if (a.gd) launch_gd_phi(a, a.sh, a.phi, 0, nrhs, s);
     if (ev) cudaEventRecord(ev[2], s);
     kb_t<T><<<grid, kThreads, 0, s>>>(a);
     if (ev) cudaEventRecord(ev[3], s);
@@ -965,12 +1116,12 @@ template <typename T> void launch_bicg_finish(const KArgs<T> &a, int nrhs, cudaS
     counted(1);
     kb_finish<T><<<dim3(a.nblk, nrhs), kThreads, 0, s>>>(a);
 }
-template void launch_apply<double>(const KArgs<double> &, const double2 *, double2 *, int, int, cudaStream_t);
-template void launch_apply<float>(const KArgs<float> &, const float2 *, float2 *, int, int, cudaStream_t);
+template void launch_apply<double>(const KArgs<double> &, const double2 *, double2 *, int, int, cudaStream_t, int);
+template void launch_apply<float>(const KArgs<float> &, const float2 *, float2 *, int, int, cudaStream_t, int);
 template void launch_bicg_init<double>(const KArgs<double> &, int, cudaStream_t);
 template void launch_bicg_init<float>(const KArgs<float> &, int, cudaStream_t);
-template void launch_bicg_iter<double>(const KArgs<double> &, int, cudaStream_t, cudaEvent_t *);
-template void launch_bicg_iter<float>(const KArgs<float> &, int, cudaStream_t, cudaEvent_t *);
+template void launch_bicg_iter<double>(const KArgs<double> &, int, cudaStream_t, cudaEvent_t *, const ColArgs<double> *);
+template void launch_bicg_iter<float>(const KArgs<float> &, int, cudaStream_t, cudaEvent_t *, const ColArgs<float> *);
 template void launch_bicg_finish<double>(const KArgs<double> &, int, cudaStream_t);
 template void launch_bicg_finish<float>(const KArgs<float> &, int, cudaStream_t);
 
@@ -982,6 +1133,7 @@ void launch_norm_b(const KArgs<double> &a, int nrhs, cudaStream_t s)
 void launch_res64(const KArgs<double> &a, int nrhs, cudaStream_t s)
 {
     counted(1);
+    if (a.gd) launch_gd_phi(a, a.x0, a.phi, 0, nrhs, s);
     km_res64<<<dim3(a.nblk, nrhs), kThreads, 0, s>>>(a, 0.0);
 }
 static int grid_for(long n) { return (int)std::min<long>((n + kThreads - 1) / kThreads, 148L * 16); }

@@ -20,6 +20,14 @@ template <typename T> struct KArgs {
     int chunk, nblk;
     int maxit;
     int inner;    // 1: tolerance from OuterState::tol_inner (mixed inner solve)
+    int pc_ext;   // 1: ph / sh come from an external preconditioner kernel
+    int restart;  // restart BiCGStab every `restart` iterations (0: never)
+    // grad-div term (SP2 formulation): gd != 0 adds DFA G phi, phi computed by
+    // launch_gd_phi from the stencil input; gdw / gde node weights and flags
+    int gd;
+    const T *gdw;
+    const unsigned char *gde;
+    C2<T> *phi;
     double dsgn;  // ISIGN (-1) for A, +1 for the conjugate transpose
 };
 
@@ -45,10 +53,43 @@ struct DArgs {
     double tol;
 };
 
-template <typename T> void launch_apply(const KArgs<T> &a, const C2<T> *x, C2<T> *y, int neg, int nrhs, cudaStream_t s);
+// column-marching kernels (colkernels.cu)
+struct ColMap {
+    int tiles_x, tiles;  // tiles of kColX x kColY columns
+};
+using ColMapHost = ColMap;
+ColMapHost col_map(int nx, int ny);
+
+template <typename T> struct ColArgs {
+    Geo<T> g;
+    const T *sigma;
+    OuterState *ost;
+    BicgState *st;
+    ColMap map;
+    C2<T> *r, *z, *p, *q, *x0, *x1;
+    C2<T> *zm, *zc;  // z-line pivots m_k and c'_k (per right-hand side)
+    double *parts;
+    unsigned *cnt;
+    double *rerr;
+    int rerr_stride;
+    size_t stride;
+    double dsgn;
+};
+template <typename T> void launch_col_apply(const ColArgs<T> &a, const C2<T> *x, C2<T> *y, int neg, int nrhs,
+                                            cudaStream_t s);
+template <typename T> void launch_zl_setup(const ColArgs<T> &a, int nrhs, cudaStream_t s);
+template <typename T> void launch_cocg_start(const ColArgs<T> &a, int nrhs, cudaStream_t s);
+template <typename T> void launch_col_prec(const ColArgs<T> &a, const C2<T> *in, C2<T> *out, int nrhs, cudaStream_t s);
+template <typename T> void launch_cocg_iter(const ColArgs<T> &a, int nrhs, cudaStream_t s, cudaEvent_t *ev = nullptr);
+
+template <typename T>
+void launch_apply(const KArgs<T> &a, const C2<T> *x, C2<T> *y, int neg, int nrhs, cudaStream_t s, int use_gd = 0);
 template <typename T> void launch_bicg_init(const KArgs<T> &a, int nrhs, cudaStream_t s);
-template <typename T> void launch_bicg_iter(const KArgs<T> &a, int nrhs, cudaStream_t s, cudaEvent_t *ev = nullptr);
+template <typename T> void launch_bicg_iter(const KArgs<T> &a, int nrhs, cudaStream_t s, cudaEvent_t *ev = nullptr,
+                                            const ColArgs<T> *pc = nullptr);
 template <typename T> void launch_bicg_finish(const KArgs<T> &a, int nrhs, cudaStream_t s);
+template <typename T> void launch_gd_phi(const KArgs<T> &a, const C2<T> *x, C2<T> *phi, int mode, int nrhs, cudaStream_t s);
+template <typename T> void launch_gd_add(const KArgs<T> &a, C2<T> *b, const C2<T> *phi, int nrhs, cudaStream_t s);
 void launch_norm_b(const KArgs<double> &a, int nrhs, cudaStream_t s);
 void launch_res64(const KArgs<double> &a, int nrhs, cudaStream_t s);
 void launch_cast(const OuterState *ost, int nE, size_t stride, const double2 *r64, float2 *b32, float2 *x32, int nrhs,

@@ -261,6 +261,45 @@ int Solver::update_cond(const double *m_earth, double airCond)
     for (int k = 0; k < nz; k++)
         for (int j = 0; j <= ny; j++)
             for (int i = 0; i <= nx; i++) sig[nX + nY + i + (nx + 1) * (j + (int64_t)(ny + 1) * k)] = avg(2, i, j, k);
+    // SP2 (grad-div) data: edge conductivity with the air at exp(airCond) and
+    // the boundary edges zero (UpdateCond, f90/3D_MT/FWD_SP2/modelOperator3D.f90:
+    // 176-230), node conductivity (ModelParamToNode) and the node weights of
+    // GradDivSetup2 with airNIndex (:916-1008, 1086-1130)
+    std::vector<double> sig_sp2(sig);
+    auto is_int = [&](int64_t e) -> bool {
+        if (e < nX) { int64_t t = e / nx; int j = (int)(t % (ny + 1)), k = (int)(t / (ny + 1)); return j >= 1 && j <= ny - 1 && k >= 1 && k <= nz - 1; }
+        if (e < nX + nY) { int64_t f = e - nX; int i = (int)(f % (nx + 1)), k = (int)(f / ((int64_t)(nx + 1) * ny)); return i >= 1 && i <= nx - 1 && k >= 1 && k <= nz - 1; }
+        int64_t f = e - nX - nY; int i = (int)(f % (nx + 1)), j = (int)((f / (nx + 1)) % (ny + 1)); return i >= 1 && i <= nx - 1 && j >= 1 && j <= ny - 1;
+    };
+    for (int64_t e = 0; e < nE; e++) if (!is_int(e)) sig_sp2[e] = 0.0;
+    std::vector<double> gdw(nN, 0.0);
+    std::vector<unsigned char> gde(nN, 0);
+    {
+        auto ndx = [&](int i, int j, int k) { return (int64_t)i + (nx + 1) * (j + (int64_t)(ny + 1) * k); };
+        auto exi = [&](int i, int j, int k) { return (int64_t)i + nx * (j + (int64_t)(ny + 1) * k); };
+        auto eyi = [&](int i, int j, int k) { return nX + i + (nx + 1) * (j + (int64_t)ny * k); };
+        auto ezi = [&](int i, int j, int k) { return nX + nY + i + (nx + 1) * (j + (int64_t)(ny + 1) * k); };
+        const double thr = 1.1 * kSigmaAir;
+        for (int k = 1; k < nz; k++)
+            for (int j = 1; j < ny; j++)
+                for (int i = 1; i < nx; i++) {
+                    const int64_t inc[6] = {exi(i - 1, j, k), exi(i, j, k), eyi(i, j - 1, k), eyi(i, j, k),
+                                            ezi(i, j, k - 1), ezi(i, j, k)};
+                    bool earth = false;
+                    for (int q = 0; q < 6; q++) earth = earth || sig_sp2[inc[q]] >= thr;
+                    // node conductivity: volume-weighted mean of the 8 cells around the node
+                    double num = 0.0, den = 0.0;
+                    for (int c = 0; c < 8; c++) {
+                        const int ci = i - 1 + (c & 1), cj = j - 1 + ((c >> 1) & 1), ck = k - 1 + ((c >> 2) & 1);
+                        num += CT[cl(ci, cj, ck)];
+                        den += VC[cl(ci, cj, ck)];
+                    }
+                    const double vn = delX_[i] * delY_[j] * delZ_[k];
+                    const int64_t n = ndx(i, j, k);
+                    gde[n] = earth ? 1 : 0;
+                    gdw[n] = earth ? 1.0 / ((num / den) * vn) : 1.0 / vn;
+                }
+    }
     auto ex = [&](int i, int j, int k) { return (int64_t)i + nx * (j + (int64_t)(ny + 1) * k); };
     auto ey = [&](int i, int j, int k) { return nX + i + (nx + 1) * (j + (int64_t)ny * k); };
     auto ez = [&](int i, int j, int k) { return nX + nY + i + (nx + 1) * (j + (int64_t)(ny + 1) * k); };
@@ -309,9 +348,17 @@ int Solver::update_cond(const double *m_earth, double airCond)
                 if (k == nz - 1) db2z[n] = 0.0;
             }
     std::vector<float> sigf(sig.begin(), sig.end());
+    std::vector<float> sigsf(sig_sp2.begin(), sig_sp2.end()), gdwf(gdw.begin(), gdw.end());
     int rc;
-    if (sig64_.alloc(nE * sizeof(double)) || sig32_.alloc(nE * sizeof(float)) || coef_.alloc(coef.size() * sizeof(double)))
+    if (sig64_.alloc(nE * sizeof(double)) || sig32_.alloc(nE * sizeof(float)) || coef_.alloc(coef.size() * sizeof(double)) ||
+        sigs64_.alloc(nE * sizeof(double)) || sigs32_.alloc(nE * sizeof(float)) || gdw64_.alloc(nN * sizeof(double)) ||
+        gdw32_.alloc(nN * sizeof(float)) || gde_.alloc(nN))
         return fail(8, "mt3d_update_cond: out of device memory");
+    cudaMemcpyAsync(sigs64_.as<void>(), sig_sp2.data(), nE * sizeof(double), cudaMemcpyHostToDevice, stream_);
+    cudaMemcpyAsync(sigs32_.as<void>(), sigsf.data(), nE * sizeof(float), cudaMemcpyHostToDevice, stream_);
+    cudaMemcpyAsync(gdw64_.as<void>(), gdw.data(), nN * sizeof(double), cudaMemcpyHostToDevice, stream_);
+    cudaMemcpyAsync(gdw32_.as<void>(), gdwf.data(), nN * sizeof(float), cudaMemcpyHostToDevice, stream_);
+    cudaMemcpyAsync(gde_.as<void>(), gde.data(), nN, cudaMemcpyHostToDevice, stream_);
     if ((rc = check(cudaMemcpyAsync(sig64_.as<void>(), sig.data(), nE * sizeof(double), cudaMemcpyHostToDevice, stream_), "copy sigma")))
         return rc;
     if ((rc = check(cudaMemcpyAsync(sig32_.as<void>(), sigf.data(), nE * sizeof(float), cudaMemcpyHostToDevice, stream_), "copy sigma")))
@@ -349,28 +396,39 @@ static int blocks_for(int64_t n, int nrhs, int &chunk)
 int Solver::ensure_workspace(int nrhs, int precision)
 {
     const int rlen = std::max(ctl.IterPerDivCor, 1) + 1, dlen = std::max(ctl.MaxIterDivCor, 1) + 1;
-    if (ws_.nrhs >= nrhs && ws_.precision == precision && ws_.rlen == rlen && ws_.dlen == dlen) return 0;
+    if (ws_.nrhs >= nrhs && ws_.precision == precision && ws_.rlen == rlen && ws_.dlen == dlen &&
+        ws_.solver == ctl.solver && ws_.formulation == ctl.formulation)
+        return 0;
     Workspace &w = ws_;
     const size_t e64 = (size_t)nrhs * nE * sizeof(double2), e32 = (size_t)nrhs * nE * sizeof(float2);
     const size_t n64 = (size_t)nrhs * nN * sizeof(double2);
     // release everything first so a precision change does not hold both sets
     DevBuf *all[] = {&w.b, &w.X, &w.x1, &w.r, &w.rt, &w.p, &w.v, &w.ph, &w.s, &w.sh, &w.t, &w.bc, &w.tmp,
                      &w.f_b, &w.f_x0, &w.f_x1, &w.f_r, &w.f_rt, &w.f_p, &w.f_v, &w.f_ph, &w.f_s, &w.f_sh, &w.f_t,
-                     &w.px, &w.pr, &w.pp, &w.pq, &w.phi0};
+                     &w.px, &w.pr, &w.pp, &w.pq, &w.phi0, &w.zm, &w.zc, &w.f_zm, &w.f_zc, &w.phi64, &w.phi32};
     for (DevBuf *d : all) d->release();
     int err = 0;
     err |= w.b.alloc(e64) | w.X.alloc(e64) | w.bc.alloc(e64) | w.tmp.alloc(e64);
     if (precision == 0) {
         DevBuf *v64[] = {&w.x1, &w.r, &w.rt, &w.p, &w.v, &w.ph, &w.s, &w.sh, &w.t};
         for (DevBuf *d : v64) err |= d->alloc(e64);
+        if (ctl.solver == 3) err |= w.zm.alloc(e64) | w.zc.alloc(e64);
     } else {
         DevBuf *v32[] = {&w.f_b, &w.f_x0, &w.f_x1, &w.f_r, &w.f_rt, &w.f_p, &w.f_v, &w.f_ph, &w.f_s, &w.f_sh, &w.f_t};
         for (DevBuf *d : v32) err |= d->alloc(e32);
+        if (ctl.solver == 3) err |= w.f_zm.alloc(e32) | w.f_zc.alloc(e32);
     }
-    DevBuf *nv[] = {&w.px, &w.pr, &w.pp, &w.pq, &w.phi0};
-    for (DevBuf *d : nv) err |= d->alloc(n64);
+    if (ctl.formulation == 0) {
+        DevBuf *nv[] = {&w.px, &w.pr, &w.pp, &w.pq, &w.phi0};
+        for (DevBuf *d : nv) err |= d->alloc(n64);
+    } else {
+        err |= w.phi64.alloc(n64);
+        if (precision == 1) err |= w.phi32.alloc((size_t)nrhs * nN * sizeof(float2));
+    }
     int c;
-    const int nb = std::max(blocks_for(nE, nrhs, c), blocks_for(nN, nrhs, c));
+    const ColMapHost cm = col_map(nx, ny);
+    const int nb = std::max({blocks_for(nE, nrhs, c), blocks_for(nN, nrhs, c), cm.tiles * std::max(1, (nz + 1) / 8),
+                             1184});
     err |= w.bst.alloc(nrhs * sizeof(BicgState)) | w.pst.alloc(nrhs * sizeof(PcgState)) |
            w.ost.alloc(nrhs * sizeof(OuterState));
     err |= w.parts.alloc((size_t)nrhs * nb * kMaxParts * sizeof(double)) | w.cnt.alloc(3 * nrhs * sizeof(unsigned));
@@ -388,6 +446,8 @@ int Solver::ensure_workspace(int nrhs, int precision)
     w.precision = precision;
     w.rlen = rlen;
     w.dlen = dlen;
+    w.solver = ctl.solver;
+    w.formulation = ctl.formulation;
     return 0;
 }
 
@@ -412,6 +472,14 @@ template <> KArgs<double> Solver::kargs<double>(int nrhs, int)
     a.maxit = ctl.IterPerDivCor;
     a.inner = 0;
     a.dsgn = -1.0;
+    if (ctl.formulation == 1) {
+        a.sigma = sigs64_.as<double>();
+        a.gd = 1;
+        a.gdw = gdw64_.as<double>();
+        a.gde = gde_.as<unsigned char>();
+        a.phi = w.phi64.as<double2>();
+        a.restart = 120;
+    }
     return a;
 }
 template <> KArgs<float> Solver::kargs<float>(int nrhs, int)
@@ -434,6 +502,55 @@ template <> KArgs<float> Solver::kargs<float>(int nrhs, int)
     a.nblk = blocks_for(nE, nrhs, a.chunk);
     a.maxit = ctl.IterPerDivCor;
     a.inner = 1;
+    a.dsgn = -1.0;
+    if (ctl.formulation == 1) {
+        a.sigma = sigs32_.as<float>();
+        a.gd = 1;
+        a.gdw = gdw32_.as<float>();
+        a.gde = gde_.as<unsigned char>();
+        a.phi = w.phi32.as<float2>();
+        a.restart = 120;
+    }
+    return a;
+}
+
+template <> ColArgs<double> Solver::cargs<double>()
+{
+    ColArgs<double> a{};
+    Workspace &w = ws_;
+    a.g = g64_;
+    a.sigma = sig64_.as<double>();
+    a.ost = w.ost.as<OuterState>();
+    a.st = w.bst.as<BicgState>();
+    a.map = col_map(nx, ny);
+    a.r = w.r.as<double2>(); a.z = w.rt.as<double2>(); a.p = w.p.as<double2>(); a.q = w.v.as<double2>();
+    a.x0 = w.X.as<double2>(); a.x1 = w.x1.as<double2>();
+    a.zm = w.ph.as<double2>(); a.zc = w.s.as<double2>();
+    a.parts = w.parts.as<double>();
+    a.cnt = w.cnt.as<unsigned>();
+    a.rerr = w.rerr.as<double>();
+    a.rerr_stride = ctl.IterPerDivCor + 1;
+    a.stride = nE;
+    a.dsgn = -1.0;
+    return a;
+}
+template <> ColArgs<float> Solver::cargs<float>()
+{
+    ColArgs<float> a{};
+    Workspace &w = ws_;
+    a.g = g32_;
+    a.sigma = sig32_.as<float>();
+    a.ost = w.ost.as<OuterState>();
+    a.st = w.bst.as<BicgState>();
+    a.map = col_map(nx, ny);
+    a.r = w.f_r.as<float2>(); a.z = w.f_rt.as<float2>(); a.p = w.f_p.as<float2>(); a.q = w.f_v.as<float2>();
+    a.x0 = w.f_x0.as<float2>(); a.x1 = w.f_x1.as<float2>();
+    a.zm = w.f_ph.as<float2>(); a.zc = w.f_s.as<float2>();
+    a.parts = w.parts.as<double>();
+    a.cnt = w.cnt.as<unsigned>();
+    a.rerr = w.rerr.as<double>();
+    a.rerr_stride = ctl.IterPerDivCor + 1;
+    a.stride = nE;
     a.dsgn = -1.0;
     return a;
 }
@@ -466,17 +583,50 @@ DArgs Solver::dargs(int nrhs)
 int Solver::run_bicg(int nrhs, int precision, int maxit)
 {
     if (prof_) prof_prec_ = precision;
+    if (ctl.solver == 2) {  // Bi-CG for the complex-symmetric system (COCG) with z-line preconditioner
+        if (precision == 0) {
+            KArgs<double> a = kargs<double>(nrhs, 0);
+            a.maxit = maxit;
+            ColArgs<double> c = cargs<double>();
+            launch_bicg_init(a, nrhs, stream_);
+            launch_zl_setup(c, nrhs, stream_);
+            launch_cocg_start(c, nrhs, stream_);
+            for (int it = 0; it < maxit; it++) launch_cocg_iter(c, nrhs, stream_, next_events(2));
+            launch_bicg_finish(a, nrhs, stream_);
+        } else {
+            KArgs<float> a = kargs<float>(nrhs, 1);
+            a.maxit = maxit;
+            ColArgs<float> c = cargs<float>();
+            launch_bicg_init(a, nrhs, stream_);
+            launch_zl_setup(c, nrhs, stream_);
+            launch_cocg_start(c, nrhs, stream_);
+            for (int it = 0; it < maxit; it++) launch_cocg_iter(c, nrhs, stream_, next_events(2));
+            launch_bicg_finish(a, nrhs, stream_);
+        }
+        return check(cudaGetLastError(), "Bi-CG launch");
+    }
+    const bool zl = ctl.solver == 3;  // BiCGStab with the z-line preconditioner
     if (precision == 0) {
         KArgs<double> a = kargs<double>(nrhs, 0);
         a.maxit = maxit;
+        a.pc_ext = zl;
+        ColArgs<double> c = cargs<double>();
+        c.zm = ws_.zm.as<double2>();
+        c.zc = ws_.zc.as<double2>();
         launch_bicg_init(a, nrhs, stream_);
-        for (int it = 0; it < maxit; it++) launch_bicg_iter(a, nrhs, stream_, next_events(4));
+        if (zl) launch_zl_setup(c, nrhs, stream_);
+        for (int it = 0; it < maxit; it++) launch_bicg_iter(a, nrhs, stream_, next_events(4), zl ? &c : nullptr);
         launch_bicg_finish(a, nrhs, stream_);
     } else {
         KArgs<float> a = kargs<float>(nrhs, 1);
         a.maxit = maxit;
+        a.pc_ext = zl;
+        ColArgs<float> c = cargs<float>();
+        c.zm = ws_.f_zm.as<float2>();
+        c.zc = ws_.f_zc.as<float2>();
         launch_bicg_init(a, nrhs, stream_);
-        for (int it = 0; it < maxit; it++) launch_bicg_iter(a, nrhs, stream_, next_events(4));
+        if (zl) launch_zl_setup(c, nrhs, stream_);
+        for (int it = 0; it < maxit; it++) launch_bicg_iter(a, nrhs, stream_, next_events(4), zl ? &c : nullptr);
         launch_bicg_finish(a, nrhs, stream_);
     }
     return check(cudaGetLastError(), "BiCG launch");
@@ -511,7 +661,7 @@ int Solver::mult_aii(int adjt, const double *x, double *y)
     launch_scatter_interior((int)nEi, edgei_d_.as<int>(), xi, xf, stream_);
     KArgs<double> a = kargs<double>(1, 0);
     a.dsgn = adjt ? 1.0 : -1.0;
-    launch_apply(a, xf, yf, 0, 1, stream_);
+    launch_apply(a, xf, yf, 0, 1, stream_, ctl.formulation == 1);
     launch_gather_interior((int)nEi, edgei_d_.as<int>(), yf, xi, stream_);
     cudaMemcpyAsync(y, xi, nEi * sizeof(double2), cudaMemcpyDeviceToHost, stream_);
     return sync("mt3d_mult_aii");
@@ -632,10 +782,18 @@ int Solver::solve(int nrhs, const double *omegas, const int *trans, const double
         any_src = any_src || o.has_src;
     }
     cudaMemcpyAsync(w.ost.as<void>(), os.data(), nrhs * sizeof(OuterState), cudaMemcpyHostToDevice, stream_);
-    // sources: b += V_E src (forward) or b = src (transposed); phi0
+    // sources: b += V_E src (forward) or b = src (transposed); phi0 for the
+    // divergence correction, or the grad-div source correction of the SP2
+    // right-hand side (f90/3D_MT/FWD_SP2/EMsolve3D.f90:215-228, 271-289)
     if (any_src) {
         launch_add_src(g64_, B, TMP, nE, w.ost.as<OuterState>(), nrhs, stream_);
-        launch_phi0(g64_, TMP, nE, w.phi0.as<double2>(), nN, w.ost.as<OuterState>(), nrhs, stream_);
+        if (ctl.formulation == 0) {
+            launch_phi0(g64_, TMP, nE, w.phi0.as<double2>(), nN, w.ost.as<OuterState>(), nrhs, stream_);
+        } else {
+            KArgs<double> a = kargs<double>(nrhs, 0);
+            launch_gd_phi(a, TMP, a.phi, 1, nrhs, stream_);
+            launch_gd_add(a, B, a.phi, nrhs, stream_);
+        }
     }
     {
         KArgs<double> a = kargs<double>(nrhs, 0);
@@ -676,7 +834,7 @@ int Solver::solve(int nrhs, const double *omegas, const int *trans, const double
     // initial divergence correction for a source term (EMsolve3D.f90:298-303)
     bool any_dc = false;
     for (int r = 0; r < nrhs; r++) {
-        os[r].dc_run = os[r].active && os[r].has_src;
+        os[r].dc_run = ctl.formulation == 0 && os[r].active && os[r].has_src;
         if (os[r].dc_run) { os[r].nDivCor = 1; any_dc = true; }
     }
     push_state();
@@ -692,8 +850,9 @@ int Solver::solve(int nrhs, const double *omegas, const int *trans, const double
         for (auto &o : os) if (o.active) return true;
         return false;
     };
+    const bool refine = prec == 1 || ctl.formulation == 1;  // loop driven by the true FP64 residual
     while (any_active()) {
-        if (prec == 1) {
+        if (refine) {
             // true FP64 residual r64 = b - A X (into tmp); converged right-hand
             // sides leave the loop, the others get an FP32 correction solve
             for (auto &o : os) o.dc_run = 0;
@@ -716,8 +875,9 @@ int Solver::solve(int nrhs, const double *omegas, const int *trans, const double
             }
             if (!work) break;
             push_state();
-            launch_cast(w.ost.as<OuterState>(), (int)nE, nE, w.tmp.as<double2>(), w.f_b.as<float2>(),
-                        w.f_x0.as<float2>(), nrhs, stream_);
+            if (prec == 1)
+                launch_cast(w.ost.as<OuterState>(), (int)nE, nE, w.tmp.as<double2>(), w.f_b.as<float2>(),
+                            w.f_x0.as<float2>(), nrhs, stream_);
         }
         // Krylov call: FP64 on (b, X), or FP32 on the normalised residual
         if ((rc = run_bicg(nrhs, prec, ctl.IterPerDivCor))) return rc;
@@ -739,7 +899,7 @@ int Solver::solve(int nrhs, const double *omegas, const int *trans, const double
             if (!conv) h[maxit - 1] = st.imin > 0 ? h[st.imin - 1] : h[0];
             for (int k = 0; k < niter; k++) dg[r].EMrelErr.push_back(h[k]);
             o.nIterTotal += niter;
-            if (prec == 0) {
+            if (!refine) {
                 if (conv) o.converged = 1;
                 if (st.status == KS_BREAKDOWN || st.status == KS_NAN) o.failed = (st.status == KS_NAN) ? 3 : 2;
             } else if (st.status == KS_NAN) {
@@ -747,8 +907,8 @@ int Solver::solve(int nrhs, const double *omegas, const int *trans, const double
             }
             o.nDivCor += 1;
             if (o.nDivCor < ctl.MaxDivCor) {
-                o.dc_run = 1;
-            } else if (prec == 0) {
+                o.dc_run = ctl.formulation == 0;
+            } else if (!refine) {
                 if (!o.failed) o.failed = 1;
             }
         }
@@ -765,7 +925,7 @@ int Solver::solve(int nrhs, const double *omegas, const int *trans, const double
             OuterState &o = os[r];
             o.dc_run = 0;
             if (!o.active) continue;
-            if (prec == 0) {
+            if (!refine) {
                 if (o.converged || o.failed) o.active = 0;
             } else if (o.failed == 3) {
                 o.active = 0;

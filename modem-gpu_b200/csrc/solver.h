@@ -15,8 +15,9 @@ struct Control {
     double tolEMfwd = 1e-7;
     double tolEMadj = 1e-7;
     double tolDivCor = 1e-5;
-    int solver = 1;     // BICG
+    int solver = 1;     // 1: BiCGStab (reference BICG) + diagonal; 2: Bi-CG/COCG + z-line
     int precision = 0;  // 0 FP64, 1 mixed
+    int formulation = 0;  // 0 curl-curl + divergence correction (MF), 1 curl-curl + grad-div (SP2)
 };
 
 struct Diag {
@@ -46,12 +47,16 @@ struct Workspace {
     int nrhs = 0;
     int precision = -1;
     int rlen = 0, dlen = 0;  // rerr row lengths the buffers were sized for
+    int solver = 0;
+    int formulation = 0;
     // FP64 edge vectors [nrhs][nE]
     DevBuf b, X, x1, r, rt, p, v, ph, s, sh, t, bc, tmp;
     // FP32 edge vectors (mixed)
     DevBuf f_b, f_x0, f_x1, f_r, f_rt, f_p, f_v, f_ph, f_s, f_sh, f_t;
     // FP64 node vectors [nrhs][nN]
     DevBuf px, pr, pp, pq, phi0;
+    DevBuf zm, zc, f_zm, f_zc;  // z-line pivots for BiCGStab + z-line
+    DevBuf phi64, phi32;        // grad-div node potentials
     DevBuf bst, pst, ost, parts, cnt, rerr, dcrerr;
 };
 
@@ -87,6 +92,7 @@ class Solver {
     int run_bicg(int nrhs, int precision, int maxit);
     int run_divcorr(int nrhs);
     template <typename T> KArgs<T> kargs(int nrhs, int precision_ws);
+    template <typename T> ColArgs<T> cargs();
     DArgs dargs(int nrhs);
     int check(cudaError_t e, const char *what);
     int sync(const char *what);
@@ -105,6 +111,7 @@ class Solver {
     Geo<double> g64_{};
     Geo<float> g32_{};
     DevBuf tab64_, tab32_, sig64_, sig32_, coef_, edgei_d_;
+    DevBuf sigs64_, sigs32_, gdw64_, gdw32_, gde_;  // grad-div (SP2) data
     Workspace ws_;
     std::vector<double> dx_, dy_, dz_, delX_, delY_, delZ_;
 };

@@ -18,12 +18,13 @@ LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libmt3d.so")
 
 STATUS = {0: "MT3D_OK", 1: "MT3D_NOT_CONVERGED", 2: "MT3D_BREAKDOWN", 3: "MT3D_NAN_INPUT", 4: "MT3D_CUDA_ERROR",
           5: "MT3D_INVALID_ARGUMENT", 6: "MT3D_DEVICE_TIMEOUT", 7: "MT3D_NO_DEVICE", 8: "MT3D_OUT_OF_MEMORY"}
-SOLVER_BICG = 1
+SOLVER_BICG, SOLVER_COCG, SOLVER_BICG_ZLINE = 1, 2, 3
 PREC_FP64, PREC_MIXED = 0, 1
+FORM_CCDC, FORM_CCGD = 0, 1
 
 #: every symbol include/mt3d.h declares
 EXPORTS = ["mt3d_version", "mt3d_device_count", "mt3d_create", "mt3d_destroy", "mt3d_set_control", "mt3d_update_cond",
-           "mt3d_update_freq", "mt3d_sizes", "mt3d_interior_index", "mt3d_mult_aii", "mt3d_bicg", "mt3d_fwdsolve",
+           "mt3d_update_freq", "mt3d_set_formulation", "mt3d_sizes", "mt3d_interior_index", "mt3d_mult_aii", "mt3d_bicg", "mt3d_fwdsolve",
            "mt3d_fwdsolve_batch", "mt3d_fwdsolve_batch_device", "mt3d_set_stream", "mt3d_profile",
            "mt3d_kernel_time", "mt3d_get_diag", "mt3d_get_batch_diag", "mt3d_pmult_t", "mt3d_launch_counter", "mt3d_last_error"]
 
@@ -55,6 +56,7 @@ def load(path: str = LIB_PATH):
     L.mt3d_set_control.argtypes = [P, I, I, I, C.c_double, C.c_double, C.c_double, I, I]
     L.mt3d_update_cond.argtypes = [P, D, C.c_double]
     L.mt3d_update_freq.argtypes = [P, C.c_double]
+    L.mt3d_set_formulation.argtypes = [P, I]
     L.mt3d_sizes.argtypes = [P, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     L.mt3d_interior_index.argtypes = [P, C.POINTER(C.c_int32)]
     L.mt3d_mult_aii.argtypes = [P, I, D, D]
@@ -128,6 +130,9 @@ class Solver:
                     tolDivCor=1e-5, solver=SOLVER_BICG, precision=PREC_FP64):
         self._check(self.L.mt3d_set_control(self.h, IterPerDivCor, MaxDivCor, MaxIterDivCor, tolEMfwd, tolEMadj,
                                             tolDivCor, solver, precision))
+
+    def set_formulation(self, formulation):
+        self._check(self.L.mt3d_set_formulation(self.h, int(formulation)))
 
     def update_cond(self, m_earth, air_cond):
         m = np.ascontiguousarray(m_earth, np.float64)

@@ -23,7 +23,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "liboracle.so")
 
 QMR, BICG, COCG = 0, 1, 2
-PC_DILU, PC_JACOBI = 0, 1
+PC_DILU, PC_JACOBI, PC_RBDILU, PC_DILU_SWEEP, PC_ZLINE = 0, 1, 2, 3, 4
 
 _lib = None
 

@@ -16,7 +16,7 @@ import pytest
 from helpers import earth_mask, random_model, relerr, small_grid
 from mt3d import bc as mbc
 from mt3d import capi, models
-from oracle.oracle import BICG, PC_JACOBI, Oracle, interior_edge_mask
+from oracle.oracle import BICG, COCG, PC_JACOBI, PC_ZLINE, Oracle, interior_edge_mask
 
 pytestmark = pytest.mark.gpu
 
@@ -224,3 +224,183 @@ def test_error_paths(cuda):
     bcv[1 + g.nx * (g.ny + 1)] = np.nan
     e, rc = s.fwdsolve(bc=bcv)
     assert rc == 3
+
+
+# ---------------------------------------------------------------------------
+# Bi-CG for the complex-symmetric system (COCG) with the z-line preconditioner
+# ---------------------------------------------------------------------------
+def make_cocg_pair(g, m, omega, **ctl):
+    o = Oracle(g)
+    o.update_cond(m.m_earth, m.air_cond)
+    o.update_freq(omega)
+    o.set_control(solver=COCG, precond=PC_ZLINE, **ctl)
+    s = capi.Solver(g)
+    s.update_cond(m.m_earth, m.air_cond)
+    s.update_freq(omega)
+    s.set_control(solver=capi.SOLVER_COCG, **ctl)
+    return o, s
+
+
+@pytest.fixture(scope="module")
+def cprob(cuda):
+    g = small_grid()
+    m = random_model(g, seed=3)
+    omega = 2 * np.pi * 0.5
+    o, s = make_cocg_pair(g, m, omega)
+    return g, m, omega, o, s
+
+
+@pytest.mark.parametrize("mode", [1, 2])
+def test_cocg_fp64_matches_oracle(cprob, mode):
+    g, m, omega, o, s = cprob
+    bcv = mbc.boundary_1d(m, omega, mode)
+    s.set_control(solver=capi.SOLVER_COCG, precision=capi.PREC_FP64)
+    eg, rc = s.fwdsolve(bc=bcv)
+    eo, rco = o.fwdsolve(bc=bcv)
+    assert rc == 0 and rco == 0
+    dg, do = s.diagnostics(), o.diagnostics()
+    # same method: the residual histories agree over the first iterations
+    k = min(15, len(do["EMrelErr"]), len(dg["EMrelErr"]))
+    assert np.max(np.abs(dg["EMrelErr"][:k] - do["EMrelErr"][:k]) / do["EMrelErr"][:k]) < 1e-6
+    em = earth_mask(g, m)
+    assert relerr(eg[em], eo[em]) < 1e-5
+    assert abs(dg["nIterTotal"] - do["nIterTotal"]) <= max(3, 0.1 * do["nIterTotal"])
+
+
+def test_cocg_mixed_matches_fp64(cprob):
+    g, m, omega, o, s = cprob
+    bcv = mbc.boundary_1d(m, omega, 2)
+    s.set_control(solver=capi.SOLVER_COCG, precision=capi.PREC_FP64)
+    e64, rc64 = s.fwdsolve(bc=bcv)
+    s.set_control(solver=capi.SOLVER_COCG, precision=capi.PREC_MIXED)
+    emx, rcm = s.fwdsolve(bc=bcv)
+    d = s.diagnostics()
+    assert rc64 == 0 and rcm == 0 and d["final_relres"] <= 1e-7
+    em = earth_mask(g, m)
+    assert relerr(emx[em], e64[em]) < 1e-5
+
+
+def test_cocg_transposed_and_batch(cprob):
+    g, m, omega, o, s = cprob
+    mask = interior_edge_mask(g)
+    em = mask & earth_mask(g, m)
+    rng = np.random.default_rng(4)
+    src = np.where(em, rng.standard_normal(g.n_edges) + 1j * rng.standard_normal(g.n_edges), 0) * o.VE
+    oms = np.array([omega, 2 * np.pi * 0.05, omega, 2 * np.pi * 0.05])
+    srcs = np.stack([src] * 4)
+    s.set_control(solver=capi.SOLVER_COCG, precision=capi.PREC_MIXED, MaxDivCor=100)
+    eb, st, rc = s.fwdsolve_batch(oms, trans=np.ones(4, np.int32), src=srcs)
+    assert rc == 0 and np.all(st == 0)
+    o.set_control(solver=COCG, precond=PC_ZLINE, MaxDivCor=100)
+    for r in (0, 1):
+        o.update_freq(oms[r])
+        eo, rco = o.fwdsolve(trans=True, src=src)
+        assert rco == 0
+        sel = earth_mask(g, m)
+        assert relerr(eb[r][sel], eo[sel]) < 1e-5
+    o.update_freq(omega)
+
+
+def test_cocg_config_small_forward(cuda):
+    m, freqs = models.config_small_forward()
+    g = m.grid
+    omega = 2 * np.pi * freqs[0]
+    o, s = make_cocg_pair(g, m, omega)
+    bcs = np.stack([mbc.boundary_1d(m, omega, md) for md in (1, 2)])
+    em = earth_mask(g, m)
+    s.set_control(solver=capi.SOLVER_COCG, precision=capi.PREC_MIXED)
+    eb, st, rc = s.fwdsolve_batch(np.array([omega, omega]), bc=bcs)
+    assert rc == 0
+    for r in range(2):
+        eo, rco = o.fwdsolve(bc=bcs[r])
+        assert rco == 0
+        assert relerr(eb[r][em], eo[em]) < 1e-5
+
+
+# ---------------------------------------------------------------------------
+# BiCGStab with the z-line preconditioner
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("prec", [0, 1])
+def test_bicg_zline_matches_oracle(cuda, prec):
+    g = small_grid()
+    m = random_model(g, seed=3)
+    omega = 2 * np.pi * 0.5
+    o = Oracle(g)
+    o.update_cond(m.m_earth, m.air_cond)
+    o.update_freq(omega)
+    o.set_control(solver=BICG, precond=PC_ZLINE)
+    s = capi.Solver(g)
+    s.update_cond(m.m_earth, m.air_cond)
+    s.update_freq(omega)
+    s.set_control(solver=capi.SOLVER_BICG_ZLINE, precision=prec)
+    bcv = mbc.boundary_1d(m, omega, 1)
+    eg, rc = s.fwdsolve(bc=bcv)
+    eo, rco = o.fwdsolve(bc=bcv)
+    assert rc == 0 and rco == 0
+    dg, do = s.diagnostics(), o.diagnostics()
+    if prec == 0:
+        k = min(12, len(do["EMrelErr"]), len(dg["EMrelErr"]))
+        assert np.max(np.abs(dg["EMrelErr"][:k] - do["EMrelErr"][:k]) / do["EMrelErr"][:k]) < 1e-6
+    em = earth_mask(g, m)
+    assert relerr(eg[em], eo[em]) < 1e-5
+
+
+# ---------------------------------------------------------------------------
+# SP2 formulation (curl-curl + grad-div, no divergence correction)
+# ---------------------------------------------------------------------------
+@pytest.fixture(scope="module")
+def gprob(cuda):
+    from oracle.sp2 import SP2
+    g = small_grid()
+    m = random_model(g, seed=3)
+    omega = 2 * np.pi * 0.5
+    ref = SP2(g, m)
+    ref.set_freq(omega)
+    s = capi.Solver(g)
+    s.set_formulation(capi.FORM_CCGD)
+    s.update_cond(m.m_earth, m.air_cond)
+    s.update_freq(omega)
+    s.set_control(IterPerDivCor=120, MaxDivCor=20)
+    return g, m, omega, ref, s
+
+
+def test_ccgd_operator_matches_sp2(gprob):
+    g, m, omega, ref, s = gprob
+    rng = np.random.default_rng(0)
+    xi = rng.standard_normal(s.nEi) + 1j * rng.standard_normal(s.nEi)
+    assert relerr(s.mult_aii(xi), ref.A @ xi) < 1e-12
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_ccgd_forward_matches_sp2_and_ccdc(gprob, prec):
+    g, m, omega, ref, s = gprob
+    bcv = mbc.boundary_1d(m, omega, 2)
+    s.set_control(IterPerDivCor=120, MaxDivCor=20, precision=prec)
+    eg, rc = s.fwdsolve(bc=bcv)
+    er, it, rerr, conv = ref.fwdsolve(bc=bcv)
+    assert rc == 0 and conv
+    em = earth_mask(g, m)
+    assert relerr(eg[em], er[em]) < 1e-5
+    assert s.diagnostics()["final_relres"] <= 1e-7
+    # the same discrete solution as the divergence-corrected curl-curl system
+    o = Oracle(g)
+    o.update_cond(m.m_earth, m.air_cond)
+    o.update_freq(omega)
+    o.set_control(solver=BICG, precond=PC_JACOBI, tolEMfwd=1e-9)
+    eo, rco = o.fwdsolve(bc=bcv)
+    assert relerr(eg[em], eo[em]) < 1e-5
+
+
+def test_ccgd_sources_match_sp2(gprob):
+    g, m, omega, ref, s = gprob
+    mask = interior_edge_mask(g)
+    em = mask & earth_mask(g, m)
+    rng = np.random.default_rng(6)
+    src = np.where(em, rng.standard_normal(g.n_edges) + 1j * rng.standard_normal(g.n_edges), 0)
+    s.set_control(IterPerDivCor=120, MaxDivCor=20, precision=capi.PREC_MIXED)
+    for trans in (False, True):
+        sv = src * ref.topo.Vedge if trans else src
+        eg, rc = s.fwdsolve(trans=trans, src=sv)
+        er, it, rerr, conv = ref.fwdsolve(trans=trans, src=sv)
+        assert rc == 0 and conv
+        assert relerr(eg[mask], er[mask]) < 1e-5

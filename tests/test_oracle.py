@@ -169,3 +169,25 @@ def test_divcorr_reduces_divergence(setup):
     e, rc = o.fwdsolve(bc=mbc.boundary_1d(m, omega, 1))
     d = o.diagnostics()
     assert np.all(d["divJ"][:, 1] <= d["divJ"][:, 0])
+
+
+def test_sp2_restatement_matches_ccdc():
+    """The SP2 (curl-curl + grad-div) restatement reaches the same discrete
+    solution as the divergence-corrected curl-curl oracle (the grad-div term
+    vanishes at the solution, f90/3D_MT/FWD_SP2/modelOperator3D.f90:797-830)."""
+    from oracle.sp2 import SP2
+    g = small_grid()
+    m = random_model(g, seed=3)
+    w = 2 * np.pi * 0.5
+    s = SP2(g, m)
+    s.set_freq(w)
+    assert abs(s.topo.CC - assemble_cc(g)).max() == 0.0
+    bcv = mbc.boundary_1d(m, w, 2)
+    e, it, rerr, conv = s.fwdsolve(bc=bcv)
+    o = Oracle(g)
+    o.update_cond(m.m_earth, m.air_cond)
+    o.update_freq(w)
+    o.set_control(solver=BICG, precond=PC_JACOBI, tolEMfwd=1e-9)
+    eo, rc = o.fwdsolve(bc=bcv)
+    em = earth_mask(g, m)
+    assert conv and rc == 0 and relerr(e[em], eo[em]) < 1e-6
