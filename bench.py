@@ -243,31 +243,29 @@ def main():
     solvers = []
     for m, oms, bcs, srcs in probs:
         s = capi.Solver(m.grid, device=local)
+        s.set_formulation(capi.FORM_CCGD)
         s.update_cond(m.m_earth, m.air_cond)
-        s.set_control(tolEMfwd=TOL, tolEMadj=TOL, MaxDivCor=200, precision=capi.PREC_MIXED)
+        s.set_control(tolEMfwd=TOL, tolEMadj=TOL, IterPerDivCor=120, MaxDivCor=100, precision=capi.PREC_MIXED)
         s.set_stream(torch.cuda.current_stream(dev).cuda_stream)
         nr = len(oms)
-        d_bc = torch.from_numpy(bcs).to(dev)
-        d_src = torch.from_numpy(srcs).to(dev)
-        d_e = torch.zeros((nr, s.nE), dtype=torch.complex128, device=dev)
-        zeros = torch.zeros_like(d_e)
-        solvers.append((s, oms, d_bc, d_src, d_e, zeros))
+        # rows 0..nr-1: forward (boundary data, no source); nr..2nr-1: adjoint (source, no boundary data)
+        zb = np.zeros_like(bcs)
+        d_bc = torch.from_numpy(np.concatenate([bcs, zb])).to(dev)
+        d_src = torch.from_numpy(np.concatenate([zb, srcs])).to(dev)
+        d_e = torch.zeros((2 * nr, s.nE), dtype=torch.complex128, device=dev)
+        tr = np.concatenate([np.zeros(nr, np.int32), np.ones(nr, np.int32)])
+        solvers.append((s, np.concatenate([oms, oms]), d_bc, d_src, d_e, tr))
     n_solves = sum(2 * len(p[1]) for p in probs)
 
     def step(stats=None):
-        for s, oms, d_bc, d_src, d_e, zeros in solvers:
-            nr = len(oms)
+        # forward and adjoint right-hand sides of a model in one batched call
+        for s, oms2, d_bc, d_src, d_e, tr in solvers:
             d_e.zero_()
-            st, rc = s.fwdsolve_batch_device(oms, d_e.data_ptr(), bc_ptr=d_bc.data_ptr())
+            st, rc = s.fwdsolve_batch_device(oms2, d_e.data_ptr(), bc_ptr=d_bc.data_ptr(), src_ptr=d_src.data_ptr(),
+                                             trans=tr)
             if stats is not None:
-                it, rr = s.batch_diagnostics(nr)
+                it, rr = s.batch_diagnostics(len(oms2))
                 stats.append((s.nE, it.copy(), rr.copy(), st.copy()))
-            d_e.zero_()
-            st2, rc2 = s.fwdsolve_batch_device(oms, d_e.data_ptr(), src_ptr=d_src.data_ptr(),
-                                               trans=np.ones(nr, np.int32))
-            if stats is not None:
-                it, rr = s.batch_diagnostics(nr)
-                stats.append((s.nE, it.copy(), rr.copy(), st2.copy()))
 
     def barrier():
         if dist is not None:
@@ -312,8 +310,9 @@ def main():
     sc = 8 if kprec else 16  # bytes of one complex entry
     sr = 4 if kprec else 8
     # per edge and right-hand side: read the preconditioned vector, rt (or s),
-    # sigma; write the result
-    b_edge = 3 * sc + sr
+    # sigma and the grad-div node potentials (one node per edge on average:
+    # nN / nE ~ 1/3 of a complex); write the result
+    b_edge = 3 * sc + sr + sc / 3
     alg_bytes = sum(float(nE) * it.sum() * 2 * b_edge for nE, it, rr, st in stats)
     converged = all(np.all(st == 0) for _, _, _, st in stats)
     max_relres = max(float(np.max(rr)) for _, _, rr, _ in stats)
@@ -326,9 +325,8 @@ def main():
 
     # end to end through the C ABI with host buffers (pinned), copies inside
     pinned = []
-    for s, oms, d_bc, d_src, d_e, zeros in solvers:
-        nr = len(oms)
-        hbc = torch.empty((nr, s.nE), dtype=torch.complex128).pin_memory()
+    for s, oms2, d_bc, d_src, d_e, tr in solvers:
+        hbc = torch.empty(tuple(d_bc.shape), dtype=torch.complex128).pin_memory()
         hsrc = torch.empty_like(hbc).pin_memory()
         he = torch.empty_like(hbc).pin_memory()
         hbc.copy_(d_bc.cpu())
@@ -338,13 +336,11 @@ def main():
     barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        for (s, oms, *_), (hbc, hsrc, he) in zip(solvers, pinned):
-            nr = len(oms)
+        for (s, oms2, d_bc, d_src, d_e, tr), (hbc, hsrc, he) in zip(solvers, pinned):
             he[:] = 0
-            s.fwdsolve_batch(oms, bc=hbc, e0=he)
-            s.fwdsolve_batch(oms, src=hsrc, e0=he, trans=np.ones(nr, np.int32))
-            h2d += hbc.nbytes + hsrc.nbytes + 2 * he.nbytes
-            d2h += 2 * he.nbytes
+            s.fwdsolve_batch(oms2, bc=hbc, src=hsrc, e0=he, trans=tr)
+            h2d += hbc.nbytes + hsrc.nbytes + he.nbytes
+            d2h += he.nbytes
     barrier()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     e2e = {"value": world * n_solves * args.steps / e2e_s, "unit": "solves/s",
@@ -356,16 +352,14 @@ def main():
         barrier()
         t0 = time.perf_counter()
         nfp = 0
-        for s, oms, d_bc, d_src, d_e, zeros in solvers:
-            s.set_control(tolEMfwd=TOL, tolEMadj=TOL, MaxDivCor=200, precision=capi.PREC_FP64)
-            for r in range(len(oms)):
+        for s, oms2, d_bc, d_src, d_e, tr in solvers:
+            s.set_control(tolEMfwd=TOL, tolEMadj=TOL, IterPerDivCor=120, MaxDivCor=100, precision=capi.PREC_FP64)
+            for r in range(len(oms2)):
                 e1 = torch.zeros((1, s.nE), dtype=torch.complex128, device=dev)
-                s.fwdsolve_batch_device(oms[r:r + 1], e1.data_ptr(), bc_ptr=d_bc[r:r + 1].data_ptr())
-                e1.zero_()
-                s.fwdsolve_batch_device(oms[r:r + 1], e1.data_ptr(), src_ptr=d_src[r:r + 1].data_ptr(),
-                                        trans=np.ones(1, np.int32))
-                nfp += 2
-            s.set_control(tolEMfwd=TOL, tolEMadj=TOL, MaxDivCor=200, precision=capi.PREC_MIXED)
+                s.fwdsolve_batch_device(oms2[r:r + 1], e1.data_ptr(), bc_ptr=d_bc[r:r + 1].data_ptr(),
+                                        src_ptr=d_src[r:r + 1].data_ptr(), trans=tr[r:r + 1])
+                nfp += 1
+            s.set_control(tolEMfwd=TOL, tolEMadj=TOL, IterPerDivCor=120, MaxDivCor=100, precision=capi.PREC_MIXED)
         barrier()
         fp64_s = max_over_ranks(time.perf_counter() - t0)
         fp64 = world * nfp / fp64_s
@@ -380,7 +374,7 @@ def main():
                 "warmup": args.warmup, "ms_per_step": ms_dev / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "c64 inner / c128 refinement", "data": "synthetic",
                 "config": {"workload": f"{args.workload}: {desc}", "solves_per_step": n_solves, "tol": TOL,
-                           "precision": "mixed (FP32 Krylov, FP64 residual + div. correction)",
+                           "precision": "mixed (FP32 BiCGStab, FP64 residual refinement)", "formulation": "curl-curl + grad-div (SP2), diagonal preconditioner",
                            "l2": "fields larger than L2 (flush not needed)" if args.workload == "combined" else
                                  "inputs smaller than L2 at this size; no flush (iterative solve re-reads its own "
                                  "vectors every iteration)",

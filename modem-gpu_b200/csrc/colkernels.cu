@@ -17,6 +17,7 @@
 #include <atomic>
 
 #include "colstencil.cuh"
+#include "finalize.cuh"
 #include "kernels.h"
 
 namespace mt3d {
@@ -354,6 +355,176 @@ template <typename T> __global__ void __launch_bounds__(kThreads) kc_xrz(ColArgs
 }
 
 // ---------------------------------------------------------------------------
+// BiCGStab stencil kernels in column-marching form (KArgs; flat elementwise
+// kernels do the vector updates).  blockIdx.z chunks the node planes; the
+// reduction counts (x, z) blocks per right-hand side.
+// ---------------------------------------------------------------------------
+template <typename T> __device__ __forceinline__ void kb_range(const Geo<T> &g, int &k0, int &k1)
+{
+    const int kc = (g.nz + 1 + gridDim.z - 1) / gridDim.z;
+    k0 = blockIdx.z * kc;
+    k1 = min(k0 + kc, g.nz + 1);
+}
+template <typename T> __device__ __forceinline__ const C2<T> *kb_phi(const KArgs<T> &a, int r)
+{
+    return a.gd ? a.phi + (size_t)r * a.g.nN : nullptr;
+}
+
+// start of a call: r = b - A x0, rt = r; |b|^2, |r|^2
+template <typename T> __global__ void __launch_bounds__(kThreads) kcb_init(KArgs<T> a)
+{
+    const int r = blockIdx.y;
+    if (!a.ost[r].active) return;
+    BicgState &st = a.st[r];
+    int i, j;
+    double v[2] = {0.0, 0.0};
+    if (col_of(a.cmap, a.g.nx, a.g.ny, i, j)) {
+        const size_t off = (size_t)r * a.stride;
+        int k0, k1;
+        kb_range(a.g, k0, k1);
+        const C2<T> *b = a.b + off;
+        C2<T> *R = a.r + off, *RT = a.rt + off;
+        col_march(a.g, a.x0 + off, a.sigma, i, j, k0, k1, c_wmu<T>(a.ost, r, a.dsgn),
+                  [&](int, int e, bool in, C2<T> ax, C2<T>, T) {
+                      C2<T> res = mk<T>(0, 0);
+                      if (in) {
+                          const C2<T> bb = b[e];
+                          res = csub(bb, ax);
+                          v[0] += (double)bb.x * bb.x + (double)bb.y * bb.y;
+                          v[1] += (double)res.x * res.x + (double)res.y * res.y;
+                      }
+                      R[e] = res;
+                      RT[e] = res;
+                  },
+                  kb_phi(a, r));
+    }
+    double tot[2];
+    if (block_reduce_last<2>(v, a.parts, a.cnt, r, blockIdx.x + gridDim.x * blockIdx.z, gridDim.x * gridDim.z, tot) &&
+        threadIdx.x == 0)
+        fin_init(st, tot, a.rerr + (size_t)r * a.rerr_stride, a.maxit, a.inner ? a.ost[r].tol_inner : a.ost[r].tol);
+}
+
+// v = A ph ; rtv = rt . v ; alpha = rho / rtv   (which = 0)
+// t = A sh ; ts = t . s, tt = t . t ; omega     (which = 1)
+template <typename T> __global__ void __launch_bounds__(kThreads) kcb_vt(KArgs<T> a, int which)
+{
+    const int r = blockIdx.y;
+    BicgState &st = a.st[r];
+    if (st.status != KS_RUNNING || !a.ost[r].active) return;
+    int i, j;
+    double v[3] = {0.0, 0.0, 0.0};
+    if (col_of(a.cmap, a.g.nx, a.g.ny, i, j)) {
+        const size_t off = (size_t)r * a.stride;
+        int k0, k1;
+        kb_range(a.g, k0, k1);
+        const C2<T> *in = (which ? a.sh : a.ph) + off;
+        const C2<T> *w = (which ? a.s : a.rt) + off;
+        C2<T> *out = (which ? a.t : a.v) + off;
+        col_march(a.g, in, a.sigma, i, j, k0, k1, c_wmu<T>(a.ost, r, a.dsgn),
+                  [&](int, int e, bool inn, C2<T> y, C2<T>, T) {
+                      if (!inn) {
+                          y = mk<T>(0, 0);
+                      } else if (which == 0) {
+                          const C2<T> t = w[e];
+                          v[0] += (double)t.x * y.x + (double)t.y * y.y;  // conj(rt) v
+                          v[1] += (double)t.x * y.y - (double)t.y * y.x;
+                      } else {
+                          const C2<T> s = w[e];
+                          v[0] += (double)y.x * s.x + (double)y.y * s.y;  // conj(t) s
+                          v[1] += (double)y.x * s.y - (double)y.y * s.x;
+                          v[2] += (double)y.x * y.x + (double)y.y * y.y;
+                      }
+                      out[e] = y;
+                  },
+                  kb_phi(a, r));
+    }
+    double tot[3];
+    if (block_reduce_last<3>(v, a.parts, a.cnt, r, blockIdx.x + gridDim.x * blockIdx.z, gridDim.x * gridDim.z, tot) &&
+        threadIdx.x == 0) {
+        if (which == 0) fin_v(st, tot);
+        else fin_t(st, tot);
+    }
+}
+
+// true FP64 residual r = b - A X (refinement loop); |r|^2 -> relres, scale
+__global__ void __launch_bounds__(kThreads) kcb_res64(KArgs<double> a)
+{
+    const int r = blockIdx.y;
+    OuterState &os = a.ost[r];
+    if (!os.active) return;
+    int i, j;
+    double v[1] = {0.0};
+    if (col_of(a.cmap, a.g.nx, a.g.ny, i, j)) {
+        const size_t off = (size_t)r * a.stride;
+        int k0, k1;
+        kb_range(a.g, k0, k1);
+        const double2 *b = a.b + off;
+        double2 *R = a.r + off;
+        col_march(a.g, a.x0 + off, a.sigma, i, j, k0, k1, c_wmu<double>(a.ost, r, a.dsgn),
+                  [&](int, int e, bool in, double2 ax, double2, double) {
+                      double2 res = make_double2(0, 0);
+                      if (in) {
+                          res = csub(b[e], ax);
+                          v[0] += res.x * res.x + res.y * res.y;
+                      }
+                      R[e] = res;
+                  },
+                  kb_phi(a, r));
+    }
+    double tot[1];
+    if (block_reduce_last<1>(v, a.parts, a.cnt, r, blockIdx.x + gridDim.x * blockIdx.z, gridDim.x * gridDim.z, tot) &&
+        threadIdx.x == 0)
+        fin_res64(os, tot);
+}
+
+// inverse diagonal of A (curl-curl diagonal, grad-div diagonal, i*dterm) for
+// the diagonal preconditioner, interior edges; zero on boundary edges
+template <typename T> __global__ void __launch_bounds__(kThreads) kcb_jacobi(KArgs<T> a)
+{
+    const int r = blockIdx.y;
+    if (!a.ost[r].active) return;
+    int i, j;
+    if (!col_of(a.cmap, a.g.nx, a.g.ny, i, j)) return;
+    const Geo<T> &g = a.g;
+    const size_t off = (size_t)r * a.stride;
+    const T wmu = c_wmu<T>(a.ost, r, a.dsgn);
+    const ColGeo<T> cg = col_geo(g, i, j);
+    C2<T> *J = a.jinv + off;
+    const int bx = i + g.nx * j, by = g.nXe + i + (g.nx + 1) * j, bz = g.nXe + g.nYe + i + (g.nx + 1) * j;
+    const int sxk = g.nx * (g.ny + 1), syk = (g.nx + 1) * g.ny, szk = (g.nx + 1) * (g.ny + 1);
+    const int bn = i + (g.nx + 1) * j, snj = g.nx + 1, snk = (g.nx + 1) * (g.ny + 1);
+    int k0, k1;
+    kb_range(g, k0, k1);
+    for (int k = k0; k < k1; k++) {
+        const PlaneGeo<T> pg = plane_geo(g, k);
+        const bool kin = k >= 1 && k <= g.nz - 1;
+        for (int comp = 0; comp < 3; comp++) {
+            const bool has = comp == 0 ? cg.hasX : comp == 1 ? cg.hasY : k < g.nz;
+            if (!has) continue;
+            const int e = comp == 0 ? bx + sxk * k : comp == 1 ? by + syk * k : bz + szk * k;
+            const bool in = comp == 0 ? (cg.intX && kin) : comp == 1 ? (cg.intY && kin) : cg.intZ;
+            C2<T> m = mk<T>(0, 0);
+            if (in) {
+                const T sg = a.sigma[e];
+                const T ve = comp == 0 ? cg.dxi * (cg.delYj * pg.delZk)
+                           : comp == 1 ? cg.dyj * (cg.delXi * pg.delZk) : pg.dzk * (cg.delXi * cg.delYj);
+                T dr = col_ccdiag(comp, cg, pg);
+                if (a.gd) {
+                    const int ns = bn + snk * k, ne = ns + (comp == 0 ? 1 : comp == 1 ? snj : snk);
+                    const T dfa = comp == 0 ? cg.delYj * pg.delZk : comp == 1 ? cg.delXi * pg.delZk : cg.delXi * cg.delYj;
+                    const T cs = a.gde[ns] ? sg : T(1), ce = a.gde[ne] ? sg : T(1);
+                    dr += dfa * dfa * (a.gdw[ns] * cs + a.gdw[ne] * ce);
+                }
+                const T di = wmu * sg * ve;
+                const T inv = T(1) / (dr * dr + di * di);
+                m = mk<T>(dr * inv, -di * inv);
+            }
+            J[e] = m;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
 static int zchunks(int nz, int ntiles, int nrhs)
@@ -395,6 +566,26 @@ template <typename T> void launch_col_prec(const ColArgs<T> &a, const C2<T> *in,
     counted(1);
     kc_prec<T><<<dim3(a.map.tiles, nrhs), kThreads, 0, s>>>(a, in, out);
 }
+template <typename T> void launch_colb_init(const KArgs<T> &a, int nrhs, cudaStream_t s)
+{
+    counted(1);
+    kcb_init<T><<<dim3(a.cmap.tiles, nrhs, zchunks(a.g.nz, a.cmap.tiles, nrhs)), kThreads, 0, s>>>(a);
+}
+template <typename T> void launch_colb_vt(const KArgs<T> &a, int which, int nrhs, cudaStream_t s)
+{
+    counted(1);
+    kcb_vt<T><<<dim3(a.cmap.tiles, nrhs, zchunks(a.g.nz, a.cmap.tiles, nrhs)), kThreads, 0, s>>>(a, which);
+}
+void launch_colb_res64(const KArgs<double> &a, int nrhs, cudaStream_t s)
+{
+    counted(1);
+    kcb_res64<<<dim3(a.cmap.tiles, nrhs, zchunks(a.g.nz, a.cmap.tiles, nrhs)), kThreads, 0, s>>>(a);
+}
+template <typename T> void launch_colb_jacobi(const KArgs<T> &a, int nrhs, cudaStream_t s)
+{
+    counted(1);
+    kcb_jacobi<T><<<dim3(a.cmap.tiles, nrhs, zchunks(a.g.nz, a.cmap.tiles, nrhs)), kThreads, 0, s>>>(a);
+}
 ColMapHost col_map(int nx, int ny)
 {
     ColMapHost m;
@@ -408,7 +599,10 @@ ColMapHost col_map(int nx, int ny)
     template void launch_zl_setup<T>(const ColArgs<T> &, int, cudaStream_t);                                          \
     template void launch_cocg_start<T>(const ColArgs<T> &, int, cudaStream_t);                                        \
     template void launch_cocg_iter<T>(const ColArgs<T> &, int, cudaStream_t, cudaEvent_t *);                         \
-    template void launch_col_prec<T>(const ColArgs<T> &, const C2<T> *, C2<T> *, int, cudaStream_t);
+    template void launch_col_prec<T>(const ColArgs<T> &, const C2<T> *, C2<T> *, int, cudaStream_t);          \
+    template void launch_colb_init<T>(const KArgs<T> &, int, cudaStream_t);                                     \
+    template void launch_colb_vt<T>(const KArgs<T> &, int, int, cudaStream_t);                                  \
+    template void launch_colb_jacobi<T>(const KArgs<T> &, int, cudaStream_t);
 INST(double)
 INST(float)
 

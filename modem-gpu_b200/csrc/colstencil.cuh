@@ -65,9 +65,14 @@ template <typename C> __device__ __forceinline__ C ldg_c(const C *p) { return __
 //   f(comp, e, interior, Ax, x_e, dterm)
 // where Ax is (A x)_e for interior edges (undefined otherwise), x_e the
 // input value and dterm = wmu * sigma_e * V_E the imaginary diagonal part.
+//
+// With phi non-null the grad-div term of the SP2 operator, DFA_e (phi_end -
+// phi_start) (GradDivSetup2, f90/3D_MT/FWD_SP2/modelOperator3D.f90:916-1008),
+// is added to every interior edge; phi holds the node potentials of x.
 template <typename T, typename F>
 __device__ __forceinline__ void col_march(const Geo<T> &g, const C2<T> *__restrict__ x, const T *__restrict__ sig,
-                                          int i, int j, int k0, int k1, T wmu, F &&f)
+                                          int i, int j, int k0, int k1, T wmu, F &&f,
+                                          const C2<T> *__restrict__ phi = nullptr)
 {
     using C = C2<T>;
     const ColGeo<T> cg = col_geo(g, i, j);
@@ -91,9 +96,14 @@ __device__ __forceinline__ void col_march(const Geo<T> &g, const C2<T> *__restri
         Y1 = ldg_c(x + by + syk * k0);
     }
     if (k0 >= 1) Z0 = ldg_c(x + bz + szk * (k0 - 1));
+    // node potentials phi(i, j, k) and phi(i, j, k+1) of the own node column
+    const int bn = i + (g.nx + 1) * j, snj = g.nx + 1, snk = (g.nx + 1) * (g.ny + 1);
+    C P0 = zero, P1 = zero;
+    if (phi) P0 = ldg_c(phi + bn + snk * k0);
     for (int k = k0; k < k1; k++) {
         const PlaneGeo<T> pg = plane_geo(g, k);
         const bool kin = k >= 1 && k <= g.nz - 1;
+        if (phi) P1 = (k < g.nz) ? ldg_c(phi + bn + snk * (k + 1)) : zero;
         X2 = (cg.hasX && k < g.nz) ? ldg_c(x + bx + sxk * (k + 1)) : zero;
         Y2 = (cg.hasY && k < g.nz) ? ldg_c(x + by + syk * (k + 1)) : zero;
         Z1 = (k < g.nz) ? ldg_c(x + bz + szk * k) : zero;
@@ -118,6 +128,7 @@ __device__ __forceinline__ void col_march(const Geo<T> &g, const C2<T> *__restri
                 out = csub(out, cscale(csub(fzp, fzm), cg.dxi * cg.delYj));
                 out.x -= dt * X1.y;
                 out.y += dt * X1.x;
+                if (phi) out = cadd(out, cscale(csub(ldg_c(phi + bn + snk * k + 1), P0), cg.delYj * pg.delZk));
             }
             f(0, e, in, out, X1, dt);
         }
@@ -132,7 +143,7 @@ __device__ __forceinline__ void col_march(const Geo<T> &g, const C2<T> *__restri
                 const int ez = bz + szk * k;  // Ez(i, j, k)
                 const int ex = bx + sxk * k;  // Ex(i, j, k)
                 const C zz = csub(cadd(csub(ldg_c(x + ez + szj), Z1), Z0), ldg_c(x + ez + szj - szk));
-                const C xx = csub(cadd(csub(ldg_c(x + ex + sxj), ldg_c(x + ex)), ldg_c(x + ex - 1)), ldg_c(x + ex - 1 + sxj));
+                const C xx = csub(cadd(csub(ldg_c(x + ex + sxj), X1), ldg_c(x + ex - 1)), ldg_c(x + ex - 1 + sxj));
                 const C fzp = cscale(csub(Y2, Y1), pg.rdzk);
                 const C fzm = cscale(csub(Y1, Y0), pg.rdzkm1);
                 const C fxp = cscale(csub(ldg_c(x + e + 1), Y1), cg.rdxi);
@@ -142,6 +153,7 @@ __device__ __forceinline__ void col_march(const Geo<T> &g, const C2<T> *__restri
                 out = csub(out, cscale(csub(fxp, fxm), cg.dyj * pg.delZk));
                 out.x -= dt * Y1.y;
                 out.y += dt * Y1.x;
+                if (phi) out = cadd(out, cscale(csub(ldg_c(phi + bn + snk * k + snj), P0), cg.delXi * pg.delZk));
             }
             f(1, e, in, out, Y1, dt);
         }
@@ -155,7 +167,7 @@ __device__ __forceinline__ void col_march(const Geo<T> &g, const C2<T> *__restri
             if (in) {
                 const int ex = bx + sxk * k;  // Ex(i, j, k)
                 const int ey = by + syk * k;  // Ey(i, j, k)
-                const C xx = csub(cadd(csub(ldg_c(x + ex + sxk), ldg_c(x + ex)), ldg_c(x + ex - 1)), ldg_c(x + ex - 1 + sxk));
+                const C xx = csub(cadd(csub(X2, X1), ldg_c(x + ex - 1)), ldg_c(x + ex - 1 + sxk));
                 const C yy = csub(cadd(csub(Y2, Y1), ldg_c(x + ey - syj)), ldg_c(x + ey - syj + syk));
                 const C fxp = cscale(csub(ldg_c(x + e + 1), Z1), cg.rdxi);
                 const C fxm = cscale(csub(Z1, ldg_c(x + e - 1)), cg.rdxim1);
@@ -166,12 +178,14 @@ __device__ __forceinline__ void col_march(const Geo<T> &g, const C2<T> *__restri
                 out = csub(out, cscale(csub(fyp, fym), pg.dzk * cg.delXi));
                 out.x -= dt * Z1.y;
                 out.y += dt * Z1.x;
+                if (phi) out = cadd(out, cscale(csub(P1, P0), cg.delXi * cg.delYj));
             }
             f(2, e, in, out, Z1, dt);
         }
         X0 = X1; X1 = X2;
         Y0 = Y1; Y1 = Y2;
         Z0 = Z1;
+        P0 = P1;
     }
 }
 

@@ -10,6 +10,7 @@
 #include <atomic>
 
 #include "common.cuh"
+#include "finalize.cuh"
 #include "kernels.h"
 
 namespace mt3d {
@@ -195,39 +196,7 @@ template <typename T> __global__ void __launch_bounds__(kThreads) kb_init(KArgs<
     }
     double tot[2];
     if (block_reduce_last<2>(v, a.parts, a.cnt, r, blockIdx.x, gridDim.x, tot) && threadIdx.x == 0) {
-        const double bnorm = sqrt(tot[0]), rnorm = sqrt(tot[1]);
-        double *rerr = a.rerr + (size_t)r * a.rerr_stride;
-        st.iter = 0;
-        st.maxit = a.maxit;
-        st.xcur = 0;
-        st.xbest = 0;
-        st.imin = 0;
-        st.first = 1;
-        st.pad = 0;
-        st.bnorm = bnorm;
-        st.rnorm = rnorm;
-        st.rnormin = rnorm;
-        st.btol = (a.inner ? a.ost[r].tol_inner : a.ost[r].tol) * bnorm;
-        st.rho1 = {1.0, 0.0};
-        st.omega = {1.0, 0.0};
-        st.alpha = {0.0, 0.0};
-        st.rho = {tot[1], 0.0};
-        if (!isfinite(bnorm)) {
-            st.status = KS_NAN;
-        } else if (bnorm == 0.0) {
-            st.status = KS_CONVERGED;  // zero right-hand side: zero solution
-            st.xbest = -1;
-            st.iter = 1;
-            rerr[0] = 0.0;
-        } else if (rnorm <= st.btol) {
-            st.status = KS_CONVERGED;  // the first guess is already good enough
-            st.iter = 1;
-            rerr[0] = rnorm / bnorm;
-        } else {
-            st.status = KS_RUNNING;
-            rerr[0] = rnorm / bnorm;
-            if (tot[1] == 0.0) st.status = KS_BREAKDOWN;
-        }
+        fin_init(st, tot, a.rerr + (size_t)r * a.rerr_stride, a.maxit, a.inner ? a.ost[r].tol_inner : a.ost[r].tol);
     }
 }
 
@@ -256,6 +225,10 @@ template <typename T> __global__ void __launch_bounds__(kThreads) kb_p(KArgs<T> 
         }
         a.p[off + e] = p;
         if (a.pc_ext) continue;
+        if (a.jinv) {
+            a.ph[off + e] = cmul(a.jinv[off + e], p);
+            continue;
+        }
         EdgeIdx q = edge_decode(g, e);
         C2<T> ph = mk<T>(0, 0);
         if (edge_interior(g, q)) {
@@ -291,11 +264,7 @@ template <typename T> __global__ void __launch_bounds__(kThreads) kb_v(KArgs<T> 
     }
     double tot[2];
     if (block_reduce_last<2>(v, a.parts, a.cnt, r, blockIdx.x, gridDim.x, tot) && threadIdx.x == 0) {
-        cd rtv = {tot[0], tot[1]};
-        if (!cd_finite(rtv)) { st.status = KS_NAN; return; }
-        if (cd_zero(rtv)) { st.status = KS_BREAKDOWN; return; }
-        st.alpha = cd_div(st.rho, rtv);
-        if (cd_zero(st.alpha)) st.status = KS_BREAKDOWN;
+        fin_v(st, tot);
     }
 }
 
@@ -314,6 +283,10 @@ template <typename T> __global__ void __launch_bounds__(kThreads) kb_s(KArgs<T> 
         C2<T> s = csub(a.r[off + e], cmul(al, a.v[off + e]));
         a.s[off + e] = s;
         if (a.pc_ext) continue;
+        if (a.jinv) {
+            a.sh[off + e] = cmul(a.jinv[off + e], s);
+            continue;
+        }
         EdgeIdx q = edge_decode(g, e);
         C2<T> sh = mk<T>(0, 0);
         if (edge_interior(g, q)) {
@@ -350,11 +323,7 @@ template <typename T> __global__ void __launch_bounds__(kThreads) kb_t(KArgs<T> 
     }
     double tot[3];
     if (block_reduce_last<3>(v, a.parts, a.cnt, r, blockIdx.x, gridDim.x, tot) && threadIdx.x == 0) {
-        if (!isfinite(tot[0]) || !isfinite(tot[1]) || !isfinite(tot[2])) { st.status = KS_NAN; return; }
-        if (tot[2] == 0.0) { st.status = KS_BREAKDOWN; return; }
-        cd ts = {tot[0], tot[1]};
-        st.omega = {ts.re / tot[2], ts.im / tot[2]};
-        if (cd_zero(st.omega)) st.status = KS_BREAKDOWN;
+        fin_t(st, tot);
     }
 }
 
@@ -802,9 +771,7 @@ __global__ void __launch_bounds__(kThreads) km_res64(KArgs<double> a, double tol
     }
     double tot[1];
     if (block_reduce_last<1>(v, a.parts, a.cnt, r, blockIdx.x, gridDim.x, tot) && threadIdx.x == 0) {
-        const double rn = sqrt(tot[0]);
-        os.relres = rn / os.bnorm64;
-        os.scale = rn > 0.0 ? 1.0 / rn : 0.0;
+        fin_res64(os, tot);
     }
 }
 
@@ -1090,7 +1057,9 @@ template <typename T> void launch_bicg_init(const KArgs<T> &a, int nrhs, cudaStr
 {
     counted(1);
     if (a.gd) launch_gd_phi(a, a.x0, a.phi, 0, nrhs, s);
-    kb_init<T><<<dim3(a.nblk, nrhs), kThreads, 0, s>>>(a);
+    if (a.jinv) launch_colb_jacobi(a, nrhs, s);
+    if (a.colstencil) launch_colb_init(a, nrhs, s);
+    else kb_init<T><<<dim3(a.nblk, nrhs), kThreads, 0, s>>>(a);
 }
 template <typename T>
 void launch_bicg_iter(const KArgs<T> &a, int nrhs, cudaStream_t s, cudaEvent_t *ev, const ColArgs<T> *pc)
@@ -1101,13 +1070,15 @@ void launch_bicg_iter(const KArgs<T> &a, int nrhs, cudaStream_t s, cudaEvent_t *
     if (pc) launch_col_prec(*pc, a.p, a.ph, nrhs, s);
     if (a.gd) launch_gd_phi(a, a.ph, a.phi, 0, nrhs, s);
     if (ev) cudaEventRecord(ev[0], s);
-    kb_v<T><<<grid, kThreads, 0, s>>>(a);
+    if (a.colstencil) launch_colb_vt(a, 0, nrhs, s);
+    else kb_v<T><<<grid, kThreads, 0, s>>>(a);
     if (ev) cudaEventRecord(ev[1], s);
     kb_s<T><<<grid, kThreads, 0, s>>>(a);
     if (pc) launch_col_prec(*pc, a.s, a.sh, nrhs, s);
     if (a.gd) launch_gd_phi(a, a.sh, a.phi, 0, nrhs, s);
     if (ev) cudaEventRecord(ev[2], s);
-    kb_t<T><<<grid, kThreads, 0, s>>>(a);
+    if (a.colstencil) launch_colb_vt(a, 1, nrhs, s);
+    else kb_t<T><<<grid, kThreads, 0, s>>>(a);
     if (ev) cudaEventRecord(ev[3], s);
     kb_xr<T><<<grid, kThreads, 0, s>>>(a);
 }
@@ -1134,7 +1105,8 @@ void launch_res64(const KArgs<double> &a, int nrhs, cudaStream_t s)
 {
     counted(1);
     if (a.gd) launch_gd_phi(a, a.x0, a.phi, 0, nrhs, s);
-    km_res64<<<dim3(a.nblk, nrhs), kThreads, 0, s>>>(a, 0.0);
+    if (a.colstencil) launch_colb_res64(a, nrhs, s);
+    else km_res64<<<dim3(a.nblk, nrhs), kThreads, 0, s>>>(a, 0.0);
 }
 static int grid_for(long n) { return (int)std::min<long>((n + kThreads - 1) / kThreads, 148L * 16); }
 void launch_cast(const OuterState *ost, int nE, size_t stride, const double2 *r64, float2 *b32, float2 *x32, int nrhs,

@@ -4,6 +4,13 @@
 
 namespace mt3d {
 
+// tiles of kColX x kColY (i, j) columns for the column-marching kernels
+struct ColMap {
+    int tiles_x, tiles;
+};
+using ColMapHost = ColMap;
+ColMapHost col_map(int nx, int ny);
+
 // arguments of the edge-vector Krylov kernels (one precision T)
 template <typename T> struct KArgs {
     Geo<T> g;
@@ -28,6 +35,10 @@ template <typename T> struct KArgs {
     const T *gdw;
     const unsigned char *gde;
     C2<T> *phi;
+    // column-marching stencil kernels and the precomputed inverse diagonal
+    int colstencil;
+    ColMap cmap;
+    C2<T> *jinv;
     double dsgn;  // ISIGN (-1) for A, +1 for the conjugate transpose
 };
 
@@ -53,12 +64,6 @@ struct DArgs {
     double tol;
 };
 
-// column-marching kernels (colkernels.cu)
-struct ColMap {
-    int tiles_x, tiles;  // tiles of kColX x kColY columns
-};
-using ColMapHost = ColMap;
-ColMapHost col_map(int nx, int ny);
 
 template <typename T> struct ColArgs {
     Geo<T> g;
@@ -80,6 +85,10 @@ template <typename T> void launch_col_apply(const ColArgs<T> &a, const C2<T> *x,
 template <typename T> void launch_zl_setup(const ColArgs<T> &a, int nrhs, cudaStream_t s);
 template <typename T> void launch_cocg_start(const ColArgs<T> &a, int nrhs, cudaStream_t s);
 template <typename T> void launch_col_prec(const ColArgs<T> &a, const C2<T> *in, C2<T> *out, int nrhs, cudaStream_t s);
+template <typename T> void launch_colb_init(const KArgs<T> &a, int nrhs, cudaStream_t s);
+template <typename T> void launch_colb_vt(const KArgs<T> &a, int which, int nrhs, cudaStream_t s);
+void launch_colb_res64(const KArgs<double> &a, int nrhs, cudaStream_t s);
+template <typename T> void launch_colb_jacobi(const KArgs<T> &a, int nrhs, cudaStream_t s);
 template <typename T> void launch_cocg_iter(const ColArgs<T> &a, int nrhs, cudaStream_t s, cudaEvent_t *ev = nullptr);
 
 template <typename T>

@@ -405,7 +405,7 @@ int Solver::ensure_workspace(int nrhs, int precision)
     // release everything first so a precision change does not hold both sets
     DevBuf *all[] = {&w.b, &w.X, &w.x1, &w.r, &w.rt, &w.p, &w.v, &w.ph, &w.s, &w.sh, &w.t, &w.bc, &w.tmp,
                      &w.f_b, &w.f_x0, &w.f_x1, &w.f_r, &w.f_rt, &w.f_p, &w.f_v, &w.f_ph, &w.f_s, &w.f_sh, &w.f_t,
-                     &w.px, &w.pr, &w.pp, &w.pq, &w.phi0, &w.zm, &w.zc, &w.f_zm, &w.f_zc, &w.phi64, &w.phi32};
+                     &w.px, &w.pr, &w.pp, &w.pq, &w.phi0, &w.zm, &w.zc, &w.f_zm, &w.f_zc, &w.phi64, &w.phi32, &w.jinv64, &w.jinv32};
     for (DevBuf *d : all) d->release();
     int err = 0;
     err |= w.b.alloc(e64) | w.X.alloc(e64) | w.bc.alloc(e64) | w.tmp.alloc(e64);
@@ -413,10 +413,12 @@ int Solver::ensure_workspace(int nrhs, int precision)
         DevBuf *v64[] = {&w.x1, &w.r, &w.rt, &w.p, &w.v, &w.ph, &w.s, &w.sh, &w.t};
         for (DevBuf *d : v64) err |= d->alloc(e64);
         if (ctl.solver == 3) err |= w.zm.alloc(e64) | w.zc.alloc(e64);
+        if (ctl.solver == 1) err |= w.jinv64.alloc(e64);
     } else {
         DevBuf *v32[] = {&w.f_b, &w.f_x0, &w.f_x1, &w.f_r, &w.f_rt, &w.f_p, &w.f_v, &w.f_ph, &w.f_s, &w.f_sh, &w.f_t};
         for (DevBuf *d : v32) err |= d->alloc(e32);
         if (ctl.solver == 3) err |= w.f_zm.alloc(e32) | w.f_zc.alloc(e32);
+        if (ctl.solver == 1) err |= w.jinv32.alloc(e32);
     }
     if (ctl.formulation == 0) {
         DevBuf *nv[] = {&w.px, &w.pr, &w.pp, &w.pq, &w.phi0};
@@ -472,6 +474,9 @@ template <> KArgs<double> Solver::kargs<double>(int nrhs, int)
     a.maxit = ctl.IterPerDivCor;
     a.inner = 0;
     a.dsgn = -1.0;
+    a.colstencil = 1;
+    a.cmap = col_map(nx, ny);
+    a.jinv = ctl.solver == 1 ? w.jinv64.as<double2>() : nullptr;
     if (ctl.formulation == 1) {
         a.sigma = sigs64_.as<double>();
         a.gd = 1;
@@ -503,6 +508,9 @@ template <> KArgs<float> Solver::kargs<float>(int nrhs, int)
     a.maxit = ctl.IterPerDivCor;
     a.inner = 1;
     a.dsgn = -1.0;
+    a.colstencil = 1;
+    a.cmap = col_map(nx, ny);
+    a.jinv = ctl.solver == 1 ? w.jinv32.as<float2>() : nullptr;
     if (ctl.formulation == 1) {
         a.sigma = sigs32_.as<float>();
         a.gd = 1;

@@ -57,6 +57,7 @@ struct Workspace {
     DevBuf px, pr, pp, pq, phi0;
     DevBuf zm, zc, f_zm, f_zc;  // z-line pivots for BiCGStab + z-line
     DevBuf phi64, phi32;        // grad-div node potentials
+    DevBuf jinv64, jinv32;      // inverse diagonal (diagonal preconditioner)
     DevBuf bst, pst, ost, parts, cnt, rerr, dcrerr;
 };
 

@@ -181,7 +181,7 @@ class Solver:
                          allow=(0, 1, 2, 3))
         return e, st, rc
 
-    def fwdsolve_batch_device(self, omegas, e_ptr, bc_ptr=None, src_ptr=None, trans=None):
+    def fwdsolve_batch_device(self, omegas, e_ptr, bc_ptr=None, src_ptr=None, trans=None):  # noqa: D401
         """Batched solve on device-resident fields: e_ptr, bc_ptr, src_ptr are
         device addresses (e.g. torch tensor data_ptr()) of nrhs full edge
         vectors each (complex128)."""
