@@ -7,6 +7,12 @@
  * cpu_baseline leg of bench.py may load the library built from it; the product
  * never calls it.
  *
+ * Parity unpinned against the reference's own outputs: the reference cannot
+ * be built here (Fortran, no compiler) and its forward fixture
+ * (unit_testing/3D/CylinderModel_1per.dat) needs the 2-D boundary solver and
+ * the impedance functional, which this file does not restate.  The tests pin
+ * it by a closed-form layered solution, direct solves and operator identities.
+ *
  * Every routine cites the reference routine it restates (paths relative to the
  * ModEM-GPU source tree).  Indices in the loops are kept 1-based, as in the
  * Fortran, through the IEX/IEY/IEZ/IND/ICL macros, so that each loop can be

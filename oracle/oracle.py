@@ -8,8 +8,12 @@ The oracle restates ModEM's matrix-free 3D-MT forward solver
 (f90/3D_MT/FWD/modelOperator3D.f90, f90/3D_MT/FWD/EMsolve3D.f90,
 f90/3D_MT/FWD/solver.f90) and the sensitivity glue
 (f90/3D_MT/SolverSens.f90:63-116, f90/3D_MT/modelParam/ModelMap.inc).
-Its pinning against the reference's own fixtures is described in the
-tests that load it (tests/test_oracle_*.py).
+Parity unpinned: the reference (Fortran) cannot be built here and its one
+forward fixture (unit_testing/3D/CylinderModel_1per.dat, impedances) needs
+the 2-D boundary solver and the impedance functional, which are not
+restated.  The oracle is pinned instead by a closed-form layered solution,
+scipy direct solves, the CC-DC/SP2 equivalence and operator identities
+(tests/test_oracle.py).
 """
 from __future__ import annotations
 
