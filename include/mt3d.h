@@ -123,6 +123,26 @@ MT3D_API int mt3d_interior_index(mt3d_handle h, int32_t *edgei);
  * adjt != 0 the conjugate-transposed operator is applied. */
 MT3D_API int mt3d_mult_aii(mt3d_handle h, int adjt, const double *x, double *y);
 
+/* The product of mt3d_mult_aii on DEVICE vectors, allocating no device
+ * memory.  This entry has no counterpart in the reference.  It is meant for
+ * callers that drive the operator from their own iterative loop on vectors
+ * they already hold on the GPU and that cannot allocate per call: a memory
+ * pool or caching allocator that owns all free device memory, or a loop in
+ * which the device-wide synchronisation of cudaMalloc/cudaFree is unwanted.
+ *
+ * x and y are interior vectors (nEi complex doubles, 16-byte aligned) in
+ * device memory of the handle's device.  The work is only enqueued on the
+ * handle's stream (mt3d_set_stream); y is ready when that stream reaches
+ * this point.  The scratch (two full edge vectors, the grad-div node
+ * potentials and a state record) is one fixed 16 MiB device array per
+ * device: grids whose 256 + 16 * (2 nE + nN) bytes exceed it (about 52^3
+ * cells) are rejected with MT3D_INVALID_ARGUMENT.  The first call on a
+ * device looks up the scratch address (cudaGetSymbolAddress); make that first
+ * call before any stream capture.  The scratch is shared by all handles on a
+ * device, so calls whose GPU work overlaps in time (different streams,
+ * handles or host threads) race; calls on one stream are safe. */
+MT3D_API int mt3d_mult_aii_device_noalloc(mt3d_handle h, int adjt, const double *x, double *y);
+
 /* One Krylov call on the interior system A x = b: BICG(b, x, KSSiter,
  * device_id) -> cuBiCG (f90/3D_MT/FWD_SP2/EMsolve3D.f90:369-387,
  * f90/3D_MT/FWD_SP2/solver.f90:931-2009; algorithm of BICG,

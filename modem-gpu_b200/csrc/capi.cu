@@ -164,6 +164,11 @@ int mt3d_mult_aii(mt3d_handle h, int adjt, const double *x, double *y)
     return wrap(h, [&] { return h->s.mult_aii(adjt, x, y); });
 }
 
+int mt3d_mult_aii_device_noalloc(mt3d_handle h, int adjt, const double *x, double *y)
+{
+    return wrap(h, [&] { return h->s.mult_aii_noalloc(adjt, x, y); });
+}
+
 int mt3d_bicg(mt3d_handle h, const double *b, double *x, int maxit, double tol, int *niter, double *rerr, int *failed)
 {
     return wrap(h, [&] { return h->s.bicg(b, x, maxit, tol, niter, rerr, failed); });

@@ -68,6 +68,7 @@ class Solver {
     int update_cond(const double *m_earth, double airCond);
     int update_freq(double omega);
     int mult_aii(int adjt, const double *x, double *y);
+    int mult_aii_noalloc(int adjt, const double *x, double *y);  // device vectors, fixed scratch
     int bicg(const double *b, double *x, int maxit, double tol, int *niter, double *rerr, int *failed);
     int solve(int nrhs, const double *omegas, const int *trans, const double *bc, const double *src, double *e,
               int *status, bool device = false);

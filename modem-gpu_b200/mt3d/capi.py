@@ -24,7 +24,8 @@ FORM_CCDC, FORM_CCGD = 0, 1
 
 #: every symbol include/mt3d.h declares
 EXPORTS = ["mt3d_version", "mt3d_device_count", "mt3d_create", "mt3d_destroy", "mt3d_set_control", "mt3d_update_cond",
-           "mt3d_update_freq", "mt3d_set_formulation", "mt3d_sizes", "mt3d_interior_index", "mt3d_mult_aii", "mt3d_bicg", "mt3d_fwdsolve",
+           "mt3d_update_freq", "mt3d_set_formulation", "mt3d_sizes", "mt3d_interior_index", "mt3d_mult_aii",
+           "mt3d_mult_aii_device_noalloc", "mt3d_bicg", "mt3d_fwdsolve",
            "mt3d_fwdsolve_batch", "mt3d_fwdsolve_batch_device", "mt3d_set_stream", "mt3d_profile",
            "mt3d_kernel_time", "mt3d_get_diag", "mt3d_get_batch_diag", "mt3d_pmult_t", "mt3d_launch_counter", "mt3d_last_error"]
 
@@ -60,6 +61,7 @@ def load(path: str = LIB_PATH):
     L.mt3d_sizes.argtypes = [P, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     L.mt3d_interior_index.argtypes = [P, C.POINTER(C.c_int32)]
     L.mt3d_mult_aii.argtypes = [P, I, D, D]
+    L.mt3d_mult_aii_device_noalloc.argtypes = [P, I, C.c_void_p, C.c_void_p]
     L.mt3d_bicg.argtypes = [P, D, D, I, C.c_double, IP, D, IP]
     L.mt3d_fwdsolve.argtypes = [P, I, D, D, D]
     L.mt3d_fwdsolve_batch.argtypes = [P, I, D, IP, D, D, D, IP]
@@ -151,6 +153,12 @@ class Solver:
         y = np.zeros(self.nEi, np.complex128)
         self._check(self.L.mt3d_mult_aii(self.h, int(adjt), _d(x), _d(y)))
         return y
+
+    def mult_aii_device_noalloc(self, x_ptr, y_ptr, adjt=False):
+        """y = A x on device interior vectors (nEi complex128 each, given by
+        device address, e.g. a torch tensor's data_ptr()); enqueued on the
+        handle's stream, no device allocation."""
+        self._check(self.L.mt3d_mult_aii_device_noalloc(self.h, int(adjt), C.c_void_p(x_ptr), C.c_void_p(y_ptr)))
 
     def bicg(self, b, x0, maxit, tol):
         b = np.ascontiguousarray(b, np.complex128)
