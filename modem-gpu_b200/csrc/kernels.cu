@@ -1055,29 +1055,39 @@ template void launch_gd_phi<float>(const KArgs<float> &, const float2 *, float2 
 template void launch_gd_add<double>(const KArgs<double> &, double2 *, const double2 *, int, cudaStream_t);
 template <typename T> void launch_bicg_init(const KArgs<T> &a, int nrhs, cudaStream_t s)
 {
-    counted(1);
-    if (a.gd) launch_gd_phi(a, a.x0, a.phi, 0, nrhs, s);
     if (a.jinv) launch_colb_jacobi(a, nrhs, s);
-    if (a.colstencil) launch_colb_init(a, nrhs, s);
-    else kb_init<T><<<dim3(a.nblk, nrhs), kThreads, 0, s>>>(a);
+    if (a.colstencil == 2) {
+        launch_stage_init(a, nrhs, s);
+        return;
+    }
+    if (a.gd) launch_gd_phi(a, a.x0, a.phi, 0, nrhs, s);
+    if (a.colstencil) {
+        launch_colb_init(a, nrhs, s);
+    } else {
+        counted(1);
+        kb_init<T><<<dim3(a.nblk, nrhs), kThreads, 0, s>>>(a);
+    }
 }
 template <typename T>
 void launch_bicg_iter(const KArgs<T> &a, int nrhs, cudaStream_t s, cudaEvent_t *ev, const ColArgs<T> *pc)
 {
-    counted(5);
+    counted(a.colstencil ? 3 : 5);
     dim3 grid(a.nblk, nrhs);
+    const bool staged = a.colstencil == 2;
     kb_p<T><<<grid, kThreads, 0, s>>>(a);
     if (pc) launch_col_prec(*pc, a.p, a.ph, nrhs, s);
-    if (a.gd) launch_gd_phi(a, a.ph, a.phi, 0, nrhs, s);
+    if (a.gd && !staged) launch_gd_phi(a, a.ph, a.phi, 0, nrhs, s);
     if (ev) cudaEventRecord(ev[0], s);
-    if (a.colstencil) launch_colb_vt(a, 0, nrhs, s);
+    if (staged) launch_stage_vt(a, 0, nrhs, s);
+    else if (a.colstencil) launch_colb_vt(a, 0, nrhs, s);
     else kb_v<T><<<grid, kThreads, 0, s>>>(a);
     if (ev) cudaEventRecord(ev[1], s);
     kb_s<T><<<grid, kThreads, 0, s>>>(a);
     if (pc) launch_col_prec(*pc, a.s, a.sh, nrhs, s);
-    if (a.gd) launch_gd_phi(a, a.sh, a.phi, 0, nrhs, s);
+    if (a.gd && !staged) launch_gd_phi(a, a.sh, a.phi, 0, nrhs, s);
     if (ev) cudaEventRecord(ev[2], s);
-    if (a.colstencil) launch_colb_vt(a, 1, nrhs, s);
+    if (staged) launch_stage_vt(a, 1, nrhs, s);
+    else if (a.colstencil) launch_colb_vt(a, 1, nrhs, s);
     else kb_t<T><<<grid, kThreads, 0, s>>>(a);
     if (ev) cudaEventRecord(ev[3], s);
     kb_xr<T><<<grid, kThreads, 0, s>>>(a);
@@ -1103,10 +1113,17 @@ void launch_norm_b(const KArgs<double> &a, int nrhs, cudaStream_t s)
 }
 void launch_res64(const KArgs<double> &a, int nrhs, cudaStream_t s)
 {
-    counted(1);
+    if (a.colstencil == 2) {
+        launch_stage_res64(a, nrhs, s);
+        return;
+    }
     if (a.gd) launch_gd_phi(a, a.x0, a.phi, 0, nrhs, s);
-    if (a.colstencil) launch_colb_res64(a, nrhs, s);
-    else km_res64<<<dim3(a.nblk, nrhs), kThreads, 0, s>>>(a, 0.0);
+    if (a.colstencil) {
+        launch_colb_res64(a, nrhs, s);
+    } else {
+        counted(1);
+        km_res64<<<dim3(a.nblk, nrhs), kThreads, 0, s>>>(a, 0.0);
+    }
 }
 static int grid_for(long n) { return (int)std::min<long>((n + kThreads - 1) / kThreads, 148L * 16); }
 void launch_cast(const OuterState *ost, int nE, size_t stride, const double2 *r64, float2 *b32, float2 *x32, int nrhs,

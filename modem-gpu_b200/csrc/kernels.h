@@ -34,8 +34,10 @@ template <typename T> struct KArgs {
     int gd;
     const T *gdw;
     const unsigned char *gde;
+    const T *gdn;  // node weight with the earth flag as its sign (staged kernels)
     C2<T> *phi;
-    // column-marching stencil kernels and the precomputed inverse diagonal
+    // stencil kernels: 0 flat, 1 column-marching, 2 shared-memory staged
+    // (grad-div potentials formed inside); the precomputed inverse diagonal
     int colstencil;
     ColMap cmap;
     C2<T> *jinv;
@@ -89,6 +91,11 @@ template <typename T> void launch_colb_init(const KArgs<T> &a, int nrhs, cudaStr
 template <typename T> void launch_colb_vt(const KArgs<T> &a, int which, int nrhs, cudaStream_t s);
 void launch_colb_res64(const KArgs<double> &a, int nrhs, cudaStream_t s);
 template <typename T> void launch_colb_jacobi(const KArgs<T> &a, int nrhs, cudaStream_t s);
+// shared-memory staged stencil kernels (colstencil == 2; grad-div potentials fused)
+template <typename T> void launch_stage_init(const KArgs<T> &a, int nrhs, cudaStream_t s);
+template <typename T> void launch_stage_vt(const KArgs<T> &a, int which, int nrhs, cudaStream_t s);
+void launch_stage_res64(const KArgs<double> &a, int nrhs, cudaStream_t s);
+int stage_chunks(int nz, int tiles, int nrhs, int resident);
 template <typename T> void launch_cocg_iter(const ColArgs<T> &a, int nrhs, cudaStream_t s, cudaEvent_t *ev = nullptr);
 
 template <typename T>

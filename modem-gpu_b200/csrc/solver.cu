@@ -349,16 +349,23 @@ int Solver::update_cond(const double *m_earth, double airCond)
             }
     std::vector<float> sigf(sig.begin(), sig.end());
     std::vector<float> sigsf(sig_sp2.begin(), sig_sp2.end()), gdwf(gdw.begin(), gdw.end());
+    // node weight with the earth flag as its sign, for the staged stencil kernels
+    std::vector<double> gdn(nN);
+    for (int64_t n = 0; n < nN; n++) gdn[n] = gde[n] ? -gdw[n] : gdw[n];
+    std::vector<float> gdnf(gdn.begin(), gdn.end());
     int rc;
     if (sig64_.alloc(nE * sizeof(double)) || sig32_.alloc(nE * sizeof(float)) || coef_.alloc(coef.size() * sizeof(double)) ||
         sigs64_.alloc(nE * sizeof(double)) || sigs32_.alloc(nE * sizeof(float)) || gdw64_.alloc(nN * sizeof(double)) ||
-        gdw32_.alloc(nN * sizeof(float)) || gde_.alloc(nN))
+        gdw32_.alloc(nN * sizeof(float)) || gde_.alloc(nN) || gdn64_.alloc(nN * sizeof(double)) ||
+        gdn32_.alloc(nN * sizeof(float)))
         return fail(8, "mt3d_update_cond: out of device memory");
     cudaMemcpyAsync(sigs64_.as<void>(), sig_sp2.data(), nE * sizeof(double), cudaMemcpyHostToDevice, stream_);
     cudaMemcpyAsync(sigs32_.as<void>(), sigsf.data(), nE * sizeof(float), cudaMemcpyHostToDevice, stream_);
     cudaMemcpyAsync(gdw64_.as<void>(), gdw.data(), nN * sizeof(double), cudaMemcpyHostToDevice, stream_);
     cudaMemcpyAsync(gdw32_.as<void>(), gdwf.data(), nN * sizeof(float), cudaMemcpyHostToDevice, stream_);
     cudaMemcpyAsync(gde_.as<void>(), gde.data(), nN, cudaMemcpyHostToDevice, stream_);
+    cudaMemcpyAsync(gdn64_.as<void>(), gdn.data(), nN * sizeof(double), cudaMemcpyHostToDevice, stream_);
+    cudaMemcpyAsync(gdn32_.as<void>(), gdnf.data(), nN * sizeof(float), cudaMemcpyHostToDevice, stream_);
     if ((rc = check(cudaMemcpyAsync(sig64_.as<void>(), sig.data(), nE * sizeof(double), cudaMemcpyHostToDevice, stream_), "copy sigma")))
         return rc;
     if ((rc = check(cudaMemcpyAsync(sig32_.as<void>(), sigf.data(), nE * sizeof(float), cudaMemcpyHostToDevice, stream_), "copy sigma")))
@@ -474,7 +481,7 @@ template <> KArgs<double> Solver::kargs<double>(int nrhs, int)
     a.maxit = ctl.IterPerDivCor;
     a.inner = 0;
     a.dsgn = -1.0;
-    a.colstencil = 1;
+    a.colstencil = 2;
     a.cmap = col_map(nx, ny);
     a.jinv = ctl.solver == 1 ? w.jinv64.as<double2>() : nullptr;
     if (ctl.formulation == 1) {
@@ -482,6 +489,7 @@ template <> KArgs<double> Solver::kargs<double>(int nrhs, int)
         a.gd = 1;
         a.gdw = gdw64_.as<double>();
         a.gde = gde_.as<unsigned char>();
+        a.gdn = gdn64_.as<double>();
         a.phi = w.phi64.as<double2>();
         a.restart = 120;
     }
@@ -508,7 +516,7 @@ template <> KArgs<float> Solver::kargs<float>(int nrhs, int)
     a.maxit = ctl.IterPerDivCor;
     a.inner = 1;
     a.dsgn = -1.0;
-    a.colstencil = 1;
+    a.colstencil = 2;
     a.cmap = col_map(nx, ny);
     a.jinv = ctl.solver == 1 ? w.jinv32.as<float2>() : nullptr;
     if (ctl.formulation == 1) {
@@ -516,6 +524,7 @@ template <> KArgs<float> Solver::kargs<float>(int nrhs, int)
         a.gd = 1;
         a.gdw = gdw32_.as<float>();
         a.gde = gde_.as<unsigned char>();
+        a.gdn = gdn32_.as<float>();
         a.phi = w.phi32.as<float2>();
         a.restart = 120;
     }
@@ -939,6 +948,8 @@ int Solver::solve(int nrhs, const double *omegas, const int *trans, const double
                 o.active = 0;
             }
         }
+        // right-hand sides that finished in this cycle sit out the next one
+        push_state();
     }
     // true relative residual of the returned interior field (all right-hand sides)
     for (auto &o : os) { o.active = 1; o.dc_run = 0; }

@@ -113,7 +113,7 @@ class Solver {
     Geo<double> g64_{};
     Geo<float> g32_{};
     DevBuf tab64_, tab32_, sig64_, sig32_, coef_, edgei_d_;
-    DevBuf sigs64_, sigs32_, gdw64_, gdw32_, gde_;  // grad-div (SP2) data
+    DevBuf sigs64_, sigs32_, gdw64_, gdw32_, gde_, gdn64_, gdn32_;  // grad-div (SP2) data
     Workspace ws_;
     std::vector<double> dx_, dy_, dz_, delX_, delY_, delZ_;
 };
