@@ -1,17 +1,27 @@
 #!/usr/bin/env python
 """Throughput of the 3D-MT forward + adjoint solve on B200 GPUs.
 
-One step = every right-hand side of the workload solved to a relative residual
-of 1e-7 of the FP64 system: the forward solves (all frequencies x 2
-polarisations, plane-wave boundary data) and the adjoint (transposed) solves
-(all frequencies x 2 polarisations, synthetic receiver sources), each batch in
-one call of the C ABI.  The metric is solves/s over all ranks.
+Workload (default "combined"): the 200x200x100 model (12 air + 88 earth
+layers, seeded Gaussian random field of log10 resistivity), 16 frequencies
+log-spaced 1e-4..1e2 Hz, 2 polarisations, forward solves (plane-wave boundary
+data) and adjoint (transposed) solves (synthetic receiver sources on a 20x20
+array) -- 64 right-hand sides.  One step solves 8 of them in one batched call
+of the C ABI: frequencies f and f+8 (f = step mod 8) x 2 polarisations x
+{forward, adjoint}, each to a relative residual of 1e-7 of the FP64 system;
+8 steps cover all 64.  The metric is solves/s over all ranks.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--workload combined|precision|batch|small]
+                  [--no-cpu] [--no-fp64] [--no-e2e]
 
-With N > 1 (torchrun) every rank solves its own copy of the workload (replicas;
-the right-hand sides are independent), timed between barriers, max over ranks.
+value: device time (CUDA events on the solver stream) of the K timed steps,
+inputs resident in HBM.  e2e: the same solves through mt3d_fwdsolve_batch
+with pinned host buffers (host->device copies of the inputs and the
+device->host copy of the fields inside the timed region), over min(K, 2)
+steps.  fp64: the same right-hand sides as the first timed step, solved one
+at a time by the plain FP64 path.  With N > 1 (torchrun) every rank solves its
+own copy of the workload (replicas; the right-hand sides are independent),
+timed between barriers, max over ranks.
 """
 from __future__ import annotations
 
@@ -35,6 +45,12 @@ from mt3d import models  # noqa: E402
 
 METRIC = "fwd+adjoint solves/s, mixed-precision batched vs plain FP64 GPU at 1e-7 residual"
 TOL = 1e-7
+# refinement cycle: FP32 BiCGStab iterations between FP64 residual updates
+# (the shadow residual is still restarted every 120 iterations, as cuBiCG
+# does); shorter cycles stall the low-frequency forward solves of the
+# 200x200x100 model, 300 converges all 64 right-hand sides
+CYCLE = 300
+MAX_CYCLES = 30
 
 
 def peaks():
@@ -76,7 +92,8 @@ def receiver_sources(model: models.Model, nrec: int, seed: int) -> np.ndarray:
 
 
 def workload(name: str):
-    """[(model, omegas, bc[nf*2], src[nf*2])] and a description."""
+    """[(model, omegas[nf*2], bc[nf*2], src[nf*2])] (rows: frequency major,
+    polarisation minor) and a description."""
     if name == "combined":
         m, f = models.config_combined()
         probs = [(m, f)]
@@ -106,6 +123,26 @@ def workload(name: str):
                 oms.append(w)
         out.append((m, np.asarray(oms), np.stack(bcs), np.stack(srcs)))
     return out, desc
+
+
+def step_rows(name: str, nf: int, step: int) -> list:
+    """Frequency indices solved by a step (all 2 x {fwd, adj} of each)."""
+    if name == "combined":
+        h = nf // 2
+        return [step % h, step % h + h]
+    return list(range(nf))
+
+
+def step_batch(oms, bcs, srcs, fidx):
+    """Right-hand sides of the frequencies fidx: forward rows (boundary data,
+    no source) then adjoint rows (source, no boundary data)."""
+    rows = [2 * f + p for f in fidx for p in (0, 1)]
+    n = len(rows)
+    om = np.concatenate([oms[rows]] * 2)
+    bc = np.concatenate([bcs[rows], np.zeros_like(bcs[rows])])
+    src = np.concatenate([np.zeros_like(srcs[rows]), srcs[rows]])
+    tr = np.concatenate([np.zeros(n, np.int32), np.ones(n, np.int32)])
+    return om, bc, src, tr
 
 
 # --------------------------------------------------------------------------
@@ -161,19 +198,36 @@ class Clocks:
 # the D-ILU preconditioner and divergence correction every 40 iterations)
 # --------------------------------------------------------------------------
 CPU_SAMPLE_ITERS = 10
+# QMR + D-ILU iterations (divergence correction every 40) per solve to 1e-7,
+# measured with the oracle on the 100x100x60 workload (forward, both
+# polarisations, and adjoint); the per-iteration cost is timed on the
+# workload's own grid
+CPU_ITERS_PER_SOLVE = 600
+
+
+def _models(name: str):
+    """[(model, frequencies)] of a workload, without its right-hand sides."""
+    if name == "combined":
+        return [models.config_combined()]
+    if name == "precision":
+        return [models.config_precision()]
+    if name == "batch":
+        return models.config_batch()
+    return [models.config_small_forward()]
 
 
 def _cpu_worker(args):
-    name, k, w, seconds = args
+    name, mode = args
     from oracle.oracle import Oracle, QMR, PC_DILU
-    probs, _ = workload(name)
-    m, oms, bcs, _ = probs[k]
+    m, f = _models(name)[0]
+    omega = 2 * np.pi * float(f[0])
+    bc = mbc.boundary_1d(m, omega, mode)
     o = Oracle(m.grid)
     o.update_cond(m.m_earth, m.air_cond)
-    o.update_freq(oms[w])
+    o.update_freq(omega)
     o.set_control(solver=QMR, precond=PC_DILU, IterPerDivCor=CPU_SAMPLE_ITERS, MaxDivCor=1)
     t0 = time.perf_counter()
-    o.fwdsolve(bc=bcs[w])
+    o.fwdsolve(bc=bc)
     d = o.diagnostics()
     return (time.perf_counter() - t0), max(1, d["nIterTotal"])
 
@@ -187,7 +241,7 @@ def cpu_baseline(name: str, iters_per_solve: float, procs: int):
     ctx = mp.get_context("spawn")
     with ctx.Pool(procs) as pool:
         t0 = time.perf_counter()
-        res = pool.map(_cpu_worker, [(name, 0, i % 2, 0) for i in range(procs)])
+        res = pool.map(_cpu_worker, [(name, 1 + i % 2) for i in range(procs)])
         wall = time.perf_counter() - t0
     t_it = float(np.mean([t / n for t, n in res]))
     per_proc = 1.0 / (t_it * iters_per_solve)
@@ -198,29 +252,47 @@ def cpu_baseline(name: str, iters_per_solve: float, procs: int):
 
 
 # --------------------------------------------------------------------------
+def stencil_bytes(kprec: int, nE: int, nN: int) -> float:
+    """Algorithmic bytes per edge and right-hand side of one staged stencil
+    launch (v = A ph with rt . v, or t = A sh with t . s, t . t): read the
+    input vector, the auxiliary vector and sigma, the signed node weight
+    (nN / nE per edge), write the output."""
+    sc = 8 if kprec else 16
+    sr = 4 if kprec else 8
+    return 3 * sc + sr + sr * nN / nE
+
+
+# DRAM bytes (read + write) per edge and right-hand side of one kcs_vt<float>
+# launch, measured by ncu on the 100x100x60 workload (4 right-hand sides);
+# see profiles/kcs_vt_100x100x60_4rhs.md
+TRAFFIC_PER_EDGE_RHS = None
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--steps", type=int, default=8)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default=os.environ.get("MT3D_BENCH_WORKLOAD", "precision"))
+    ap.add_argument("--workload", default=os.environ.get("MT3D_BENCH_WORKLOAD", "combined"))
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    probs, desc = workload(args.workload)
+    per_step = [sum(4 * len(step_rows(args.workload, len(p[1]) // 2, s)) for p in probs) for s in range(args.steps)]
 
     if args.impl == "reference":
         if rank != 0:
             return
-        probs, desc = workload(args.workload)
         procs = min(os.cpu_count() or 1, 8)
-        iters = float(os.environ.get("MT3D_CPU_ITERS_PER_SOLVE", "600"))
+        iters = float(os.environ.get("MT3D_CPU_ITERS_PER_SOLVE", str(CPU_ITERS_PER_SOLVE)))
         cb = cpu_baseline(args.workload, iters, procs)
-        step_s = 1.0 / cb["value"] * sum(2 * len(p[1]) for p in probs)
+        step_s = sum(per_step) / args.steps / cb["value"]
         line = {"metric": METRIC, "value": cb["value"], "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "c128", "data": "synthetic",
@@ -234,38 +306,39 @@ def main():
     if world > 1:
         import torch.distributed as dist
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=600))
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=900))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
     from mt3d import capi
 
-    probs, desc = workload(args.workload)
+    # per model: solver handle and the device-resident inputs of every step
     solvers = []
+    nsteps_distinct = min(args.steps, 8) if args.workload == "combined" else 1
     for m, oms, bcs, srcs in probs:
         s = capi.Solver(m.grid, device=local)
         s.set_formulation(capi.FORM_CCGD)
         s.update_cond(m.m_earth, m.air_cond)
-        s.set_control(tolEMfwd=TOL, tolEMadj=TOL, IterPerDivCor=120, MaxDivCor=100, precision=capi.PREC_MIXED)
-        s.set_stream(torch.cuda.current_stream(dev).cuda_stream)
-        nr = len(oms)
-        # rows 0..nr-1: forward (boundary data, no source); nr..2nr-1: adjoint (source, no boundary data)
-        zb = np.zeros_like(bcs)
-        d_bc = torch.from_numpy(np.concatenate([bcs, zb])).to(dev)
-        d_src = torch.from_numpy(np.concatenate([zb, srcs])).to(dev)
-        d_e = torch.zeros((2 * nr, s.nE), dtype=torch.complex128, device=dev)
-        tr = np.concatenate([np.zeros(nr, np.int32), np.ones(nr, np.int32)])
-        solvers.append((s, np.concatenate([oms, oms]), d_bc, d_src, d_e, tr))
-    n_solves = sum(2 * len(p[1]) for p in probs)
+        s.set_control(tolEMfwd=TOL, tolEMadj=TOL, IterPerDivCor=CYCLE, MaxDivCor=MAX_CYCLES, precision=capi.PREC_MIXED)
+        s.set_stream(stream.cuda_stream)
+        batches = []
+        for st in range(nsteps_distinct):
+            om, bc, src, tr = step_batch(oms, bcs, srcs, step_rows(args.workload, len(oms) // 2, st))
+            batches.append((om, torch.from_numpy(bc).to(dev), torch.from_numpy(src).to(dev), tr))
+        nmax = max(len(b[0]) for b in batches)
+        d_e = torch.zeros((nmax, s.nE), dtype=torch.complex128, device=dev)
+        solvers.append((s, batches, d_e))
 
-    def step(stats=None):
-        # forward and adjoint right-hand sides of a model in one batched call
-        for s, oms2, d_bc, d_src, d_e, tr in solvers:
-            d_e.zero_()
-            st, rc = s.fwdsolve_batch_device(oms2, d_e.data_ptr(), bc_ptr=d_bc.data_ptr(), src_ptr=d_src.data_ptr(),
+    def step(k, stats=None):
+        for s, batches, d_e in solvers:
+            om, d_bc, d_src, tr = batches[k % len(batches)]
+            e = d_e[:len(om)]
+            e.zero_()
+            st, rc = s.fwdsolve_batch_device(om, e.data_ptr(), bc_ptr=d_bc.data_ptr(), src_ptr=d_src.data_ptr(),
                                              trans=tr)
             if stats is not None:
-                it, rr = s.batch_diagnostics(len(oms2))
-                stats.append((s.nE, it.copy(), rr.copy(), st.copy()))
+                it, rr = s.batch_diagnostics(len(om))
+                stats.append((s.nE, s.nN, it.copy(), rr.copy(), st.copy()))
 
     def barrier():
         if dist is not None:
@@ -279,8 +352,8 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    for _ in range(args.warmup):
-        step()
+    for k in range(args.warmup):
+        step(k)
     clocks = Clocks(local)
     for s, *_ in solvers:
         s.profile(True)
@@ -289,17 +362,19 @@ def main():
     barrier()
     launches0 = int(L.mt3d_launch_counter())
     clocks.start()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ev0.record()
-    for _ in range(args.steps):
-        step(stats)
-    ev1.record()
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    evs[0].record(stream)
+    for k in range(args.steps):
+        step(k, stats)
+        evs[k + 1].record(stream)
     barrier()
     launches = int(L.mt3d_launch_counter()) - launches0
     ck = clocks.stop()
-    ms_dev = max_over_ranks(ev0.elapsed_time(ev1))
-    value = world * n_solves * args.steps / (ms_dev / 1e3)
-    # roofline of the stencil kernels (v = A ph and t = A sh, fused dot products)
+    step_ms = [evs[k].elapsed_time(evs[k + 1]) for k in range(args.steps)]
+    ms_dev = max_over_ranks(sum(step_ms))
+    n_solves = sum(per_step)
+    value = world * n_solves / (ms_dev / 1e3)
+    # roofline of the stencil kernel (both launches of every iteration, events on the solver stream)
     kn, kms, kprec = 0, 0.0, 1
     for s, *_ in solvers:
         n, ms, pr = s.kernel_time()
@@ -307,81 +382,93 @@ def main():
         kms += ms
         kprec = pr
         s.profile(False)
-    sc = 8 if kprec else 16  # bytes of one complex entry
-    sr = 4 if kprec else 8
-    # per edge and right-hand side: read the preconditioned vector, rt (or s),
-    # sigma and the grad-div node potentials (one node per edge on average:
-    # nN / nE ~ 1/3 of a complex); write the result
-    b_edge = 3 * sc + sr + sc / 3
-    alg_bytes = sum(float(nE) * it.sum() * 2 * b_edge for nE, it, rr, st in stats)
-    converged = all(np.all(st == 0) for _, _, _, st in stats)
-    max_relres = max(float(np.max(rr)) for _, _, rr, _ in stats)
+    alg = sum(float(nE) * stencil_bytes(kprec, nE, nN) * it.sum() * 2 for nE, nN, it, rr, st in stats)
+    units = sum(float(nE) * it.sum() * 2 for nE, nN, it, rr, st in stats)
+    converged = all(np.all(st == 0) for *_, st in stats)
+    max_relres = max(float(np.max(rr)) for _, _, _, rr, _ in stats)
     peak, peak_kind = peaks()
-    achieved = (alg_bytes / (kms / 1e3) / 1e9) if kms > 0 else None
+    achieved = (alg / (kms / 1e3) / 1e9) if kms > 0 else None
+    traffic = (TRAFFIC_PER_EDGE_RHS * units / kn) if (TRAFFIC_PER_EDGE_RHS and kn) else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": (achieved / peak) if achieved else None, "traffic": None,
-                "kernel": "kb_v/kb_t (stencil + fused dots), FP32 complex" if kprec else "kb_v/kb_t FP64",
-                "peak_kind": peak_kind, "timed_launches": kn, "bytes_per_edge_rhs": b_edge}
+                "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                "kernel": "kcs_vt (staged stencil + grad-div + fused dots), " + ("FP32" if kprec else "FP64") + " complex",
+                "peak_kind": peak_kind, "timed_launches": kn, "bytes_per_edge_rhs": alg / units if units else None,
+                "algorithmic_bytes_per_launch": alg / kn if kn else None}
 
-    # end to end through the C ABI with host buffers (pinned), copies inside
-    pinned = []
-    for s, oms2, d_bc, d_src, d_e, tr in solvers:
-        hbc = torch.empty(tuple(d_bc.shape), dtype=torch.complex128).pin_memory()
-        hsrc = torch.empty_like(hbc).pin_memory()
-        he = torch.empty_like(hbc).pin_memory()
-        hbc.copy_(d_bc.cpu())
-        hsrc.copy_(d_src.cpu())
-        pinned.append((hbc.numpy(), hsrc.numpy(), he.numpy()))
-    h2d = d2h = 0
-    barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        for (s, oms2, d_bc, d_src, d_e, tr), (hbc, hsrc, he) in zip(solvers, pinned):
-            he[:] = 0
-            s.fwdsolve_batch(oms2, bc=hbc, src=hsrc, e0=he, trans=tr)
-            h2d += hbc.nbytes + hsrc.nbytes + he.nbytes
-            d2h += he.nbytes
-    barrier()
-    e2e_s = max_over_ranks(time.perf_counter() - t0)
-    e2e = {"value": world * n_solves * args.steps / e2e_s, "unit": "solves/s",
-           "h2d_bytes_per_step": h2d // args.steps, "d2h_bytes_per_step": d2h // args.steps}
+    # end to end through the C ABI with pinned host buffers, copies inside the timed region
+    e2e = None
+    if not args.no_e2e:
+        ke = min(args.steps, 2)
+        pinned = []
+        for s, batches, d_e in solvers:
+            per = []
+            for k in range(ke):
+                om, d_bc, d_src, tr = batches[k % len(batches)]
+                hbc = torch.empty(tuple(d_bc.shape), dtype=torch.complex128).pin_memory()
+                hsrc = torch.empty_like(hbc).pin_memory()
+                he = torch.empty_like(hbc).pin_memory()
+                hbc.copy_(d_bc.cpu())
+                hsrc.copy_(d_src.cpu())
+                per.append((om, hbc.numpy(), hsrc.numpy(), he.numpy(), tr))
+            pinned.append(per)
+        h2d = d2h = 0
+        barrier()
+        t0 = time.perf_counter()
+        for k in range(ke):
+            for (s, batches, d_e), per in zip(solvers, pinned):
+                om, hbc, hsrc, he, tr = per[k]
+                he[:] = 0
+                s.fwdsolve_batch(om, bc=hbc, src=hsrc, e0=he, trans=tr)
+                h2d += hbc.nbytes + hsrc.nbytes + he.nbytes
+                d2h += he.nbytes
+        barrier()
+        e2e_s = max_over_ranks(time.perf_counter() - t0)
+        e2e = {"value": world * sum(per_step[:ke]) / e2e_s, "unit": "solves/s", "steps": ke,
+               "h2d_bytes_per_step": h2d // ke, "d2h_bytes_per_step": d2h // ke}
+        del pinned
 
-    # plain FP64 path, one right-hand side at a time (the comparison point)
+    # plain FP64 path on the right-hand sides of the first timed step, one at a time
     fp64 = None
     if not args.no_fp64:
         barrier()
         t0 = time.perf_counter()
         nfp = 0
-        for s, oms2, d_bc, d_src, d_e, tr in solvers:
-            s.set_control(tolEMfwd=TOL, tolEMadj=TOL, IterPerDivCor=120, MaxDivCor=100, precision=capi.PREC_FP64)
-            for r in range(len(oms2)):
-                e1 = torch.zeros((1, s.nE), dtype=torch.complex128, device=dev)
-                s.fwdsolve_batch_device(oms2[r:r + 1], e1.data_ptr(), bc_ptr=d_bc[r:r + 1].data_ptr(),
+        for s, batches, d_e in solvers:
+            om, d_bc, d_src, tr = batches[0]
+            s.set_control(tolEMfwd=TOL, tolEMadj=TOL, IterPerDivCor=CYCLE, MaxDivCor=MAX_CYCLES, precision=capi.PREC_FP64)
+            for r in range(len(om)):
+                e1 = d_e[:1]
+                e1.zero_()
+                s.fwdsolve_batch_device(om[r:r + 1], e1.data_ptr(), bc_ptr=d_bc[r:r + 1].data_ptr(),
                                         src_ptr=d_src[r:r + 1].data_ptr(), trans=tr[r:r + 1])
                 nfp += 1
-            s.set_control(tolEMfwd=TOL, tolEMadj=TOL, IterPerDivCor=120, MaxDivCor=100, precision=capi.PREC_MIXED)
+            s.set_control(tolEMfwd=TOL, tolEMadj=TOL, IterPerDivCor=CYCLE, MaxDivCor=MAX_CYCLES, precision=capi.PREC_MIXED)
         barrier()
         fp64_s = max_over_ranks(time.perf_counter() - t0)
-        fp64 = world * nfp / fp64_s
+        fp64 = {"value": world * nfp / fp64_s, "unit": "solves/s", "solves": nfp,
+                "mixed_same_rhs": world * per_step[0] / max_over_ranks(step_ms[0] / 1e3),
+                "speedup": (per_step[0] / (step_ms[0] / 1e3)) / (nfp / fp64_s)}
 
     if rank == 0:
         cb = None
         if world == 1 and not args.no_cpu:
-            its = [int(np.mean(it)) for _, it, _, _ in stats]
-            cb = cpu_baseline(args.workload, float(os.environ.get("MT3D_CPU_ITERS_PER_SOLVE", "600")),
+            cb = cpu_baseline(args.workload, float(os.environ.get("MT3D_CPU_ITERS_PER_SOLVE", str(CPU_ITERS_PER_SOLVE))),
                               min(os.cpu_count() or 1, 8))
+        its = np.concatenate([it for _, _, it, _, _ in stats])
         line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_dev / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "c64 inner / c128 refinement", "data": "synthetic",
-                "config": {"workload": f"{args.workload}: {desc}", "solves_per_step": n_solves, "tol": TOL,
-                           "precision": "mixed (FP32 BiCGStab, FP64 residual refinement)", "formulation": "curl-curl + grad-div (SP2), diagonal preconditioner",
-                           "l2": "fields larger than L2 (flush not needed)" if args.workload == "combined" else
-                                 "inputs smaller than L2 at this size; no flush (iterative solve re-reads its own "
-                                 "vectors every iteration)",
+                "scaling": "weak", "vs_baseline": None, "dtype": "c64 (Krylov) / c128 (refinement)",
+                "data": "synthetic (seeded random-field models of the stated shapes)",
+                "config": {"workload": f"{args.workload}: {desc}", "solves_per_step": per_step[0], "tol": TOL,
+                           "precision": "mixed: FP32 BiCGStab cycles, FP64 residual refinement",
+                           "formulation": "curl-curl + grad-div (SP2), diagonal preconditioner",
+                           "l2": "fields larger than L2 (no flush)" if args.workload == "combined" else
+                                 "no flush: the solve re-reads its own vectors every iteration",
                            "parallelism": f"replicas x{world}"},
                 "converged": bool(converged), "max_relres": max_relres,
-                "fp64_solves_per_s": fp64, "speedup_vs_fp64": (value / fp64) if fp64 else None,
-                "e2e": e2e, "roofline": roofline, "cpu_baseline": cb, "clocks": ck, "gpu_launches": launches}
+                "iterations_per_solve": {"mean": float(its.mean()), "min": int(its.min()), "max": int(its.max())},
+                "fp64": fp64, "e2e": e2e, "roofline": roofline, "cpu_baseline": cb, "clocks": ck,
+                "gpu_launches": launches}
         print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()

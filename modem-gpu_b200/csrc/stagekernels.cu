@@ -54,19 +54,19 @@ template <typename T> __global__ void __launch_bounds__(kThreads, sizeof(T) == 4
     const size_t off = (size_t)r * a.stride;
     const C2<T> *b = a.b + off;
     C2<T> *R = a.r + off, *RT = a.rt + off;
-    T u[2] = {T(0), T(0)};
+    double u[2] = {0.0, 0.0};
     stage_march(stage_smem<T>(), a.g, a.x0 + off, a.sigma, a.gd ? a.gdn : nullptr, b, stage_wmu(a, r), i0, j0, k0,
                 k1, [&](int, int e, bool in, C2<T> ax, C2<T>, C2<T> bb) {
                     C2<T> res = mk<T>(0, 0);
                     if (in) {
                         res = csub(bb, ax);
-                        u[0] += bb.x * bb.x + bb.y * bb.y;
-                        u[1] += res.x * res.x + res.y * res.y;
+                        u[0] += (double)bb.x * bb.x + (double)bb.y * bb.y;
+                        u[1] += (double)res.x * res.x + (double)res.y * res.y;
                     }
                     R[e] = res;
                     RT[e] = res;
                 });
-    double v[2] = {(double)u[0], (double)u[1]};
+    double v[2] = {u[0], u[1]};
     double tot[2];
     if (block_reduce_last<2>(v, a.parts, a.cnt, r, blockIdx.x + gridDim.x * blockIdx.z, gridDim.x * gridDim.z, tot) &&
         threadIdx.x == 0)
@@ -87,23 +87,24 @@ template <typename T> __global__ void __launch_bounds__(kThreads, sizeof(T) == 4
     const C2<T> *in = (which ? a.sh : a.ph) + off;
     const C2<T> *w = (which ? a.s : a.rt) + off;
     C2<T> *out = (which ? a.t : a.v) + off;
-    // per-thread partial sums in T (a column's few dozen terms), blocks in double
-    T u[3] = {T(0), T(0), T(0)};
+    // partial sums in double: the Krylov scalars of a converging iteration are
+    // small differences of large sums, which FP32 sums lose at large grids
+    double u[3] = {0.0, 0.0, 0.0};
     stage_march(stage_smem<T>(), a.g, in, a.sigma, a.gd ? a.gdn : nullptr, w, stage_wmu(a, r), i0, j0, k0, k1,
                 [&](int, int e, bool inn, C2<T> y, C2<T>, C2<T> q) {
                     if (inn) {
                         if (which == 0) {
-                            u[0] += q.x * y.x + q.y * y.y;  // conj(rt) v
-                            u[1] += q.x * y.y - q.y * y.x;
+                            u[0] += (double)q.x * y.x + (double)q.y * y.y;  // conj(rt) v
+                            u[1] += (double)q.x * y.y - (double)q.y * y.x;
                         } else {
-                            u[0] += y.x * q.x + y.y * q.y;  // conj(t) s
-                            u[1] += y.x * q.y - y.y * q.x;
-                            u[2] += y.x * y.x + y.y * y.y;
+                            u[0] += (double)y.x * q.x + (double)y.y * q.y;  // conj(t) s
+                            u[1] += (double)y.x * q.y - (double)y.y * q.x;
+                            u[2] += (double)y.x * y.x + (double)y.y * y.y;
                         }
                     }
                     out[e] = y;
                 });
-    double v[3] = {(double)u[0], (double)u[1], (double)u[2]};
+    double v[3] = {u[0], u[1], u[2]};
     double tot[3];
     if (block_reduce_last<3>(v, a.parts, a.cnt, r, blockIdx.x + gridDim.x * blockIdx.z, gridDim.x * gridDim.z, tot) &&
         threadIdx.x == 0) {
