@@ -527,10 +527,11 @@ template <typename T> __global__ void __launch_bounds__(kThreads) kcb_jacobi(KAr
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
-static int zchunks(int nz, int ntiles, int nrhs)
+static int zchunks(int nz, int ntiles, int)
 {
-    // enough blocks for ~8 per SM over the batch, chunks of >= 8 planes
-    const int want = std::max(1, (148 * 8) / std::max(1, ntiles * nrhs));
+    // ~8 blocks per SM for one right-hand side (the blocks of converged ones
+    // exit at once), chunks of >= 8 planes
+    const int want = std::max(1, (148 * 8) / std::max(1, ntiles));
     return std::max(1, std::min(want, (nz + 1) / 8));
 }
 

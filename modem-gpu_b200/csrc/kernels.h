@@ -95,7 +95,7 @@ template <typename T> void launch_colb_jacobi(const KArgs<T> &a, int nrhs, cudaS
 template <typename T> void launch_stage_init(const KArgs<T> &a, int nrhs, cudaStream_t s);
 template <typename T> void launch_stage_vt(const KArgs<T> &a, int which, int nrhs, cudaStream_t s);
 void launch_stage_res64(const KArgs<double> &a, int nrhs, cudaStream_t s);
-int stage_chunks(int nz, int tiles, int nrhs, int resident);
+int stage_chunks(int nz, int tiles, int resident);
 template <typename T> void launch_cocg_iter(const ColArgs<T> &a, int nrhs, cudaStream_t s, cudaEvent_t *ev = nullptr);
 
 template <typename T>

@@ -6,6 +6,7 @@
 // cycle.
 #include <algorithm>
 #include <cmath>
+#include <limits>
 #include <cstdio>
 #include <cstring>
 
@@ -388,16 +389,38 @@ int Solver::update_freq(double w)
 // ---------------------------------------------------------------------------
 // workspace and argument blocks
 // ---------------------------------------------------------------------------
-static int blocks_for(int64_t n, int nrhs, int &chunk)
+static int blocks_for(int64_t n, int &chunk)
 {
     // contiguous chunks of >= 4 sweeps of the block; about 8 resident blocks
-    // per SM over the whole batch
-    const int64_t target = std::max<int64_t>(1, (148LL * 8) / std::max(1, nrhs));
+    // per SM for ONE right-hand side: the right-hand sides of a batch converge
+    // at different iterations, the blocks of finished ones exit at once, and
+    // the grid must still fill the GPU when a single right-hand side is left
+    const int64_t target = 148LL * 8;
     int64_t per = (n + target - 1) / target;
     per = std::max<int64_t>(per, 4 * kThreads);
     per = (per + kThreads - 1) / kThreads * kThreads;
     chunk = (int)per;
     return (int)((n + per - 1) / per);
+}
+
+// FP64 Krylov vectors in a mixed-precision workspace (allocated when a
+// right-hand side first falls back to FP64 cycles; kept with the workspace)
+int Solver::ensure_fp64_krylov(int nrhs)
+{
+    Workspace &w = ws_;
+    const size_t e64 = (size_t)nrhs * nE * sizeof(double2);
+    if (w.r.bytes() >= e64) return 0;
+    DevBuf *v64[] = {&w.x1, &w.r, &w.rt, &w.p, &w.v, &w.ph, &w.s, &w.sh, &w.t, &w.jinv64, &w.zm, &w.zc};
+    int err = 0;
+    for (int q = 0; q < 9; q++) err |= v64[q]->alloc(e64);
+    if (ctl.solver == 1) err |= w.jinv64.alloc(e64);
+    if (ctl.solver == 3) err |= w.zm.alloc(e64) | w.zc.alloc(e64);
+    if (err) {
+        for (DevBuf *d : v64) d->release();
+        cudaGetLastError();
+        return fail(8, "out of device memory for the FP64 Krylov vectors");
+    }
+    return 0;
 }
 
 int Solver::ensure_workspace(int nrhs, int precision)
@@ -436,7 +459,7 @@ int Solver::ensure_workspace(int nrhs, int precision)
     }
     int c;
     const ColMapHost cm = col_map(nx, ny);
-    const int nb = std::max({blocks_for(nE, nrhs, c), blocks_for(nN, nrhs, c), cm.tiles * std::max(1, (nz + 1) / 8),
+    const int nb = std::max({blocks_for(nE, c), blocks_for(nN, c), cm.tiles * std::max(1, (nz + 1) / 8),
                              1184});
     err |= w.bst.alloc(nrhs * sizeof(BicgState)) | w.pst.alloc(nrhs * sizeof(PcgState)) |
            w.ost.alloc(nrhs * sizeof(OuterState));
@@ -477,7 +500,7 @@ template <> KArgs<double> Solver::kargs<double>(int nrhs, int)
     a.rerr = w.rerr.as<double>();
     a.rerr_stride = ctl.IterPerDivCor + 1;
     a.stride = nE;
-    a.nblk = blocks_for(nE, nrhs, a.chunk);
+    a.nblk = blocks_for(nE, a.chunk);
     a.maxit = ctl.IterPerDivCor;
     a.inner = 0;
     a.dsgn = -1.0;
@@ -512,7 +535,7 @@ template <> KArgs<float> Solver::kargs<float>(int nrhs, int)
     a.rerr = w.rerr.as<double>();
     a.rerr_stride = ctl.IterPerDivCor + 1;
     a.stride = nE;
-    a.nblk = blocks_for(nE, nrhs, a.chunk);
+    a.nblk = blocks_for(nE, a.chunk);
     a.maxit = ctl.IterPerDivCor;
     a.inner = 1;
     a.dsgn = -1.0;
@@ -590,8 +613,8 @@ DArgs Solver::dargs(int nrhs)
     a.rerr_stride = ctl.MaxIterDivCor + 1;
     a.stride = nN;
     a.estride = nE;
-    a.nblk = blocks_for(nN, nrhs, a.chunk);
-    a.enblk = blocks_for(nE, nrhs, a.echunk);
+    a.nblk = blocks_for(nN, a.chunk);
+    a.enblk = blocks_for(nE, a.echunk);
     a.maxit = ctl.MaxIterDivCor;
     a.tol = ctl.tolDivCor;
     return a;
@@ -868,6 +891,12 @@ int Solver::solve(int nrhs, const double *omegas, const int *trans, const double
         return false;
     };
     const bool refine = prec == 1 || ctl.formulation == 1;  // loop driven by the true FP64 residual
+    // mixed precision: a right-hand side whose last FP32 cycle did not halve
+    // its true FP64 residual continues with FP64 Krylov cycles (the FP32
+    // operator's rounding can stop an FP32 solve from reducing a residual
+    // that is already small relative to the field)
+    std::vector<double> prev_relres(nrhs, std::numeric_limits<double>::infinity());
+    std::vector<char> hi(nrhs, 0);
     while (any_active()) {
         if (refine) {
             // true FP64 residual r64 = b - A X (into tmp); converged right-hand
@@ -888,18 +917,44 @@ int Solver::solve(int nrhs, const double *omegas, const int *trans, const double
                 if (o.relres <= o.tol) { o.active = 0; o.converged = 1; continue; }
                 if (o.nDivCor >= ctl.MaxDivCor) { o.active = 0; o.failed = 1; continue; }
                 o.tol_inner = o.tol * o.bnorm64 * o.scale;  // tol*||b|| relative to ||r64||
+                if (prec == 1 && !hi[r] && o.relres > 0.5 * prev_relres[r]) hi[r] = 1;
+                prev_relres[r] = o.relres;
                 work = true;
             }
             if (!work) break;
             push_state();
-            if (prec == 1)
+        }
+        if (prec == 1) {
+            // FP32 cycles on the normalised residual, FP64 cycles on (b, X) for
+            // the right-hand sides that left FP32; each group runs with the
+            // other group's right-hand sides marked inactive on the device
+            bool n32 = false, n64 = false;
+            for (int r = 0; r < nrhs; r++) {
+                if (!os[r].active) continue;
+                (hi[r] ? n64 : n32) = true;
+            }
+            std::vector<OuterState> grp(os);
+            if (n32) {
+                for (int r = 0; r < nrhs; r++) grp[r].active = os[r].active && !hi[r];
+                cudaMemcpyAsync(w.ost.as<void>(), grp.data(), nrhs * sizeof(OuterState), cudaMemcpyHostToDevice,
+                                stream_);
                 launch_cast(w.ost.as<OuterState>(), (int)nE, nE, w.tmp.as<double2>(), w.f_b.as<float2>(),
                             w.f_x0.as<float2>(), nrhs, stream_);
+                if ((rc = run_bicg(nrhs, 1, ctl.IterPerDivCor))) return rc;
+                launch_update(w.ost.as<OuterState>(), (int)nE, nE, w.f_x0.as<float2>(), X, nrhs, stream_);
+            }
+            if (n64) {
+                if ((rc = ensure_fp64_krylov(nrhs))) return rc;
+                for (int r = 0; r < nrhs; r++) grp[r].active = os[r].active && hi[r];
+                cudaMemcpyAsync(w.ost.as<void>(), grp.data(), nrhs * sizeof(OuterState), cudaMemcpyHostToDevice,
+                                stream_);
+                if ((rc = run_bicg(nrhs, 0, ctl.IterPerDivCor))) return rc;
+            }
+            push_state();
+        } else {
+            // Krylov call: FP64 on (b, X)
+            if ((rc = run_bicg(nrhs, prec, ctl.IterPerDivCor))) return rc;
         }
-        // Krylov call: FP64 on (b, X), or FP32 on the normalised residual
-        if ((rc = run_bicg(nrhs, prec, ctl.IterPerDivCor))) return rc;
-        if (prec == 1)
-            launch_update(w.ost.as<OuterState>(), (int)nE, nE, w.f_x0.as<float2>(), X, nrhs, stream_);
         cudaMemcpyAsync(bs.data(), w.bst.as<void>(), nrhs * sizeof(BicgState), cudaMemcpyDeviceToHost, stream_);
         cudaMemcpyAsync(rerr.data(), w.rerr.as<void>(), rerr.size() * sizeof(double), cudaMemcpyDeviceToHost, stream_);
         if ((rc = sync("fwdsolve Krylov cycle"))) return rc;

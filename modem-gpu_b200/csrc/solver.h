@@ -91,6 +91,7 @@ class Solver {
 
   private:
     int ensure_workspace(int nrhs, int precision);
+    int ensure_fp64_krylov(int nrhs);
     int run_bicg(int nrhs, int precision, int maxit);
     int run_divcorr(int nrhs);
     template <typename T> KArgs<T> kargs(int nrhs, int precision_ws);

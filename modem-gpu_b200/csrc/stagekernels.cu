@@ -104,9 +104,8 @@ template <typename T> __global__ void __launch_bounds__(kThreads, sizeof(T) == 4
                     }
                     out[e] = y;
                 });
-    double v[3] = {u[0], u[1], u[2]};
     double tot[3];
-    if (block_reduce_last<3>(v, a.parts, a.cnt, r, blockIdx.x + gridDim.x * blockIdx.z, gridDim.x * gridDim.z, tot) &&
+    if (block_reduce_last<3>(u, a.parts, a.cnt, r, blockIdx.x + gridDim.x * blockIdx.z, gridDim.x * gridDim.z, tot) &&
         threadIdx.x == 0) {
         if (which == 0) fin_v(st, tot);
         else fin_t(st, tot);
@@ -169,11 +168,13 @@ template <typename K> static int stage_setup(K kern, size_t smem, int slot)
 }
 
 // chunks of node planes: the count that minimises (waves of resident blocks)
-// x (planes per chunk + the 3 planes of the prologue), chunks >= 8 planes
-int stage_chunks(int nz, int tiles, int nrhs, int resident)
+// x (planes per chunk + the 3 planes of the prologue), chunks >= 8 planes.
+// Sized for one right-hand side: the blocks of right-hand sides that have
+// converged exit at once, and the last one left must still fill the GPU.
+int stage_chunks(int nz, int tiles, int resident)
 {
     const int planes = nz + 1;
-    const long per = (long)tiles * nrhs;
+    const long per = tiles;
     int best = 1;
     double best_t = 1e300;
     for (int c = 1; c <= std::max(1, planes / 8); c++) {
@@ -187,7 +188,7 @@ int stage_chunks(int nz, int tiles, int nrhs, int resident)
 
 template <typename T> static dim3 stage_grid(const KArgs<T> &a, int nrhs, int resident)
 {
-    return dim3(a.cmap.tiles, nrhs, stage_chunks(a.g.nz, a.cmap.tiles, nrhs, resident));
+    return dim3(a.cmap.tiles, nrhs, stage_chunks(a.g.nz, a.cmap.tiles, resident));
 }
 
 template <typename T> void launch_stage_init(const KArgs<T> &a, int nrhs, cudaStream_t s)

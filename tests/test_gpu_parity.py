@@ -404,3 +404,24 @@ def test_ccgd_sources_match_sp2(gprob):
         er, it, rerr, conv = ref.fwdsolve(trans=trans, src=sv)
         assert rc == 0 and conv
         assert relerr(eg[mask], er[mask]) < 1e-5
+
+
+def test_mixed_cycles_fall_back_to_fp64(gprob):
+    """Mixed precision with short (8-iteration) FP32 cycles, which do not
+    always halve the FP64 residual, so right-hand sides may continue with FP64
+    cycles; either way the batch must converge to the FP64 solution (1e-5 on
+    earth edges) with a true residual <= 1e-7."""
+    g, m, omega, ref, s = gprob
+    oms = np.array([omega, omega])
+    bcs = np.stack([mbc.boundary_1d(m, omega, md) for md in (1, 2)])
+    s.set_control(IterPerDivCor=120, MaxDivCor=20, precision=capi.PREC_FP64)
+    e64, st64, rc64 = s.fwdsolve_batch(oms, bc=bcs)
+    s.set_control(IterPerDivCor=8, MaxDivCor=4000, precision=capi.PREC_MIXED)
+    em_, st, rc = s.fwdsolve_batch(oms, bc=bcs)
+    it, rr = s.batch_diagnostics(2)
+    s.set_control(IterPerDivCor=120, MaxDivCor=20, precision=capi.PREC_FP64)
+    assert rc64 == 0 and rc == 0 and np.all(st == 0)
+    assert np.all(rr <= 1e-7)
+    mask = earth_mask(g, m)
+    for r in range(2):
+        assert relerr(em_[r][mask], e64[r][mask]) < 1e-5
