@@ -199,10 +199,10 @@ class Clocks:
 # --------------------------------------------------------------------------
 CPU_SAMPLE_ITERS = 10
 # QMR + D-ILU iterations (divergence correction every 40) per solve to 1e-7,
-# measured with the oracle on the 100x100x60 workload (forward, both
-# polarisations, and adjoint); the per-iteration cost is timed on the
-# workload's own grid
-CPU_ITERS_PER_SOLVE = 600
+# measured with the oracle on the 100x100x60 workload at 1 Hz: 3450 and 3059
+# for the two forward polarisations (933 s and 799 s on one core); the mean
+# scales the per-iteration cost timed on the workload's own grid
+CPU_ITERS_PER_SOLVE = 3250
 
 
 def _models(name: str):
@@ -263,9 +263,9 @@ def stencil_bytes(kprec: int, nE: int, nN: int) -> float:
 
 
 # DRAM bytes (read + write) per edge and right-hand side of one kcs_vt<float>
-# launch, measured by ncu on the 100x100x60 workload (4 right-hand sides);
-# see profiles/kcs_vt_100x100x60_4rhs.md
-TRAFFIC_PER_EDGE_RHS = None
+# launch, measured by ncu on the 200x200x100 workload with 8 right-hand sides
+# (profiles/launches_200x200x100_8rhs.md)
+TRAFFIC_PER_EDGE_RHS = 28.6
 
 
 def main():
