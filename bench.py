@@ -252,6 +252,28 @@ def cpu_baseline(name: str, iters_per_solve: float, procs: int):
 
 
 # --------------------------------------------------------------------------
+# replicas: every rank solves its own copy; the job's rate is the solves of all
+# ranks over the slowest rank's time
+# --------------------------------------------------------------------------
+def make_max_over_ranks(dist, device):
+    """x -> max of x over the ranks of the default process group (identity
+    without one)."""
+    def f(x):
+        if dist is None:
+            return x
+        import torch
+        t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+    return f
+
+
+def replica_rate(solves_per_rank: float, seconds: float, world: int, max_over_ranks) -> float:
+    """Whole-job throughput of `world` replicas: world * solves / max time."""
+    return world * solves_per_rank / max_over_ranks(seconds)
+
+
+# --------------------------------------------------------------------------
 def stencil_bytes(kprec: int, nE: int, nN: int) -> float:
     """Algorithmic bytes per edge and right-hand side of one staged stencil
     launch (v = A ph with rt . v, or t = A sh with t . s, t . t): read the
@@ -345,12 +367,7 @@ def main():
             dist.barrier()
         torch.cuda.synchronize(dev)
 
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    max_over_ranks = make_max_over_ranks(dist, dev)
 
     for k in range(args.warmup):
         step(k)
@@ -373,7 +390,7 @@ def main():
     step_ms = [evs[k].elapsed_time(evs[k + 1]) for k in range(args.steps)]
     ms_dev = max_over_ranks(sum(step_ms))
     n_solves = sum(per_step)
-    value = world * n_solves / (ms_dev / 1e3)
+    value = replica_rate(n_solves, sum(step_ms) / 1e3, world, max_over_ranks)
     # roofline of the stencil kernel (both launches of every iteration, events on the solver stream)
     kn, kms, kprec = 0, 0.0, 1
     for s, *_ in solvers:

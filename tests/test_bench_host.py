@@ -1,0 +1,59 @@
+"""Host logic of bench.py on CPU: the replica aggregation over ranks (gloo,
+world size 2) and the step schedule of the 16-frequency workload."""
+import os
+import socket
+
+import pytest
+import torch
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+import bench
+
+
+def _free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank(rank, world, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=__import__("datetime").timedelta(seconds=60))
+    mor = bench.make_max_over_ranks(dist, "cpu")
+    # rank r took 2 + r seconds for its 8 solves
+    rate = bench.replica_rate(8, 2.0 + rank, world, mor)
+    slowest = mor(2.0 + rank)
+    q.put((rank, rate, slowest))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_replica_rate_is_total_over_slowest_rank():
+    world, port = 2, _free_port()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_rank, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=120) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank, rate, slowest in res:
+        assert slowest == pytest.approx(3.0)
+        assert rate == pytest.approx(2 * 8 / 3.0)
+
+
+def test_single_process_rate():
+    mor = bench.make_max_over_ranks(None, "cpu")
+    assert bench.replica_rate(8, 4.0, 1, mor) == pytest.approx(2.0)
+
+
+def test_steps_cover_all_frequencies_once():
+    seen = []
+    for s in range(8):
+        seen += bench.step_rows("combined", 16, s)
+    assert sorted(seen) == list(range(16))
+    assert bench.step_rows("precision", 1, 5) == [0]
