@@ -489,7 +489,7 @@ template <typename T> __global__ void __launch_bounds__(kThreads) kcb_jacobi(KAr
     const size_t off = (size_t)r * a.stride;
     const T wmu = c_wmu<T>(a.ost, r, a.dsgn);
     const ColGeo<T> cg = col_geo(g, i, j);
-    C2<T> *J = a.jinv + off;
+    C2<T> *J = a.jinv + (a.padded ? (size_t)r * a.pl.len() : off);
     const int bx = i + g.nx * j, by = g.nXe + i + (g.nx + 1) * j, bz = g.nXe + g.nYe + i + (g.nx + 1) * j;
     const int sxk = g.nx * (g.ny + 1), syk = (g.nx + 1) * g.ny, szk = (g.nx + 1) * (g.ny + 1);
     const int bn = i + (g.nx + 1) * j, snj = g.nx + 1, snk = (g.nx + 1) * (g.ny + 1);
@@ -519,7 +519,7 @@ template <typename T> __global__ void __launch_bounds__(kThreads) kcb_jacobi(KAr
                 const T inv = T(1) / (dr * dr + di * di);
                 m = mk<T>(dr * inv, -di * inv);
             }
-            J[e] = m;
+            J[a.padded ? a.pl.idx(comp, i, j, k) : e] = m;
         }
     }
 }

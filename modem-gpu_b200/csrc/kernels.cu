@@ -212,7 +212,7 @@ template <typename T> __global__ void __launch_bounds__(kThreads) kb_p(KArgs<T> 
     const bool first = st.first, reset_rt = st.first && st.pad;
     const C2<T> beta = mk<T>((T)st.beta.re, (T)st.beta.im);
     const C2<T> om = mk<T>((T)st.omega.re, (T)st.omega.im);
-    const int end = min((blockIdx.x + 1) * a.chunk, g.nE);
+    const int end = min((blockIdx.x + 1) * a.chunk, a.len);
     for (int e = chunk_begin(a.chunk); e < end; e += kThreads) {
         C2<T> rr = a.r[off + e];
         C2<T> p;
@@ -278,7 +278,7 @@ template <typename T> __global__ void __launch_bounds__(kThreads) kb_s(KArgs<T> 
     const Geo<T> &g = a.g;
     const T wmu = rhs_wmu(a, r);
     const C2<T> al = mk<T>((T)st.alpha.re, (T)st.alpha.im);
-    const int end = min((blockIdx.x + 1) * a.chunk, g.nE);
+    const int end = min((blockIdx.x + 1) * a.chunk, a.len);
     for (int e = chunk_begin(a.chunk); e < end; e += kThreads) {
         C2<T> s = csub(a.r[off + e], cmul(al, a.v[off + e]));
         a.s[off + e] = s;
@@ -343,7 +343,7 @@ template <typename T> __global__ void __launch_bounds__(kThreads) kb_xr(KArgs<T>
     const C2<T> *xs = (cur == 0 ? a.x0 : a.x1) + off;
     C2<T> *xd = (dst == 0 ? a.x0 : a.x1) + off;
     double v[3] = {0.0, 0.0, 0.0};
-    const int end = min((blockIdx.x + 1) * a.chunk, g.nE);
+    const int end = min((blockIdx.x + 1) * a.chunk, a.len);
     for (int e = chunk_begin(a.chunk); e < end; e += kThreads) {
         C2<T> xn = cadd(cadd(xs[e], cmul(al, a.ph[off + e])), cmul(om, a.sh[off + e]));
         xd[e] = xn;
@@ -405,7 +405,7 @@ template <typename T> __global__ void __launch_bounds__(kThreads) kb_finish(KArg
     const BicgState &st = a.st[r];
     if (!a.ost[r].active) return;
     const size_t off = (size_t)r * a.stride;
-    const int end = min((blockIdx.x + 1) * a.chunk, a.g.nE);
+    const int end = min((blockIdx.x + 1) * a.chunk, a.len);
     if (st.xbest == -1) {
         for (int e = chunk_begin(a.chunk); e < end; e += kThreads) a.x0[off + e] = mk<T>(0, 0);
     } else if (st.xbest == 1) {
@@ -805,6 +805,58 @@ __global__ void __launch_bounds__(kThreads) km_update(const OuterState *ost, int
     }
 }
 
+// b32 = r64 * scale and x32 = 0 on the padded layout (the padding keeps the
+// zeros it was allocated with)
+__global__ void __launch_bounds__(kThreads) km_cast_p(Geo<double> g, const OuterState *ost, size_t stride64,
+                                                      const double2 *r64, PadLayout pl, float2 *b32, float2 *x32)
+{
+    const int r = blockIdx.y;
+    if (!ost[r].active) return;
+    const size_t off = (size_t)r * stride64, offp = (size_t)r * pl.len();
+    const double sc = ost[r].scale;
+    for (int e = blockIdx.x * kThreads + threadIdx.x; e < g.nE; e += gridDim.x * kThreads) {
+        const EdgeIdx q = edge_decode(g, e);
+        const int pe = pl.idx(q.c, q.i, q.j, q.k);
+        const double2 v = r64[off + e];
+        b32[offp + pe] = make_float2((float)(v.x * sc), (float)(v.y * sc));
+        x32[offp + pe] = make_float2(0.f, 0.f);
+    }
+}
+
+// X += d32 / scale, d32 on the padded layout
+__global__ void __launch_bounds__(kThreads) km_update_p(Geo<double> g, const OuterState *ost, size_t stride64,
+                                                        PadLayout pl, const float2 *d32, double2 *X)
+{
+    const int r = blockIdx.y;
+    if (!ost[r].active) return;
+    const size_t off = (size_t)r * stride64, offp = (size_t)r * pl.len();
+    const double inv = ost[r].scale > 0.0 ? 1.0 / ost[r].scale : 0.0;
+    for (int e = blockIdx.x * kThreads + threadIdx.x; e < g.nE; e += gridDim.x * kThreads) {
+        const EdgeIdx q = edge_decode(g, e);
+        const float2 d = d32[offp + pl.idx(q.c, q.i, q.j, q.k)];
+        const double2 x = X[off + e];
+        X[off + e] = make_double2(x.x + (double)d.x * inv, x.y + (double)d.y * inv);
+    }
+}
+
+// an edge array (sigma) and a node array (signed weights) in FP32 on the
+// padded layout; the destinations are zeroed first by the caller
+__global__ void __launch_bounds__(kThreads) k_to_padded(Geo<double> g, const double *src, PadLayout pl, float *dst)
+{
+    for (int e = blockIdx.x * kThreads + threadIdx.x; e < g.nE; e += gridDim.x * kThreads) {
+        const EdgeIdx q = edge_decode(g, e);
+        dst[pl.idx(q.c, q.i, q.j, q.k)] = (float)src[e];
+    }
+}
+__global__ void __launch_bounds__(kThreads) k_nodes_to_padded(Geo<double> g, const double *src, PadLayout pl,
+                                                              float *dst)
+{
+    for (int n = blockIdx.x * kThreads + threadIdx.x; n < g.nN; n += gridDim.x * kThreads) {
+        const int i = n % (g.nx + 1), t = n / (g.nx + 1), j = t % (g.ny + 1), k = t / (g.ny + 1);
+        dst[pl.idx(0, i, j, k)] = (float)src[n];
+    }
+}
+
 // ||b||^2 per right-hand side (FP64 interior system)
 __global__ void __launch_bounds__(kThreads) k_norm_b(KArgs<double> a)
 {
@@ -1056,6 +1108,10 @@ template void launch_gd_add<double>(const KArgs<double> &, double2 *, const doub
 template <typename T> void launch_bicg_init(const KArgs<T> &a, int nrhs, cudaStream_t s)
 {
     if (a.jinv) launch_colb_jacobi(a, nrhs, s);
+    if (a.colstencil == 3) {
+        if constexpr (sizeof(T) == 4) launch_tma_init(a, a.tma, nrhs, s);
+        return;
+    }
     if (a.colstencil == 2) {
         launch_stage_init(a, nrhs, s);
         return;
@@ -1073,12 +1129,14 @@ void launch_bicg_iter(const KArgs<T> &a, int nrhs, cudaStream_t s, cudaEvent_t *
 {
     counted(a.colstencil ? 3 : 5);
     dim3 grid(a.nblk, nrhs);
-    const bool staged = a.colstencil == 2;
+    const bool staged = a.colstencil >= 2;
     kb_p<T><<<grid, kThreads, 0, s>>>(a);
     if (pc) launch_col_prec(*pc, a.p, a.ph, nrhs, s);
     if (a.gd && !staged) launch_gd_phi(a, a.ph, a.phi, 0, nrhs, s);
     if (ev) cudaEventRecord(ev[0], s);
-    if (staged) launch_stage_vt(a, 0, nrhs, s);
+    if (a.colstencil == 3) {
+        if constexpr (sizeof(T) == 4) launch_tma_vt(a, a.tma, 0, nrhs, s);
+    } else if (staged) launch_stage_vt(a, 0, nrhs, s);
     else if (a.colstencil) launch_colb_vt(a, 0, nrhs, s);
     else kb_v<T><<<grid, kThreads, 0, s>>>(a);
     if (ev) cudaEventRecord(ev[1], s);
@@ -1086,7 +1144,9 @@ void launch_bicg_iter(const KArgs<T> &a, int nrhs, cudaStream_t s, cudaEvent_t *
     if (pc) launch_col_prec(*pc, a.s, a.sh, nrhs, s);
     if (a.gd && !staged) launch_gd_phi(a, a.sh, a.phi, 0, nrhs, s);
     if (ev) cudaEventRecord(ev[2], s);
-    if (staged) launch_stage_vt(a, 1, nrhs, s);
+    if (a.colstencil == 3) {
+        if constexpr (sizeof(T) == 4) launch_tma_vt(a, a.tma, 1, nrhs, s);
+    } else if (staged) launch_stage_vt(a, 1, nrhs, s);
     else if (a.colstencil) launch_colb_vt(a, 1, nrhs, s);
     else kb_t<T><<<grid, kThreads, 0, s>>>(a);
     if (ev) cudaEventRecord(ev[3], s);
@@ -1131,6 +1191,28 @@ void launch_cast(const OuterState *ost, int nE, size_t stride, const double2 *r6
 {
     counted(1);
     km_cast<<<dim3(grid_for(nE), nrhs), kThreads, 0, s>>>(ost, nE, stride, r64, b32, x32);
+}
+void launch_cast_padded(const Geo<double> &g, const OuterState *ost, size_t stride64, const double2 *r64,
+                        PadLayout pl, float2 *b32, float2 *x32, int nrhs, cudaStream_t s)
+{
+    counted(1);
+    km_cast_p<<<dim3(grid_for(g.nE), nrhs), kThreads, 0, s>>>(g, ost, stride64, r64, pl, b32, x32);
+}
+void launch_update_padded(const Geo<double> &g, const OuterState *ost, size_t stride64, PadLayout pl,
+                          const float2 *d32, double2 *X, int nrhs, cudaStream_t s)
+{
+    counted(1);
+    km_update_p<<<dim3(grid_for(g.nE), nrhs), kThreads, 0, s>>>(g, ost, stride64, pl, d32, X);
+}
+void launch_to_padded(const Geo<double> &g, const double *src, PadLayout pl, float *dst, cudaStream_t s)
+{
+    counted(1);
+    k_to_padded<<<grid_for(g.nE), kThreads, 0, s>>>(g, src, pl, dst);
+}
+void launch_nodes_to_padded(const Geo<double> &g, const double *src, PadLayout pl, float *dst, cudaStream_t s)
+{
+    counted(1);
+    k_nodes_to_padded<<<grid_for(g.nN), kThreads, 0, s>>>(g, src, pl, dst);
 }
 void launch_update(const OuterState *ost, int nE, size_t stride, const float2 *d32, double2 *X, int nrhs, cudaStream_t s)
 {

@@ -4,6 +4,18 @@
 
 namespace mt3d {
 
+// Padded layout of the FP32 Krylov vectors for the TMA-staged kernels: each
+// component is a Px x Py x Pz block (Px = nx + 1 rounded up to 4, Py = ny + 1,
+// Pz = nz + 1), entry (c, i, j, k) at ((c Pz + k) Py + j) Px + i; entries
+// outside the component's range are zero.  Rows are 16-byte multiples, which
+// the TMA tensor maps need and the reference's own order (rows of nx and
+// nx + 1) does not give.
+struct PadLayout {
+    int Px, Py, Pz;
+    __host__ __device__ int idx(int c, int i, int j, int k) const { return ((c * Pz + k) * Py + j) * Px + i; }
+    __host__ __device__ long long len() const { return 3LL * Px * Py * Pz; }
+};
+
 // tiles of kColX x kColY (i, j) columns for the column-marching kernels
 struct ColMap {
     int tiles_x, tiles;
@@ -37,11 +49,19 @@ template <typename T> struct KArgs {
     const T *gdn;  // node weight with the earth flag as its sign (staged kernels)
     C2<T> *phi;
     // stencil kernels: 0 flat, 1 column-marching, 2 shared-memory staged
-    // (grad-div potentials formed inside); the precomputed inverse diagonal
+    // (grad-div potentials formed inside), 3 TMA-staged on the padded layout;
+    // the precomputed inverse diagonal
     int colstencil;
     ColMap cmap;
     C2<T> *jinv;
     double dsgn;  // ISIGN (-1) for A, +1 for the conjugate transpose
+    // entries per right-hand side swept by the elementwise kernels (nE, or
+    // the padded length) and the padded layout of the vectors (padded != 0)
+    int len;
+    int padded;
+    PadLayout pl;
+    int *err;  // set by a bounded device-side wait that gave up
+    const struct TmaMaps *tma;  // host pointer: tensor maps of the padded vectors (colstencil == 3)
 };
 
 // arguments of the divergence-correction kernels (FP64)
@@ -95,6 +115,21 @@ template <typename T> void launch_colb_jacobi(const KArgs<T> &a, int nrhs, cudaS
 template <typename T> void launch_stage_init(const KArgs<T> &a, int nrhs, cudaStream_t s);
 template <typename T> void launch_stage_vt(const KArgs<T> &a, int which, int nrhs, cudaStream_t s);
 void launch_stage_res64(const KArgs<double> &a, int nrhs, cudaStream_t s);
+// TMA-staged FP32 stencil kernels on the padded layout (colstencil == 3):
+// tensor maps of the input vectors, of sigma and of the signed node weights
+struct TmaMaps;
+int tma_maps_build(TmaMaps *m, const float2 *x0, const float2 *ph, const float2 *sh, const float *sig,
+                   const float *gdn, PadLayout pl, int nrhs);
+TmaMaps *tma_maps_new();
+void tma_maps_free(TmaMaps *m);
+void launch_tma_init(const KArgs<float> &a, const TmaMaps *m, int nrhs, cudaStream_t s);
+void launch_tma_vt(const KArgs<float> &a, const TmaMaps *m, int which, int nrhs, cudaStream_t s);
+void launch_cast_padded(const Geo<double> &g, const OuterState *ost, size_t stride64, const double2 *r64,
+                        PadLayout pl, float2 *b32, float2 *x32, int nrhs, cudaStream_t s);
+void launch_update_padded(const Geo<double> &g, const OuterState *ost, size_t stride64, PadLayout pl,
+                          const float2 *d32, double2 *X, int nrhs, cudaStream_t s);
+void launch_to_padded(const Geo<double> &g, const double *src, PadLayout pl, float *dst, cudaStream_t s);
+void launch_nodes_to_padded(const Geo<double> &g, const double *src, PadLayout pl, float *dst, cudaStream_t s);
 int stage_chunks(int nz, int tiles, int resident);
 template <typename T> void launch_cocg_iter(const ColArgs<T> &a, int nrhs, cudaStream_t s, cudaEvent_t *ev = nullptr);
 

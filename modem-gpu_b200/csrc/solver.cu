@@ -38,6 +38,7 @@ Solver::~Solver()
 {
     cudaSetDevice(dev_);
     if (stream_) cudaStreamSynchronize(stream_);
+    if (tma_) tma_maps_free(tma_);
     for (cudaEvent_t e : ev_) cudaEventDestroy(e);
     if (own_stream_) cudaStreamDestroy(own_stream_);
 }
@@ -156,6 +157,11 @@ int Solver::create(int dev, int nx_, int ny_, int nz_, int nzAir_, const double 
     if ((rc = check(cudaStreamCreateWithFlags(&own_stream_, cudaStreamNonBlocking), "cudaStreamCreate"))) return rc;
     stream_ = own_stream_;
 
+    pl_.Px = (nx + 1 + 3) / 4 * 4;
+    pl_.Py = ny + 1;
+    pl_.Pz = nz + 1;
+    if (errf_.alloc(sizeof(int))) return fail(8, "mt3d_create: out of device memory");
+    cudaMemset(errf_.as<void>(), 0, sizeof(int));
     dx_.assign(dx, dx + nx); dy_.assign(dy, dy + ny); dz_.assign(dz, dz + nz);
     deltas(dx_, delX_); deltas(dy_, delY_); deltas(dz_, delZ_);
     // tables: dx dy dz delX delY delZ rdx rdy rdz
@@ -374,9 +380,45 @@ int Solver::update_cond(const double *m_earth, double airCond)
     if ((rc = check(cudaMemcpyAsync(coef_.as<void>(), coef.data(), coef.size() * sizeof(double), cudaMemcpyHostToDevice, stream_),
                     "copy div-corr coefficients")))
         return rc;
+    // sigma of both formulations and the signed node weights on the padded
+    // layout (FP32), for the TMA-staged kernels
+    const size_t pe = (size_t)pl_.len(), pn = (size_t)pl_.Px * pl_.Py * pl_.Pz;
+    if (sigP32_.alloc(pe * sizeof(float)) || sigsP32_.alloc(pe * sizeof(float)) || gdnP32_.alloc(pn * sizeof(float)))
+        return fail(8, "mt3d_update_cond: out of device memory");
+    cudaMemsetAsync(sigP32_.as<void>(), 0, pe * sizeof(float), stream_);
+    cudaMemsetAsync(sigsP32_.as<void>(), 0, pe * sizeof(float), stream_);
+    cudaMemsetAsync(gdnP32_.as<void>(), 0, pn * sizeof(float), stream_);
+    launch_to_padded(g64_, sig64_.as<double>(), pl_, sigP32_.as<float>(), stream_);
+    launch_to_padded(g64_, sigs64_.as<double>(), pl_, sigsP32_.as<float>(), stream_);
+    launch_nodes_to_padded(g64_, gdn64_.as<double>(), pl_, gdnP32_.as<float>(), stream_);
+    tma_stale_ = true;
     if ((rc = sync("mt3d_update_cond"))) return rc;
     cond_set = true;
     return 0;
+}
+
+// tensor maps of the padded FP32 vectors, rebuilt after the workspace or the
+// conductivity changed
+int Solver::tma_ready()
+{
+    if (!tma_stale_) return 0;
+    if (!tma_) tma_ = tma_maps_new();
+    Workspace &w = ws_;
+    if (tma_maps_build(tma_, w.f_x0.as<float2>(), w.f_ph.as<float2>(), w.f_sh.as<float2>(),
+                       (ctl.formulation == 1 ? sigsP32_ : sigP32_).as<float>(), gdnP32_.as<float>(), pl_, w.nrhs))
+        return fail(4, "cuTensorMapEncodeTiled failed for the padded FP32 vectors");
+    tma_stale_ = false;
+    return 0;
+}
+
+// a bounded device-side wait gave up (MT3D_DEVICE_TIMEOUT)
+int Solver::check_device_error(const char *what)
+{
+    int e = 0;
+    cudaMemcpy(&e, errf_.as<void>(), sizeof(int), cudaMemcpyDeviceToHost);
+    if (!e) return 0;
+    cudaMemset(errf_.as<void>(), 0, sizeof(int));
+    return fail(6, std::string(what) + ": a bounded device-side wait gave up");
 }
 
 int Solver::update_freq(double w)
@@ -429,8 +471,12 @@ int Solver::ensure_workspace(int nrhs, int precision)
     if (ws_.nrhs >= nrhs && ws_.precision == precision && ws_.rlen == rlen && ws_.dlen == dlen &&
         ws_.solver == ctl.solver && ws_.formulation == ctl.formulation)
         return 0;
+    tma_stale_ = true;
     Workspace &w = ws_;
-    const size_t e64 = (size_t)nrhs * nE * sizeof(double2), e32 = (size_t)nrhs * nE * sizeof(float2);
+    // FP32 vectors on the padded layout for the TMA-staged BiCGStab + diagonal path
+    const bool padded = precision == 1 && ctl.solver == 1;
+    const size_t e64 = (size_t)nrhs * nE * sizeof(double2),
+                 e32 = (size_t)nrhs * (padded ? (size_t)pl_.len() : (size_t)nE) * sizeof(float2);
     const size_t n64 = (size_t)nrhs * nN * sizeof(double2);
     // release everything first so a precision change does not hold both sets
     DevBuf *all[] = {&w.b, &w.X, &w.x1, &w.r, &w.rt, &w.p, &w.v, &w.ph, &w.s, &w.sh, &w.t, &w.bc, &w.tmp,
@@ -449,6 +495,10 @@ int Solver::ensure_workspace(int nrhs, int precision)
         for (DevBuf *d : v32) err |= d->alloc(e32);
         if (ctl.solver == 3) err |= w.f_zm.alloc(e32) | w.f_zc.alloc(e32);
         if (ctl.solver == 1) err |= w.jinv32.alloc(e32);
+        if (!err && padded) {  // the padding entries must read as zero
+            for (DevBuf *d : v32) cudaMemsetAsync(d->as<void>(), 0, e32, stream_);
+            cudaMemsetAsync(w.jinv32.as<void>(), 0, e32, stream_);
+        }
     }
     if (ctl.formulation == 0) {
         DevBuf *nv[] = {&w.px, &w.pr, &w.pp, &w.pq, &w.phi0};
@@ -480,6 +530,7 @@ int Solver::ensure_workspace(int nrhs, int precision)
     w.dlen = dlen;
     w.solver = ctl.solver;
     w.formulation = ctl.formulation;
+    w.padded = padded;
     return 0;
 }
 
@@ -501,6 +552,8 @@ template <> KArgs<double> Solver::kargs<double>(int nrhs, int)
     a.rerr_stride = ctl.IterPerDivCor + 1;
     a.stride = nE;
     a.nblk = blocks_for(nE, a.chunk);
+    a.len = (int)nE;
+    a.err = errf_.as<int>();
     a.maxit = ctl.IterPerDivCor;
     a.inner = 0;
     a.dsgn = -1.0;
@@ -535,11 +588,22 @@ template <> KArgs<float> Solver::kargs<float>(int nrhs, int)
     a.rerr = w.rerr.as<double>();
     a.rerr_stride = ctl.IterPerDivCor + 1;
     a.stride = nE;
-    a.nblk = blocks_for(nE, a.chunk);
+    a.len = (int)nE;
+    a.err = errf_.as<int>();
+    if (w.padded) {
+        // padded layout: the elementwise kernels sweep the padded length and
+        // the stencil runs on the TMA-staged kernels
+        a.padded = 1;
+        a.pl = pl_;
+        a.len = (int)pl_.len();
+        a.stride = (size_t)pl_.len();
+        a.tma = tma_;
+    }
+    a.nblk = blocks_for(a.len, a.chunk);
     a.maxit = ctl.IterPerDivCor;
     a.inner = 1;
     a.dsgn = -1.0;
-    a.colstencil = 2;
+    a.colstencil = w.padded ? 3 : 2;
     a.cmap = col_map(nx, ny);
     a.jinv = ctl.solver == 1 ? w.jinv32.as<float2>() : nullptr;
     if (ctl.formulation == 1) {
@@ -938,10 +1002,19 @@ int Solver::solve(int nrhs, const double *omegas, const int *trans, const double
                 for (int r = 0; r < nrhs; r++) grp[r].active = os[r].active && !hi[r];
                 cudaMemcpyAsync(w.ost.as<void>(), grp.data(), nrhs * sizeof(OuterState), cudaMemcpyHostToDevice,
                                 stream_);
-                launch_cast(w.ost.as<OuterState>(), (int)nE, nE, w.tmp.as<double2>(), w.f_b.as<float2>(),
-                            w.f_x0.as<float2>(), nrhs, stream_);
+                if (w.padded) {
+                    if ((rc = tma_ready())) return rc;
+                    launch_cast_padded(g64_, w.ost.as<OuterState>(), nE, w.tmp.as<double2>(), pl_, w.f_b.as<float2>(),
+                                       w.f_x0.as<float2>(), nrhs, stream_);
+                } else {
+                    launch_cast(w.ost.as<OuterState>(), (int)nE, nE, w.tmp.as<double2>(), w.f_b.as<float2>(),
+                                w.f_x0.as<float2>(), nrhs, stream_);
+                }
                 if ((rc = run_bicg(nrhs, 1, ctl.IterPerDivCor))) return rc;
-                launch_update(w.ost.as<OuterState>(), (int)nE, nE, w.f_x0.as<float2>(), X, nrhs, stream_);
+                if (w.padded)
+                    launch_update_padded(g64_, w.ost.as<OuterState>(), nE, pl_, w.f_x0.as<float2>(), X, nrhs, stream_);
+                else
+                    launch_update(w.ost.as<OuterState>(), (int)nE, nE, w.f_x0.as<float2>(), X, nrhs, stream_);
             }
             if (n64) {
                 if ((rc = ensure_fp64_krylov(nrhs))) return rc;
@@ -958,6 +1031,7 @@ int Solver::solve(int nrhs, const double *omegas, const int *trans, const double
         cudaMemcpyAsync(bs.data(), w.bst.as<void>(), nrhs * sizeof(BicgState), cudaMemcpyDeviceToHost, stream_);
         cudaMemcpyAsync(rerr.data(), w.rerr.as<void>(), rerr.size() * sizeof(double), cudaMemcpyDeviceToHost, stream_);
         if ((rc = sync("fwdsolve Krylov cycle"))) return rc;
+        if ((rc = check_device_error("fwdsolve Krylov cycle"))) return rc;
         if (prof_) collect_events();
         for (int r = 0; r < nrhs; r++) {
             OuterState &o = os[r];

@@ -49,6 +49,7 @@ struct Workspace {
     int rlen = 0, dlen = 0;  // rerr row lengths the buffers were sized for
     int solver = 0;
     int formulation = 0;
+    bool padded = false;  // FP32 vectors on the padded layout (TMA-staged kernels)
     // FP64 edge vectors [nrhs][nE]
     DevBuf b, X, x1, r, rt, p, v, ph, s, sh, t, bc, tmp;
     // FP32 edge vectors (mixed)
@@ -115,6 +116,15 @@ class Solver {
     Geo<float> g32_{};
     DevBuf tab64_, tab32_, sig64_, sig32_, coef_, edgei_d_;
     DevBuf sigs64_, sigs32_, gdw64_, gdw32_, gde_, gdn64_, gdn32_;  // grad-div (SP2) data
+    // padded FP32 layout of the TMA-staged kernels: sigma of both
+    // formulations, signed node weights, the tensor maps and a device flag
+    // that bounded waits set
+    PadLayout pl_{};
+    DevBuf sigP32_, sigsP32_, gdnP32_, errf_;
+    TmaMaps *tma_ = nullptr;
+    bool tma_stale_ = true;
+    int tma_ready();
+    int check_device_error(const char *what);
     Workspace ws_;
     std::vector<double> dx_, dy_, dz_, delX_, delY_, delZ_;
 };
