@@ -284,10 +284,10 @@ def stencil_bytes(kprec: int, nE: int, nN: int) -> float:
     return 3 * sc + sr + sr * nN / nE
 
 
-# DRAM bytes (read + write) per edge and right-hand side of one kcs_vt<float>
-# launch, measured by ncu on the 200x200x100 workload with 8 right-hand sides
+# DRAM bytes (read + write) per edge and right-hand side of one kct_vt launch,
+# measured by ncu on the 200x200x100 workload with 8 right-hand sides
 # (profiles/launches_200x200x100_8rhs.md)
-TRAFFIC_PER_EDGE_RHS = 28.6
+TRAFFIC_PER_EDGE_RHS = 28.7
 
 
 def main():
@@ -408,7 +408,8 @@ def main():
     traffic = (TRAFFIC_PER_EDGE_RHS * units / kn) if (TRAFFIC_PER_EDGE_RHS and kn) else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                "kernel": "kcs_vt (staged stencil + grad-div + fused dots), " + ("FP32" if kprec else "FP64") + " complex",
+                "kernel": ("kct_vt (TMA-staged stencil + grad-div + fused dots), FP32" if kprec else
+                           "kcs_vt (cp.async-staged stencil + grad-div + fused dots), FP64") + " complex",
                 "peak_kind": peak_kind, "timed_launches": kn, "bytes_per_edge_rhs": alg / units if units else None,
                 "algorithmic_bytes_per_launch": alg / kn if kn else None}
 
