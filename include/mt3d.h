@@ -218,6 +218,22 @@ MT3D_API int mt3d_get_batch_diag(mt3d_handle h, int nrhs, int *niter, double *re
 MT3D_API int mt3d_pmult_t(mt3d_handle h, int npol, const double *e0, const double *eadj, const double *m0_earth,
                  double *dm);
 
+/* Full impedance tensor at nsite sites from the fields of the two
+ * polarisations at angular frequency omega: dataResp for Full_Impedance
+ * (f90/3D_MT/DataFunc.f90:143-189) with the interpolation functionals
+ * EinterpSetUp and BfromESetUp (f90/3D_MT/EMfieldInterp.f90:141-324,
+ * 470-647), site azimuths zero.  xyz holds x, y, z per site (z positive down,
+ * 0 at the Earth's surface) in the frame of the grid origin `origin` (ox, oy,
+ * oz of the reference's grid: the first x and y nodes and the surface depth);
+ * e1, e2 are full edge vectors (polarisations 1 and 2).  Z receives
+ * Zxx, Zxy, Zyx, Zyy (complex, interleaved) per site: E / B in SI units. */
+MT3D_API int mt3d_impedance(mt3d_handle h, double omega, int nsite, const double *xyz, const double *origin,
+                            const double *e1, const double *e2, double *Z);
+/* As mt3d_impedance with e1 and e2 in device memory of the handle's device
+ * (the fields stay in HBM; only the sites and Z cross the bus). */
+MT3D_API int mt3d_impedance_device(mt3d_handle h, double omega, int nsite, const double *xyz, const double *origin,
+                                   const double *e1_dev, const double *e2_dev, double *Z);
+
 /* Number of kernels the library has launched in this process (all handles). */
 MT3D_API int64_t mt3d_launch_counter(void);
 

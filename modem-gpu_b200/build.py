@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libmt3d.so")
-SOURCES = ["kernels.cu", "colkernels.cu", "stagekernels.cu", "tmakernels.cu", "solver.cu", "noalloc.cu", "capi.cu"]
+SOURCES = ["kernels.cu", "colkernels.cu", "stagekernels.cu", "tmakernels.cu", "datafunc.cu", "solver.cu", "noalloc.cu", "capi.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

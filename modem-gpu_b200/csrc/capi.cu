@@ -169,6 +169,18 @@ int mt3d_mult_aii_device_noalloc(mt3d_handle h, int adjt, const double *x, doubl
     return wrap(h, [&] { return h->s.mult_aii_noalloc(adjt, x, y); });
 }
 
+int mt3d_impedance(mt3d_handle h, double omega, int nsite, const double *xyz, const double *origin, const double *e1,
+                   const double *e2, double *Z)
+{
+    return wrap(h, [&] { return h->s.impedance(omega, nsite, xyz, origin, e1, e2, Z, false); });
+}
+
+int mt3d_impedance_device(mt3d_handle h, double omega, int nsite, const double *xyz, const double *origin,
+                          const double *e1_dev, const double *e2_dev, double *Z)
+{
+    return wrap(h, [&] { return h->s.impedance(omega, nsite, xyz, origin, e1_dev, e2_dev, Z, true); });
+}
+
 int mt3d_bicg(mt3d_handle h, const double *b, double *x, int maxit, double tol, int *niter, double *rerr, int *failed)
 {
     return wrap(h, [&] { return h->s.bicg(b, x, maxit, tol, niter, rerr, failed); });

@@ -77,6 +77,8 @@ class Solver {
     int profile(int enable);
     int kernel_time(int *launches, double *ms, int *precision);
     int pmult_t(int npol, const double *e0, const double *eadj, const double *m0, double *dm);
+    int impedance(double omega, int nsite, const double *xyz, const double *origin, const double *e1, const double *e2,
+                  double *Z, bool device);
 
     int fail(int code, const std::string &msg);
     std::string last_error;

@@ -27,7 +27,7 @@ EXPORTS = ["mt3d_version", "mt3d_device_count", "mt3d_create", "mt3d_destroy", "
            "mt3d_update_freq", "mt3d_set_formulation", "mt3d_sizes", "mt3d_interior_index", "mt3d_mult_aii",
            "mt3d_mult_aii_device_noalloc", "mt3d_bicg", "mt3d_fwdsolve",
            "mt3d_fwdsolve_batch", "mt3d_fwdsolve_batch_device", "mt3d_set_stream", "mt3d_profile",
-           "mt3d_kernel_time", "mt3d_get_diag", "mt3d_get_batch_diag", "mt3d_pmult_t", "mt3d_launch_counter", "mt3d_last_error"]
+           "mt3d_kernel_time", "mt3d_get_diag", "mt3d_get_batch_diag", "mt3d_pmult_t", "mt3d_impedance", "mt3d_impedance_device", "mt3d_launch_counter", "mt3d_last_error"]
 
 _lib = None
 
@@ -62,6 +62,8 @@ def load(path: str = LIB_PATH):
     L.mt3d_interior_index.argtypes = [P, C.POINTER(C.c_int32)]
     L.mt3d_mult_aii.argtypes = [P, I, D, D]
     L.mt3d_mult_aii_device_noalloc.argtypes = [P, I, C.c_void_p, C.c_void_p]
+    L.mt3d_impedance.argtypes = [P, C.c_double, I, D, D, D, D, D]
+    L.mt3d_impedance_device.argtypes = [P, C.c_double, I, D, D, C.c_void_p, C.c_void_p, D]
     L.mt3d_bicg.argtypes = [P, D, D, I, C.c_double, IP, D, IP]
     L.mt3d_fwdsolve.argtypes = [P, I, D, D, D]
     L.mt3d_fwdsolve_batch.argtypes = [P, I, D, IP, D, D, D, IP]
@@ -159,6 +161,23 @@ class Solver:
         device address, e.g. a torch tensor's data_ptr()); enqueued on the
         handle's stream, no device allocation."""
         self._check(self.L.mt3d_mult_aii_device_noalloc(self.h, int(adjt), C.c_void_p(x_ptr), C.c_void_p(y_ptr)))
+
+    def impedance(self, omega, sites, e1, e2, origin=(0.0, 0.0, 0.0)):
+        """Full impedance tensors [nsite, 2, 2] (E / B, SI) at sites [nsite, 3]
+        from the full edge fields e1, e2 of the two polarisations (host
+        arrays, or device addresses as ints)."""
+        xyz = np.ascontiguousarray(sites, np.float64).reshape(-1, 3)
+        org = np.ascontiguousarray(origin, np.float64)
+        Z = np.zeros(4 * len(xyz), np.complex128)
+        if isinstance(e1, int):
+            rc = self.L.mt3d_impedance_device(self.h, float(omega), len(xyz), _d(xyz), _d(org), C.c_void_p(e1),
+                                              C.c_void_p(e2), _d(Z))
+        else:
+            a = np.ascontiguousarray(e1, np.complex128)
+            b = np.ascontiguousarray(e2, np.complex128)
+            rc = self.L.mt3d_impedance(self.h, float(omega), len(xyz), _d(xyz), _d(org), _d(a), _d(b), _d(Z))
+        self._check(rc)
+        return Z.reshape(-1, 2, 2)
 
     def bicg(self, b, x0, maxit, tol):
         b = np.ascontiguousarray(b, np.complex128)

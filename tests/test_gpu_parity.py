@@ -425,3 +425,55 @@ def test_mixed_cycles_fall_back_to_fp64(gprob):
     mask = earth_mask(g, m)
     for r in range(2):
         assert relerr(em_[r][mask], e64[r][mask]) < 1e-5
+
+
+# ---------------------------------------------------------------------------
+# Full_Impedance data functional (mt3d_impedance) against oracle/datafunc.py
+# ---------------------------------------------------------------------------
+def test_impedance_matches_oracle(prob):
+    import torch
+    from oracle import datafunc as df
+    g, m, omega, o, s = prob
+    origin = (-1000.0, -800.0, 0.0)
+    c = df.coords(g.dx, g.dy, g.dz, g.nzAir, origin)
+    rng = np.random.default_rng(8)
+    e1 = rng.standard_normal(g.n_edges) + 1j * rng.standard_normal(g.n_edges)
+    e2 = rng.standard_normal(g.n_edges) + 1j * rng.standard_normal(g.n_edges)
+    sites = np.column_stack([rng.uniform(c["xC"][2], c["xC"][g.nx - 1], 12),
+                             rng.uniform(c["yC"][2], c["yC"][g.ny - 1], 12),
+                             np.concatenate([np.zeros(8), rng.uniform(10.0, 400.0, 4)])])
+    zo = df.impedance(c, omega, sites, e1, e2)
+    zg = s.impedance(omega, sites, e1, e2, origin)
+    assert relerr(zg, zo) < 1e-12
+    d1, d2 = torch.from_numpy(e1).cuda(), torch.from_numpy(e2).cuda()
+    zd = s.impedance(omega, sites, d1.data_ptr(), d2.data_ptr(), origin)
+    assert relerr(zd, zo) < 1e-12
+
+
+def test_impedance_of_halfspace_solution(cuda):
+    """Both polarisations solved on a 30 ohm-m halfspace at 10 Hz: Zxx = Zyy = 0,
+    Zxy = -Zyx, and |Zxy| = sqrt(omega rho / mu0) with phase 45 degrees, to the
+    grid's discretisation error (5 % in modulus, 3 degrees in phase)."""
+    g = small_grid()
+    rho = 30.0
+    m = models.halfspace_model(g, rho)
+    omega = 2 * np.pi * 10.0
+    s = capi.Solver(g)
+    s.update_cond(m.m_earth, m.air_cond)
+    s.update_freq(omega)
+    s.set_control(tolEMfwd=1e-9)
+    e = [s.fwdsolve(bc=mbc.boundary_1d(m, omega, mode))[0] for mode in (1, 2)]
+    from oracle import datafunc as df
+    c = df.coords(g.dx, g.dy, g.dz, g.nzAir)
+    sites = np.array([[c["xC"][5], c["yC"][6], 0.0], [c["xC"][4] + 50.0, c["yC"][7] - 30.0, 0.0]])
+    Z = s.impedance(omega, sites, e[0], e[1])
+    mu0 = 4e-7 * np.pi
+    zabs = np.sqrt(omega * rho / mu0)
+    for z in Z:
+        assert abs(z[0, 0]) < 1e-6 * zabs and abs(z[1, 1]) < 1e-6 * zabs
+        assert abs(z[0, 1] + z[1, 0]) < 1e-6 * zabs
+        assert abs(abs(z[0, 1]) / zabs - 1) < 0.05
+        ph = np.degrees(np.angle(z[0, 1])) % 180.0
+        assert min(abs(ph - 45.0), abs(ph - 135.0)) < 3.0
+    zo = df.impedance(c, omega, sites, e[0], e[1])
+    assert relerr(Z, zo) < 1e-12

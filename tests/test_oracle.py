@@ -191,3 +191,57 @@ def test_sp2_restatement_matches_ccdc():
     eo, rc = o.fwdsolve(bc=bcv)
     em = earth_mask(g, m)
     assert conv and rc == 0 and relerr(e[em], eo[em]) < 1e-6
+
+
+# ---------------------------------------------------------------------------
+# Full_Impedance data functional (oracle/datafunc.py)
+# ---------------------------------------------------------------------------
+def _linear_fields(c, f):
+    """Full edge vectors holding f(x, y, z) at the edge midpoints, per component."""
+    from oracle import datafunc as df
+    nx, ny, nz = c["n"]
+    nE = nx * (ny + 1) * (nz + 1) + (nx + 1) * ny * (nz + 1) + (nx + 1) * (ny + 1) * nz
+    out = []
+    for comp in (1, 2, 3):
+        e = np.zeros(nE, complex)
+        X = c["xC"] if comp == 1 else c["xE"]
+        Y = c["yC"] if comp == 2 else c["yE"]
+        Zc = c["zC"] if comp == 3 else c["zE"]
+        ni, nj, nk = (nx if comp == 1 else nx + 1), (ny if comp == 2 else ny + 1), (nz if comp == 3 else nz + 1)
+        for k in range(1, nk + 1):
+            for j in range(1, nj + 1):
+                for i in range(1, ni + 1):
+                    e[df.flat(c, comp, i, j, k)] = f(X[i], Y[j], Zc[k])
+        out.append(e)
+    return out
+
+
+def test_datafunc_interpolation_exact_for_linear_fields():
+    from oracle import datafunc as df
+    g = small_grid()
+    c = df.coords(g.dx, g.dy, g.dz, g.nzAir, origin=(-2000.0, -1500.0, 0.0))
+    f = lambda X, Y, Z: 1.0 + 2e-3 * X - 1e-3 * Y + 5e-4 * Z
+    ex, ey, _ = _linear_fields(c, f)
+    rng = np.random.default_rng(4)
+    for _ in range(10):
+        x = np.array([rng.uniform(c["xC"][2], c["xC"][g.nx - 1]), rng.uniform(c["yC"][2], c["yC"][g.ny - 1]),
+                      rng.uniform(-50.0, 300.0)])
+        assert abs(df.apply(c, df.e_interp(c, x, 1), ex) - f(*x)) < 1e-12
+        assert abs(df.apply(c, df.e_interp(c, x, 2), ey) - f(*x)) < 1e-12
+
+
+def test_datafunc_b_is_curl_e_over_minus_i_omega():
+    """E_y = a z, E_x = b z: (curl E)_x = -a, (curl E)_y = b, so B = (i ISIGN /
+    omega) curl E exactly at any site."""
+    from oracle import datafunc as df
+    g = small_grid()
+    c = df.coords(g.dx, g.dy, g.dz, g.nzAir)
+    a, b, omega = 3e-4, -2e-4, 2 * np.pi * 0.7
+    ex, _, _ = _linear_fields(c, lambda X, Y, Z: b * Z)
+    _, ey, _ = _linear_fields(c, lambda X, Y, Z: a * Z)
+    e = ex + ey
+    x = np.array([c["xC"][5] + 11.0, c["yC"][6] - 7.0, 0.0])
+    bx = df.apply(c, df.b_from_e(c, omega, x, 1), e)
+    by = df.apply(c, df.b_from_e(c, omega, x, 2), e)
+    assert abs(bx - (-1j / omega) * (-a)) < 1e-12 * abs(a / omega)
+    assert abs(by - (-1j / omega) * b) < 1e-12 * abs(b / omega)
