@@ -234,6 +234,21 @@ MT3D_API int mt3d_impedance(mt3d_handle h, double omega, int nsite, const double
 MT3D_API int mt3d_impedance_device(mt3d_handle h, double omega, int nsite, const double *xyz, const double *origin,
                                    const double *e1_dev, const double *e2_dev, double *Z);
 
+/* Adjoint sources of the Full_Impedance functional: Lrows + LmultT
+ * (f90/3D_MT/DataFunc.f90:465-869, f90/SENS/DataSens.f90:130-225) for the
+ * same sites and background fields e1, e2 as mt3d_impedance.  d holds the
+ * data weights per site (Zxx, Zxy, Zyx, Zyy, complex); s1, s2 (full edge
+ * vectors, overwritten) receive sum_ij conj(d_ij) L_ij,k, the source of the
+ * transposed solve of polarisation k, where L_ij,k = B^-1(k, j) (Le_i -
+ * Z_i1 Lbx - Z_i2 Lby) is the derivative of Z_ij with respect to the field of
+ * polarisation k. */
+MT3D_API int mt3d_lmult_t(mt3d_handle h, double omega, int nsite, const double *xyz, const double *origin,
+                          const double *e1, const double *e2, const double *d, double *s1, double *s2);
+/* As mt3d_lmult_t with e1, e2, s1, s2 in device memory (d and xyz on the host). */
+MT3D_API int mt3d_lmult_t_device(mt3d_handle h, double omega, int nsite, const double *xyz, const double *origin,
+                                 const double *e1_dev, const double *e2_dev, const double *d, double *s1_dev,
+                                 double *s2_dev);
+
 /* Number of kernels the library has launched in this process (all handles). */
 MT3D_API int64_t mt3d_launch_counter(void);
 

@@ -181,6 +181,18 @@ int mt3d_impedance_device(mt3d_handle h, double omega, int nsite, const double *
     return wrap(h, [&] { return h->s.impedance(omega, nsite, xyz, origin, e1_dev, e2_dev, Z, true); });
 }
 
+int mt3d_lmult_t(mt3d_handle h, double omega, int nsite, const double *xyz, const double *origin, const double *e1,
+                 const double *e2, const double *d, double *s1, double *s2)
+{
+    return wrap(h, [&] { return h->s.lmult_t(omega, nsite, xyz, origin, e1, e2, d, s1, s2, false); });
+}
+
+int mt3d_lmult_t_device(mt3d_handle h, double omega, int nsite, const double *xyz, const double *origin,
+                        const double *e1_dev, const double *e2_dev, const double *d, double *s1_dev, double *s2_dev)
+{
+    return wrap(h, [&] { return h->s.lmult_t(omega, nsite, xyz, origin, e1_dev, e2_dev, d, s1_dev, s2_dev, true); });
+}
+
 int mt3d_bicg(mt3d_handle h, const double *b, double *x, int maxit, double tol, int *niter, double *rerr, int *failed)
 {
     return wrap(h, [&] { return h->s.bicg(b, x, maxit, tol, niter, rerr, failed); });

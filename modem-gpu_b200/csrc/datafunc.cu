@@ -9,6 +9,7 @@
 // reference does per site), the dot products with the fields and the 2 x 2
 // inversions run on the device, so the fields never leave HBM.  Site
 // azimuths are zero (the reference's rotate_Model2Data with zero angles).
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <string>
@@ -202,9 +203,44 @@ static long long edge_flat(int nx, int ny, int nz, const Term &t)
     return (i <= nx && j <= ny && k < nz) ? nXe + nYe + i + (long long)(nx + 1) * (j + (long long)(ny + 1) * k) : -1;
 }
 
-// one thread per site: the 4 functionals on both polarisations, Kramer's rule
-__global__ void k_impedance(int nsite, const int *off, const int *idx, const double2 *coef, const double2 *e1,
-                            const double2 *e2, double2 *Z)
+// the four functionals (Ex, Ey, Bx, By) of every site as CSR rows 4 s + f
+static int build_functionals(const Coords &c, int nx, int ny, int nz, double om, int nsite, const double *xyz,
+                             std::vector<int> &off, std::vector<int> &idx, std::vector<double2> &coef, std::string &err)
+{
+    off.assign(4 * (size_t)nsite + 1, 0);
+    idx.clear();
+    coef.clear();
+    for (int s = 0; s < nsite; s++) {
+        const double *x = xyz + 3 * (size_t)s;
+        if (!std::isfinite(x[0]) || !std::isfinite(x[1]) || !std::isfinite(x[2])) {
+            err = "site coordinates must be finite";
+            return 5;
+        }
+        const std::vector<Term> L[4] = {e_interp(c, nx, ny, nz, x, 1), e_interp(c, nx, ny, nz, x, 2),
+                                        b_from_e(c, nx, ny, nz, om, x, 1), b_from_e(c, nx, ny, nz, om, x, 2)};
+        for (int f = 0; f < 4; f++) {
+            for (const Term &t : L[f]) {
+                const long long e = edge_flat(nx, ny, nz, t);
+                if (e < 0) {
+                    err = "site " + std::to_string(s) + " needs an edge outside the grid";
+                    return 5;
+                }
+                idx.push_back((int)e);
+                coef.push_back(make_double2(t.re, t.im));
+            }
+            off[4 * (size_t)s + f + 1] = (int)idx.size();
+        }
+    }
+    return 0;
+}
+
+// per site: the functionals on both polarisations, Z and B^-1 (dataResp);
+// with d non-null also the weights of the four functionals in the adjoint
+// source of each polarisation k (Lrows + LmultT for Full_Impedance,
+// f90/3D_MT/DataFunc.f90:465-869, f90/SENS/DataSens.f90:130-225):
+//   s_k = sum_ij conj(d_ij) B^-1(k, j) (Le_i - Z_i1 Lbx - Z_i2 Lby)
+__global__ void k_site(int nsite, const int *off, const int *idx, const double2 *coef, const double2 *e1,
+                       const double2 *e2, double2 *Z, const double2 *d, double2 *W)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= nsite) return;
@@ -222,59 +258,107 @@ __global__ void k_impedance(int nsite, const int *off, const int *idx, const dou
     }
     // EE(i, m) = v[i][m], BB(i, m) = v[2 + i][m]; BB^-1 by Kramer's rule
     const cd det = cd_sub(cd_mul(v[2][0], v[3][1]), cd_mul(v[2][1], v[3][0]));
-    cd bi[2][2];
+    cd bi[2][2], z[2][2];
     bi[0][0] = cd_div(v[3][1], det);
     bi[1][1] = cd_div(v[2][0], det);
     bi[0][1] = cd_div(cd{-v[2][1].re, -v[2][1].im}, det);
     bi[1][0] = cd_div(cd{-v[3][0].re, -v[3][0].im}, det);
     for (int i = 0; i < 2; i++)
         for (int j = 0; j < 2; j++) {
-            const cd z = cd_add(cd_mul(v[i][0], bi[0][j]), cd_mul(v[i][1], bi[1][j]));
-            Z[4 * (size_t)s + 2 * i + j] = make_double2(z.re, z.im);
+            z[i][j] = cd_add(cd_mul(v[i][0], bi[0][j]), cd_mul(v[i][1], bi[1][j]));
+            if (Z) Z[4 * (size_t)s + 2 * i + j] = make_double2(z[i][j].re, z[i][j].im);
         }
+    if (!d) return;
+    for (int k = 0; k < 2; k++) {
+        cd w[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
+        for (int i = 0; i < 2; i++)
+            for (int j = 0; j < 2; j++) {
+                const double2 dd = d[4 * (size_t)s + 2 * i + j];
+                const cd c = cd_mul(cd{dd.x, -dd.y}, bi[k][j]);  // conj(d_ij) B^-1(k, j)
+                w[i] = cd_add(w[i], c);                          // Lex (i = 0) or Ley (i = 1)
+                w[2] = cd_sub(w[2], cd_mul(c, z[i][0]));         // Lbx
+                w[3] = cd_sub(w[3], cd_mul(c, z[i][1]));         // Lby
+            }
+        for (int f = 0; f < 4; f++) W[(4 * (size_t)s + f) * 2 + k] = make_double2(w[f].re, w[f].im);
+    }
 }
 
-static void launch_impedance(int nsite, const int *off, const int *idx, const double2 *coef, const double2 *e1,
-                             const double2 *e2, double2 *Z, cudaStream_t s)
+// adjoint sources: each distinct edge sums its (site, functional, coefficient)
+// entries in a fixed order (deterministic; no atomics)
+__global__ void k_scatter(int nu, const int *uoff, const int *uedge, const int *urow, const double2 *ucoef,
+                          const double2 *W, double2 *s1, double2 *s2)
 {
-    g_launch_count.fetch_add(1, std::memory_order_relaxed);
-    k_impedance<<<(nsite + 127) / 128, 128, 0, s>>>(nsite, off, idx, coef, e1, e2, Z);
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= nu) return;
+    cd a = {0, 0}, b = {0, 0};
+    for (int q = uoff[u]; q < uoff[u + 1]; q++) {
+        const cd c = {ucoef[q].x, ucoef[q].y};
+        const double2 w0 = W[(size_t)urow[q] * 2], w1 = W[(size_t)urow[q] * 2 + 1];
+        a = cd_add(a, cd_mul(c, cd{w0.x, w0.y}));
+        b = cd_add(b, cd_mul(c, cd{w1.x, w1.y}));
+    }
+    s1[uedge[u]] = make_double2(a.re, a.im);
+    s2[uedge[u]] = make_double2(b.re, b.im);
 }
 
 int Solver::impedance(double om, int nsite, const double *xyz, const double *origin, const double *e1,
                       const double *e2, double *Zout, bool device)
 {
-    if (nsite < 1 || !xyz || !origin || !e1 || !e2 || !Zout || !(om > 0) || !std::isfinite(om))
-        return fail(5, "mt3d_impedance: invalid arguments");
+    return data_functional(om, nsite, xyz, origin, e1, e2, nullptr, Zout, nullptr, nullptr, device);
+}
+
+int Solver::lmult_t(double om, int nsite, const double *xyz, const double *origin, const double *e1, const double *e2,
+                    const double *d, double *s1, double *s2, bool device)
+{
+    if (!d || !s1 || !s2) return fail(5, "mt3d_lmult_t: invalid arguments");
+    return data_functional(om, nsite, xyz, origin, e1, e2, d, nullptr, s1, s2, device);
+}
+
+int Solver::data_functional(double om, int nsite, const double *xyz, const double *origin, const double *e1,
+                            const double *e2, const double *d, double *Zout, double *s1, double *s2, bool device)
+{
+    const char *who = d ? "mt3d_lmult_t" : "mt3d_impedance";
+    if (nsite < 1 || !xyz || !origin || !e1 || !e2 || !(om > 0) || !std::isfinite(om) || (!d && !Zout))
+        return fail(5, std::string(who) + ": invalid arguments");
     const Coords c = make_coords(dx_, dy_, dz_, delX_, delY_, delZ_, nzAir, origin);
-    std::vector<int> off(4 * (size_t)nsite + 1, 0), idx;
+    std::vector<int> off, idx;
     std::vector<double2> coef;
-    for (int s = 0; s < nsite; s++) {
-        const double *x = xyz + 3 * (size_t)s;
-        if (!std::isfinite(x[0]) || !std::isfinite(x[1]) || !std::isfinite(x[2]))
-            return fail(5, "mt3d_impedance: site coordinates must be finite");
-        const std::vector<Term> L[4] = {e_interp(c, nx, ny, nz, x, 1), e_interp(c, nx, ny, nz, x, 2),
-                                        b_from_e(c, nx, ny, nz, om, x, 1), b_from_e(c, nx, ny, nz, om, x, 2)};
-        for (int f = 0; f < 4; f++) {
-            for (const Term &t : L[f]) {
-                const long long e = edge_flat(nx, ny, nz, t);
-                if (e < 0) {
-                    char buf[160];
-                    snprintf(buf, sizeof buf, "mt3d_impedance: site %d needs an edge outside the grid", s);
-                    return fail(5, buf);
-                }
-                idx.push_back((int)e);
-                coef.push_back(make_double2(t.re, t.im));
+    std::string err;
+    if (int rc = build_functionals(c, nx, ny, nz, om, nsite, xyz, off, idx, coef, err))
+        return fail(rc, std::string(who) + ": " + err);
+    // transposed rows for the adjoint sources: entries grouped by edge in
+    // (site, functional, term) order
+    std::vector<int> uoff, uedge, urow;
+    std::vector<double2> ucoef;
+    if (d) {
+        std::vector<int> order(idx.size());
+        for (size_t q = 0; q < idx.size(); q++) order[q] = (int)q;
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return idx[a] < idx[b]; });
+        std::vector<int> row(idx.size());
+        for (size_t r = 0; r + 1 < off.size(); r++)
+            for (int q = off[r]; q < off[r + 1]; q++) row[q] = (int)r;
+        for (size_t n = 0; n < order.size(); n++) {
+            const int q = order[n];
+            if (uedge.empty() || uedge.back() != idx[q]) {
+                uedge.push_back(idx[q]);
+                uoff.push_back((int)n);
             }
-            off[4 * (size_t)s + f + 1] = (int)idx.size();
+            urow.push_back(row[q]);
+            ucoef.push_back(coef[q]);
         }
+        uoff.push_back((int)order.size());
     }
-    DevBuf doff, didx, dcoef, dz, de1, de2;
     const size_t eb = (size_t)nE * sizeof(double2);
-    if (doff.alloc(off.size() * sizeof(int)) || didx.alloc(idx.size() * sizeof(int)) ||
-        dcoef.alloc(coef.size() * sizeof(double2)) || dz.alloc(4 * (size_t)nsite * sizeof(double2)) ||
-        (!device && (de1.alloc(eb) || de2.alloc(eb))))
-        return fail(8, "mt3d_impedance: out of device memory");
+    DevBuf doff, didx, dcoef, dz, de1, de2, dd, dw, duoff, duedge, durow, ducoef, ds1, ds2;
+    int bad = doff.alloc(off.size() * sizeof(int)) || didx.alloc(idx.size() * sizeof(int)) ||
+              dcoef.alloc(coef.size() * sizeof(double2)) || (!device && (de1.alloc(eb) || de2.alloc(eb)));
+    if (Zout) bad = bad || dz.alloc(4 * (size_t)nsite * sizeof(double2));
+    if (d)
+        bad = bad || dd.alloc(4 * (size_t)nsite * sizeof(double2)) || dw.alloc(8 * (size_t)nsite * sizeof(double2)) ||
+              duoff.alloc(uoff.size() * sizeof(int)) || duedge.alloc(uedge.size() * sizeof(int)) ||
+              durow.alloc(urow.size() * sizeof(int)) || ducoef.alloc(ucoef.size() * sizeof(double2)) ||
+              (!device && (ds1.alloc(eb) || ds2.alloc(eb)));
+    if (bad) return fail(8, std::string(who) + ": out of device memory");
     cudaMemcpyAsync(doff.as<void>(), off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice, stream_);
     cudaMemcpyAsync(didx.as<void>(), idx.data(), idx.size() * sizeof(int), cudaMemcpyHostToDevice, stream_);
     cudaMemcpyAsync(dcoef.as<void>(), coef.data(), coef.size() * sizeof(double2), cudaMemcpyHostToDevice, stream_);
@@ -285,10 +369,35 @@ int Solver::impedance(double om, int nsite, const double *xyz, const double *ori
         p1 = de1.as<double2>();
         p2 = de2.as<double2>();
     }
-    launch_impedance(nsite, doff.as<int>(), didx.as<int>(), dcoef.as<double2>(), p1, p2, dz.as<double2>(), stream_);
-    cudaMemcpyAsync(Zout, dz.as<void>(), 4 * (size_t)nsite * sizeof(double2), cudaMemcpyDeviceToHost, stream_);
-    return sync("mt3d_impedance");
+    double2 *q1 = nullptr, *q2 = nullptr;
+    if (d) {
+        cudaMemcpyAsync(dd.as<void>(), d, 4 * (size_t)nsite * sizeof(double2), cudaMemcpyHostToDevice, stream_);
+        cudaMemcpyAsync(duoff.as<void>(), uoff.data(), uoff.size() * sizeof(int), cudaMemcpyHostToDevice, stream_);
+        cudaMemcpyAsync(duedge.as<void>(), uedge.data(), uedge.size() * sizeof(int), cudaMemcpyHostToDevice, stream_);
+        cudaMemcpyAsync(durow.as<void>(), urow.data(), urow.size() * sizeof(int), cudaMemcpyHostToDevice, stream_);
+        cudaMemcpyAsync(ducoef.as<void>(), ucoef.data(), ucoef.size() * sizeof(double2), cudaMemcpyHostToDevice,
+                        stream_);
+        q1 = device ? reinterpret_cast<double2 *>(s1) : ds1.as<double2>();
+        q2 = device ? reinterpret_cast<double2 *>(s2) : ds2.as<double2>();
+        cudaMemsetAsync(q1, 0, eb, stream_);
+        cudaMemsetAsync(q2, 0, eb, stream_);
+    }
+    g_launch_count.fetch_add(d ? 2 : 1, std::memory_order_relaxed);
+    k_site<<<(nsite + 127) / 128, 128, 0, stream_>>>(nsite, doff.as<int>(), didx.as<int>(), dcoef.as<double2>(), p1,
+                                                      p2, Zout ? dz.as<double2>() : nullptr,
+                                                      d ? dd.as<double2>() : nullptr, d ? dw.as<double2>() : nullptr);
+    if (d) {
+        const int nu = (int)uedge.size();
+        k_scatter<<<(nu + 127) / 128, 128, 0, stream_>>>(nu, duoff.as<int>(), duedge.as<int>(), durow.as<int>(),
+                                                          ducoef.as<double2>(), dw.as<double2>(), q1, q2);
+        if (!device) {
+            cudaMemcpyAsync(s1, q1, eb, cudaMemcpyDeviceToHost, stream_);
+            cudaMemcpyAsync(s2, q2, eb, cudaMemcpyDeviceToHost, stream_);
+        }
+    }
+    if (Zout)
+        cudaMemcpyAsync(Zout, dz.as<void>(), 4 * (size_t)nsite * sizeof(double2), cudaMemcpyDeviceToHost, stream_);
+    return sync(who);
 }
-
 
 }  // namespace mt3d

@@ -79,6 +79,10 @@ class Solver {
     int pmult_t(int npol, const double *e0, const double *eadj, const double *m0, double *dm);
     int impedance(double omega, int nsite, const double *xyz, const double *origin, const double *e1, const double *e2,
                   double *Z, bool device);
+    int lmult_t(double omega, int nsite, const double *xyz, const double *origin, const double *e1, const double *e2,
+                const double *d, double *s1, double *s2, bool device);
+    int data_functional(double omega, int nsite, const double *xyz, const double *origin, const double *e1,
+                        const double *e2, const double *d, double *Z, double *s1, double *s2, bool device);
 
     int fail(int code, const std::string &msg);
     std::string last_error;

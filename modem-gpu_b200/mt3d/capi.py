@@ -27,7 +27,7 @@ EXPORTS = ["mt3d_version", "mt3d_device_count", "mt3d_create", "mt3d_destroy", "
            "mt3d_update_freq", "mt3d_set_formulation", "mt3d_sizes", "mt3d_interior_index", "mt3d_mult_aii",
            "mt3d_mult_aii_device_noalloc", "mt3d_bicg", "mt3d_fwdsolve",
            "mt3d_fwdsolve_batch", "mt3d_fwdsolve_batch_device", "mt3d_set_stream", "mt3d_profile",
-           "mt3d_kernel_time", "mt3d_get_diag", "mt3d_get_batch_diag", "mt3d_pmult_t", "mt3d_impedance", "mt3d_impedance_device", "mt3d_launch_counter", "mt3d_last_error"]
+           "mt3d_kernel_time", "mt3d_get_diag", "mt3d_get_batch_diag", "mt3d_pmult_t", "mt3d_impedance", "mt3d_impedance_device", "mt3d_lmult_t", "mt3d_lmult_t_device", "mt3d_launch_counter", "mt3d_last_error"]
 
 _lib = None
 
@@ -64,6 +64,8 @@ def load(path: str = LIB_PATH):
     L.mt3d_mult_aii_device_noalloc.argtypes = [P, I, C.c_void_p, C.c_void_p]
     L.mt3d_impedance.argtypes = [P, C.c_double, I, D, D, D, D, D]
     L.mt3d_impedance_device.argtypes = [P, C.c_double, I, D, D, C.c_void_p, C.c_void_p, D]
+    L.mt3d_lmult_t.argtypes = [P, C.c_double, I, D, D, D, D, D, D, D]
+    L.mt3d_lmult_t_device.argtypes = [P, C.c_double, I, D, D, C.c_void_p, C.c_void_p, D, C.c_void_p, C.c_void_p]
     L.mt3d_bicg.argtypes = [P, D, D, I, C.c_double, IP, D, IP]
     L.mt3d_fwdsolve.argtypes = [P, I, D, D, D]
     L.mt3d_fwdsolve_batch.argtypes = [P, I, D, IP, D, D, D, IP]
@@ -178,6 +180,28 @@ class Solver:
             rc = self.L.mt3d_impedance(self.h, float(omega), len(xyz), _d(xyz), _d(org), _d(a), _d(b), _d(Z))
         self._check(rc)
         return Z.reshape(-1, 2, 2)
+
+    def lmult_t(self, omega, sites, e1, e2, d, origin=(0.0, 0.0, 0.0)):
+        """Adjoint sources (s1, s2) of the impedance data weights d [nsite, 2, 2]
+        for background fields e1, e2 (host arrays)."""
+        xyz = np.ascontiguousarray(sites, np.float64).reshape(-1, 3)
+        org = np.ascontiguousarray(origin, np.float64)
+        dd = np.ascontiguousarray(d, np.complex128).reshape(-1)
+        a = np.ascontiguousarray(e1, np.complex128)
+        b = np.ascontiguousarray(e2, np.complex128)
+        s1 = np.zeros(self.nE, np.complex128)
+        s2 = np.zeros(self.nE, np.complex128)
+        self._check(self.L.mt3d_lmult_t(self.h, float(omega), len(xyz), _d(xyz), _d(org), _d(a), _d(b), _d(dd),
+                                        _d(s1), _d(s2)))
+        return s1, s2
+
+    def lmult_t_device(self, omega, sites, e1_ptr, e2_ptr, d, s1_ptr, s2_ptr, origin=(0.0, 0.0, 0.0)):
+        """mt3d_lmult_t on device fields and sources (device addresses)."""
+        xyz = np.ascontiguousarray(sites, np.float64).reshape(-1, 3)
+        org = np.ascontiguousarray(origin, np.float64)
+        dd = np.ascontiguousarray(d, np.complex128).reshape(-1)
+        self._check(self.L.mt3d_lmult_t_device(self.h, float(omega), len(xyz), _d(xyz), _d(org), C.c_void_p(e1_ptr),
+                                               C.c_void_p(e2_ptr), _d(dd), C.c_void_p(s1_ptr), C.c_void_p(s2_ptr)))
 
     def bicg(self, b, x0, maxit, tol):
         b = np.ascontiguousarray(b, np.complex128)

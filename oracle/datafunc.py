@@ -171,3 +171,29 @@ def impedance(c, omega, sites, e1, e2):
         Bi = np.array([[BB[1, 1], -BB[0, 1]], [-BB[1, 0], BB[0, 0]]]) / det
         Z[s] = EE @ Bi
     return Z
+
+
+def lmult_t(c, omega, sites, e1, e2, d):
+    """Adjoint sources (s1, s2) of Lrows + LmultT for Full_Impedance
+    (f90/3D_MT/DataFunc.f90:465-869, f90/SENS/DataSens.f90:130-225):
+    s_k = sum_ij conj(d_ij) B^-1(k, j) (Le_i - Z_i1 Lbx - Z_i2 Lby)."""
+    nE = e1.size
+    out = [np.zeros(nE, complex), np.zeros(nE, complex)]
+    d = np.asarray(d, complex).reshape(-1, 2, 2)
+    for s, x in enumerate(np.asarray(sites, float)):
+        L = [e_interp(c, x, 1), e_interp(c, x, 2), b_from_e(c, omega, x, 1), b_from_e(c, omega, x, 2)]
+        EE = np.array([[apply(c, L[i], e) for e in (e1, e2)] for i in (0, 1)])
+        BB = np.array([[apply(c, L[2 + i], e) for e in (e1, e2)] for i in (0, 1)])
+        det = BB[0, 0] * BB[1, 1] - BB[0, 1] * BB[1, 0]
+        Bi = np.array([[BB[1, 1], -BB[0, 1]], [-BB[1, 0], BB[0, 0]]]) / det
+        Z = EE @ Bi
+        for k in range(2):
+            for i in range(2):
+                for j in range(2):
+                    w = np.conj(d[s, i, j]) * Bi[k, j]
+                    for a, ii, jj, kk, v in L[i]:
+                        out[k][flat(c, a, ii, jj, kk)] += w * v
+                    for m in range(2):
+                        for a, ii, jj, kk, v in L[2 + m]:
+                            out[k][flat(c, a, ii, jj, kk)] -= w * Z[i, m] * v
+    return out[0], out[1]

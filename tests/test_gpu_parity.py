@@ -477,3 +477,26 @@ def test_impedance_of_halfspace_solution(cuda):
         assert min(abs(ph - 45.0), abs(ph - 135.0)) < 3.0
     zo = df.impedance(c, omega, sites, e[0], e[1])
     assert relerr(Z, zo) < 1e-12
+
+
+def test_lmult_t_matches_oracle(prob):
+    import torch
+    from oracle import datafunc as df
+    g, m, omega, o, s = prob
+    origin = (-1000.0, -800.0, 0.0)
+    c = df.coords(g.dx, g.dy, g.dz, g.nzAir, origin)
+    rng = np.random.default_rng(12)
+    e1 = rng.standard_normal(g.n_edges) + 1j * rng.standard_normal(g.n_edges)
+    e2 = rng.standard_normal(g.n_edges) + 1j * rng.standard_normal(g.n_edges)
+    sites = np.column_stack([rng.uniform(c["xC"][2], c["xC"][g.nx - 1], 6),
+                             rng.uniform(c["yC"][2], c["yC"][g.ny - 1], 6), np.zeros(6)])
+    d = rng.standard_normal((6, 2, 2)) + 1j * rng.standard_normal((6, 2, 2))
+    o1, o2 = df.lmult_t(c, omega, sites, e1, e2, d)
+    g1, g2 = s.lmult_t(omega, sites, e1, e2, d, origin)
+    assert relerr(g1, o1) < 1e-12 and relerr(g2, o2) < 1e-12
+    t1, t2 = torch.from_numpy(e1).cuda(), torch.from_numpy(e2).cuda()
+    u1 = torch.full((g.n_edges,), complex(np.nan, np.nan), dtype=torch.complex128, device="cuda")
+    u2 = u1.clone()
+    s.lmult_t_device(omega, sites, t1.data_ptr(), t2.data_ptr(), d, u1.data_ptr(), u2.data_ptr(), origin)
+    torch.cuda.synchronize()
+    assert relerr(u1.cpu().numpy(), o1) < 1e-12 and relerr(u2.cpu().numpy(), o2) < 1e-12

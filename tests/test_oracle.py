@@ -245,3 +245,25 @@ def test_datafunc_b_is_curl_e_over_minus_i_omega():
     by = df.apply(c, df.b_from_e(c, omega, x, 2), e)
     assert abs(bx - (-1j / omega) * (-a)) < 1e-12 * abs(a / omega)
     assert abs(by - (-1j / omega) * b) < 1e-12 * abs(b / omega)
+
+
+def test_datafunc_lmult_t_is_the_derivative_of_z():
+    """sum_k s_k . de_k = sum_ij conj(d_ij) dZ_ij for the adjoint sources of
+    LmultT, dZ by central differences of the impedance functional."""
+    from oracle import datafunc as df
+    g = small_grid()
+    c = df.coords(g.dx, g.dy, g.dz, g.nzAir)
+    rng = np.random.default_rng(6)
+    nE = g.n_edges
+    e1, e2, de1, de2 = (rng.standard_normal(nE) + 1j * rng.standard_normal(nE) for _ in range(4))
+    sites = np.array([[c["xC"][4] + 10.0, c["yC"][5] + 20.0, 0.0], [c["xC"][6] - 30.0, c["yC"][7], 0.0]])
+    omega = 2 * np.pi * 0.3
+    d = rng.standard_normal((2, 2, 2)) + 1j * rng.standard_normal((2, 2, 2))
+    s1, s2 = df.lmult_t(c, omega, sites, e1, e2, d)
+    h = 1e-6
+    zp = df.impedance(c, omega, sites, e1 + h * de1, e2 + h * de2)
+    zm = df.impedance(c, omega, sites, e1 - h * de1, e2 - h * de2)
+    dz = (zp - zm) / (2 * h)
+    lhs = s1 @ de1 + s2 @ de2
+    rhs = np.sum(np.conj(d) * dz)
+    assert abs(lhs - rhs) < 1e-7 * abs(rhs)
