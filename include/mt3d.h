@@ -106,6 +106,22 @@ MT3D_API int mt3d_set_formulation(mt3d_handle h, int formulation);
  * 211-232): ModelParamToEdge (LOGE, ModelMap.inc:88-188) and DivCorrSetUp. */
 MT3D_API int mt3d_update_cond(mt3d_handle h, const double *m_earth, double airCond);
 
+/* Read back the conductivity-dependent operator data that mt3d_update_cond
+ * built on the device -- the public module variables of the reference's
+ * operator, for checking and for callers that need them:
+ *   sigma_e [nE]   Sigma_E as the curl-curl operator uses it, the air edges
+ *                  zero (f90/3D_MT/FWD/modelOperator3D.f90:1598-1605);
+ *   divcorr [7*nN] DivCorrSetUp's db1%x, db2%x, db1%y, db2%y, db1%z, db2%z
+ *                  and c (:1538-1650) per node, in that order; entry k of the
+ *                  block of db1%x is the coefficient of node k (0 off the
+ *                  interior nodes);
+ *   node_w [nN]    the grad-div node weight of the SP2 operator with the air
+ *                  nodes' sign (GradDivSetup2, f90/3D_MT/FWD_SP2/
+ *                  modelOperator3D.f90:916-1008): -w at an earth node, +w in
+ *                  the air.
+ * Any of the three may be NULL. */
+MT3D_API int mt3d_get_cond(mt3d_handle h, double *sigma_e, double *divcorr, double *node_w);
+
 /* Set the angular frequency (UpdateFreq, f90/3D_MT/FWD/modelOperator3D.f90:
  * 196-204). */
 MT3D_API int mt3d_update_freq(mt3d_handle h, double omega);

@@ -14,7 +14,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libmt3d.so")
-SOURCES = ["kernels.cu", "colkernels.cu", "stagekernels.cu", "tmakernels.cu", "datafunc.cu", "solver.cu", "noalloc.cu", "capi.cu"]
+SOURCES = ["kernels.cu", "colkernels.cu", "stagekernels.cu", "tmakernels.cu", "setupkernels.cu", "datafunc.cu", "solver.cu",
+           "noalloc.cu", "capi.cu"]
+# the operator set-up reproduces the host's operation order bit for bit: no contraction to FMA
+FILE_FLAGS = {"setupkernels.cu": ["-fmad=false"]}
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -41,7 +44,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         flags += ["-Xptxas", "-v"]
     for src in SOURCES:
         obj = os.path.join(objdir, src + ".o")
-        cmd = [nvcc(), "-c", os.path.join(CSRC, src), "-o", obj] + flags
+        cmd = [nvcc(), "-c", os.path.join(CSRC, src), "-o", obj] + flags + FILE_FLAGS.get(src, [])
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"nvcc failed on {src}:\n{r.stdout}\n{r.stderr}")

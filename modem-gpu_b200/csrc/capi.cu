@@ -138,6 +138,11 @@ int mt3d_update_cond(mt3d_handle h, const double *m_earth, double airCond)
     return wrap(h, [&] { return h->s.update_cond(m_earth, airCond); });
 }
 
+int mt3d_get_cond(mt3d_handle h, double *sigma_e, double *divcorr, double *node_w)
+{
+    return wrap(h, [&] { return h->s.get_cond(sigma_e, divcorr, node_w); });
+}
+
 int mt3d_update_freq(mt3d_handle h, double omega)
 {
     return wrap(h, [&] { return h->s.update_freq(omega); });

@@ -129,6 +129,11 @@ void launch_cast_padded(const Geo<double> &g, const OuterState *ost, size_t stri
 void launch_update_padded(const Geo<double> &g, const OuterState *ost, size_t stride64, PadLayout pl,
                           const float2 *d32, double2 *X, int nrhs, cudaStream_t s);
 void launch_to_padded(const Geo<double> &g, const double *src, PadLayout pl, float *dst, cudaStream_t s);
+// conductivity-dependent operator set-up from the model parameter (setupkernels.cu);
+// VC, CT: [nx*ny*nz] scratch; coef: [7][nN]
+void launch_setup_cond(const Geo<double> &g, const double *m_earth, double airCond, double *VC, double *CT,
+                       double *sig, double *sigs, double *gdw, unsigned char *gde, double *gdn, double *coef,
+                       float *sig32, float *sigs32, float *gdw32, float *gdn32, cudaStream_t s);
 void launch_nodes_to_padded(const Geo<double> &g, const double *src, PadLayout pl, float *dst, cudaStream_t s);
 int stage_chunks(int nz, int tiles, int resident);
 template <typename T> void launch_cocg_iter(const ColArgs<T> &a, int nrhs, cudaStream_t s, cudaEvent_t *ev = nullptr);

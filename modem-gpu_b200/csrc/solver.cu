@@ -218,168 +218,31 @@ int Solver::create(int dev, int nx_, int ny_, int nz_, int nzAir_, const double 
 }
 
 // ---------------------------------------------------------------------------
-// UpdateCond: ModelParamToEdge (LOGE, f90/3D_MT/modelParam/ModelMap.inc:88-188)
-// and DivCorrSetUp (f90/3D_MT/FWD/modelOperator3D.f90:1538-1672)
+// UpdateCond: ModelParamToEdge (LOGE, f90/3D_MT/modelParam/ModelMap.inc:88-188),
+// the SP2 edge and node data (f90/3D_MT/FWD_SP2/modelOperator3D.f90:176-230,
+// 916-1008, 1086-1130) and DivCorrSetUp (f90/3D_MT/FWD/modelOperator3D.f90:
+// 1538-1672), built on the device from the model parameter
 // ---------------------------------------------------------------------------
 int Solver::update_cond(const double *m_earth, double airCond)
 {
     if (!m_earth) return fail(5, "mt3d_update_cond: null model");
-    const int nzE = nz - nzAir;
-    const int64_t nC = (int64_t)nx * ny * nz;
-    for (int64_t c = 0; c < (int64_t)nx * ny * nzE; c++)
+    const int64_t nEarth = (int64_t)nx * ny * (nz - nzAir), nC = (int64_t)nx * ny * nz;
+    for (int64_t c = 0; c < nEarth; c++)
         if (!std::isfinite(m_earth[c])) return fail(3, "mt3d_update_cond: NaN/Inf in the model parameter");
     if (!std::isfinite(airCond)) return fail(3, "mt3d_update_cond: NaN/Inf air conductivity");
-    auto cl = [&](int i, int j, int k) { return (int64_t)i + (int64_t)nx * (j + (int64_t)ny * k); };
-    std::vector<double> VC(nC), CT(nC);
-    for (int k = 0; k < nz; k++)
-        for (int j = 0; j < ny; j++)
-            for (int i = 0; i < nx; i++) {
-                const int64_t c = cl(i, j, k);
-                VC[c] = dx_[i] * dy_[j] * dz_[k];
-                const double s = (k < nzAir) ? std::exp(airCond) : std::exp(m_earth[c - (int64_t)nx * ny * nzAir]);
-                CT[c] = VC[c] * s;
-            }
-    const int64_t nX = (int64_t)nx * (ny + 1) * (nz + 1), nY = (int64_t)(nx + 1) * ny * (nz + 1);
-    std::vector<double> sig(nE);
-    // Cell2Edge of V_C*sigma over Cell2Edge of V_C, summing the adjacent cells in
-    // the reference's order (a-1,b-1), (a,b-1), (a-1,b), (a,b)
-    auto avg = [&](int comp, int i, int j, int k) {
-        double num = 0.0, den = 0.0;
-        int n = 0;
-        for (int q = 0; q < 4; q++) {
-            const int da = (q & 1) ? 0 : -1, db = (q & 2) ? 0 : -1;
-            int ci = i, cj = j, ck = k;
-            if (comp == 0) { cj = j + da; ck = k + db; }
-            if (comp == 1) { ci = i + da; ck = k + db; }
-            if (comp == 2) { cj = j + da; ci = i + db; }
-            if (ci < 0 || ci >= nx || cj < 0 || cj >= ny || ck < 0 || ck >= nz) continue;
-            num += CT[cl(ci, cj, ck)];
-            den += VC[cl(ci, cj, ck)];
-            n++;
-        }
-        return (num / n) / (den / n);
-    };
-    for (int k = 0; k <= nz; k++)
-        for (int j = 0; j <= ny; j++)
-            for (int i = 0; i < nx; i++) sig[i + nx * (j + (int64_t)(ny + 1) * k)] = avg(0, i, j, k);
-    for (int k = 0; k <= nz; k++)
-        for (int j = 0; j < ny; j++)
-            for (int i = 0; i <= nx; i++) sig[nX + i + (nx + 1) * (j + (int64_t)ny * k)] = avg(1, i, j, k);
-    for (int k = 0; k < nz; k++)
-        for (int j = 0; j <= ny; j++)
-            for (int i = 0; i <= nx; i++) sig[nX + nY + i + (nx + 1) * (j + (int64_t)(ny + 1) * k)] = avg(2, i, j, k);
-    // SP2 (grad-div) data: edge conductivity with the air at exp(airCond) and
-    // the boundary edges zero (UpdateCond, f90/3D_MT/FWD_SP2/modelOperator3D.f90:
-    // 176-230), node conductivity (ModelParamToNode) and the node weights of
-    // GradDivSetup2 with airNIndex (:916-1008, 1086-1130)
-    std::vector<double> sig_sp2(sig);
-    auto is_int = [&](int64_t e) -> bool {
-        if (e < nX) { int64_t t = e / nx; int j = (int)(t % (ny + 1)), k = (int)(t / (ny + 1)); return j >= 1 && j <= ny - 1 && k >= 1 && k <= nz - 1; }
-        if (e < nX + nY) { int64_t f = e - nX; int i = (int)(f % (nx + 1)), k = (int)(f / ((int64_t)(nx + 1) * ny)); return i >= 1 && i <= nx - 1 && k >= 1 && k <= nz - 1; }
-        int64_t f = e - nX - nY; int i = (int)(f % (nx + 1)), j = (int)((f / (nx + 1)) % (ny + 1)); return i >= 1 && i <= nx - 1 && j >= 1 && j <= ny - 1;
-    };
-    for (int64_t e = 0; e < nE; e++) if (!is_int(e)) sig_sp2[e] = 0.0;
-    std::vector<double> gdw(nN, 0.0);
-    std::vector<unsigned char> gde(nN, 0);
-    {
-        auto ndx = [&](int i, int j, int k) { return (int64_t)i + (nx + 1) * (j + (int64_t)(ny + 1) * k); };
-        auto exi = [&](int i, int j, int k) { return (int64_t)i + nx * (j + (int64_t)(ny + 1) * k); };
-        auto eyi = [&](int i, int j, int k) { return nX + i + (nx + 1) * (j + (int64_t)ny * k); };
-        auto ezi = [&](int i, int j, int k) { return nX + nY + i + (nx + 1) * (j + (int64_t)(ny + 1) * k); };
-        const double thr = 1.1 * kSigmaAir;
-        for (int k = 1; k < nz; k++)
-            for (int j = 1; j < ny; j++)
-                for (int i = 1; i < nx; i++) {
-                    const int64_t inc[6] = {exi(i - 1, j, k), exi(i, j, k), eyi(i, j - 1, k), eyi(i, j, k),
-                                            ezi(i, j, k - 1), ezi(i, j, k)};
-                    bool earth = false;
-                    for (int q = 0; q < 6; q++) earth = earth || sig_sp2[inc[q]] >= thr;
-                    // node conductivity: volume-weighted mean of the 8 cells around the node
-                    double num = 0.0, den = 0.0;
-                    for (int c = 0; c < 8; c++) {
-                        const int ci = i - 1 + (c & 1), cj = j - 1 + ((c >> 1) & 1), ck = k - 1 + ((c >> 2) & 1);
-                        num += CT[cl(ci, cj, ck)];
-                        den += VC[cl(ci, cj, ck)];
-                    }
-                    const double vn = delX_[i] * delY_[j] * delZ_[k];
-                    const int64_t n = ndx(i, j, k);
-                    gde[n] = earth ? 1 : 0;
-                    gdw[n] = earth ? 1.0 / ((num / den) * vn) : 1.0 / vn;
-                }
-    }
-    auto ex = [&](int i, int j, int k) { return (int64_t)i + nx * (j + (int64_t)(ny + 1) * k); };
-    auto ey = [&](int i, int j, int k) { return nX + i + (nx + 1) * (j + (int64_t)ny * k); };
-    auto ez = [&](int i, int j, int k) { return nX + nY + i + (nx + 1) * (j + (int64_t)(ny + 1) * k); };
-    auto nd = [&](int i, int j, int k) { return (int64_t)i + (nx + 1) * (j + (int64_t)(ny + 1) * k); };
-    // DivCorrSetUp: air cells (1-based iz <= nzAir, ix <= nx, iy <= ny) at SIGMA_AIR
-    for (int k = 0; k < nzAir; k++)
-        for (int j = 0; j < ny; j++)
-            for (int i = 0; i < nx; i++) sig[ex(i, j, k)] = sig[ey(i, j, k)] = sig[ez(i, j, k)] = kSigmaAir;
-    std::vector<double> coef(7 * (size_t)nN, 0.0);
-    double *db1x = &coef[0], *db2x = &coef[nN], *db1y = &coef[2 * nN], *db2y = &coef[3 * nN], *db1z = &coef[4 * nN],
-           *db2z = &coef[5 * nN], *cc = &coef[6 * nN];
-    for (int k = 1; k < nz; k++)
-        for (int j = 1; j < ny; j++)
-            for (int i = 1; i < nx; i++) {
-                const int64_t n = nd(i, j, k);
-                db1x[n] = sig[ex(i - 1, j, k)] / (dx_[i - 1] * delX_[i]);
-                db2x[n] = sig[ex(i, j, k)] / (dx_[i] * delX_[i]);
-                db1y[n] = sig[ey(i, j - 1, k)] / (dy_[j - 1] * delY_[j]);
-                db2y[n] = sig[ey(i, j, k)] / (dy_[j] * delY_[j]);
-                db1z[n] = sig[ez(i, j, k - 1)] / (dz_[k - 1] * delZ_[k]);
-                db2z[n] = sig[ez(i, j, k)] / (dz_[k] * delZ_[k]);
-                cc[n] = -(db1x[n] + db2x[n] + db1y[n] + db2y[n] + db1z[n] + db2z[n]);
-            }
-    for (int k = 0; k < nzAir; k++)
-        for (int j = 0; j < ny; j++)
-            for (int i = 0; i < nx; i++) sig[ex(i, j, k)] = sig[ey(i, j, k)] = sig[ez(i, j, k)] = 0.0;
-    for (int k = 1; k < nz; k++)
-        for (int j = 1; j < ny; j++)
-            for (int i = 1; i < nx; i++) {
-                const int64_t n = nd(i, j, k);
-                const double v = delX_[i] * delY_[j] * delZ_[k];
-                db1x[n] *= v; db1y[n] *= v; db1z[n] *= v;
-                db2x[n] *= v; db2y[n] *= v; db2z[n] *= v;
-                cc[n] = cc[n] * v;
-            }
-    // coefficients that multiply boundary nodes are zero (phi = 0 on the boundary)
-    for (int k = 0; k <= nz; k++)
-        for (int j = 0; j <= ny; j++)
-            for (int i = 0; i <= nx; i++) {
-                const int64_t n = nd(i, j, k);
-                if (i == 1) db1x[n] = 0.0;
-                if (i == nx - 1) db2x[n] = 0.0;
-                if (j == 1) db1y[n] = 0.0;
-                if (j == ny - 1) db2y[n] = 0.0;
-                if (k == 1) db1z[n] = 0.0;
-                if (k == nz - 1) db2z[n] = 0.0;
-            }
-    std::vector<float> sigf(sig.begin(), sig.end());
-    std::vector<float> sigsf(sig_sp2.begin(), sig_sp2.end()), gdwf(gdw.begin(), gdw.end());
-    // node weight with the earth flag as its sign, for the staged stencil kernels
-    std::vector<double> gdn(nN);
-    for (int64_t n = 0; n < nN; n++) gdn[n] = gde[n] ? -gdw[n] : gdw[n];
-    std::vector<float> gdnf(gdn.begin(), gdn.end());
     int rc;
-    if (sig64_.alloc(nE * sizeof(double)) || sig32_.alloc(nE * sizeof(float)) || coef_.alloc(coef.size() * sizeof(double)) ||
+    if (sig64_.alloc(nE * sizeof(double)) || sig32_.alloc(nE * sizeof(float)) || coef_.alloc(7 * nN * sizeof(double)) ||
         sigs64_.alloc(nE * sizeof(double)) || sigs32_.alloc(nE * sizeof(float)) || gdw64_.alloc(nN * sizeof(double)) ||
         gdw32_.alloc(nN * sizeof(float)) || gde_.alloc(nN) || gdn64_.alloc(nN * sizeof(double)) ||
-        gdn32_.alloc(nN * sizeof(float)))
+        gdn32_.alloc(nN * sizeof(float)) || setup_.alloc((nEarth + 2 * nC) * sizeof(double)))
         return fail(8, "mt3d_update_cond: out of device memory");
-    cudaMemcpyAsync(sigs64_.as<void>(), sig_sp2.data(), nE * sizeof(double), cudaMemcpyHostToDevice, stream_);
-    cudaMemcpyAsync(sigs32_.as<void>(), sigsf.data(), nE * sizeof(float), cudaMemcpyHostToDevice, stream_);
-    cudaMemcpyAsync(gdw64_.as<void>(), gdw.data(), nN * sizeof(double), cudaMemcpyHostToDevice, stream_);
-    cudaMemcpyAsync(gdw32_.as<void>(), gdwf.data(), nN * sizeof(float), cudaMemcpyHostToDevice, stream_);
-    cudaMemcpyAsync(gde_.as<void>(), gde.data(), nN, cudaMemcpyHostToDevice, stream_);
-    cudaMemcpyAsync(gdn64_.as<void>(), gdn.data(), nN * sizeof(double), cudaMemcpyHostToDevice, stream_);
-    cudaMemcpyAsync(gdn32_.as<void>(), gdnf.data(), nN * sizeof(float), cudaMemcpyHostToDevice, stream_);
-    if ((rc = check(cudaMemcpyAsync(sig64_.as<void>(), sig.data(), nE * sizeof(double), cudaMemcpyHostToDevice, stream_), "copy sigma")))
+    double *m_d = setup_.as<double>(), *VC = m_d + nEarth, *CT = VC + nC;
+    if ((rc = check(cudaMemcpyAsync(m_d, m_earth, nEarth * sizeof(double), cudaMemcpyHostToDevice, stream_),
+                    "copy model parameter")))
         return rc;
-    if ((rc = check(cudaMemcpyAsync(sig32_.as<void>(), sigf.data(), nE * sizeof(float), cudaMemcpyHostToDevice, stream_), "copy sigma")))
-        return rc;
-    if ((rc = check(cudaMemcpyAsync(coef_.as<void>(), coef.data(), coef.size() * sizeof(double), cudaMemcpyHostToDevice, stream_),
-                    "copy div-corr coefficients")))
-        return rc;
+    launch_setup_cond(g64_, m_d, airCond, VC, CT, sig64_.as<double>(), sigs64_.as<double>(), gdw64_.as<double>(),
+                      gde_.as<unsigned char>(), gdn64_.as<double>(), coef_.as<double>(), sig32_.as<float>(),
+                      sigs32_.as<float>(), gdw32_.as<float>(), gdn32_.as<float>(), stream_);
     // sigma of both formulations and the signed node weights on the padded
     // layout (FP32), for the TMA-staged kernels
     const size_t pe = (size_t)pl_.len(), pn = (size_t)pl_.Px * pl_.Py * pl_.Pz;
@@ -395,6 +258,22 @@ int Solver::update_cond(const double *m_earth, double airCond)
     if ((rc = sync("mt3d_update_cond"))) return rc;
     cond_set = true;
     return 0;
+}
+
+int Solver::get_cond(double *sigma_e, double *divcorr, double *node_w)
+{
+    if (!cond_set) return fail(5, "mt3d_get_cond: conductivity not set (call mt3d_update_cond)");
+    int rc;
+    if (sigma_e && (rc = check(cudaMemcpyAsync(sigma_e, sig64_.as<void>(), nE * sizeof(double), cudaMemcpyDeviceToHost,
+                                               stream_), "copy sigma")))
+        return rc;
+    if (divcorr && (rc = check(cudaMemcpyAsync(divcorr, coef_.as<void>(), 7 * nN * sizeof(double),
+                                               cudaMemcpyDeviceToHost, stream_), "copy div-corr coefficients")))
+        return rc;
+    if (node_w && (rc = check(cudaMemcpyAsync(node_w, gdn64_.as<void>(), nN * sizeof(double), cudaMemcpyDeviceToHost,
+                                              stream_), "copy node weights")))
+        return rc;
+    return sync("mt3d_get_cond");
 }
 
 // tensor maps of the padded FP32 vectors, rebuilt after the workspace or the

@@ -24,7 +24,7 @@ FORM_CCDC, FORM_CCGD = 0, 1
 
 #: every symbol include/mt3d.h declares
 EXPORTS = ["mt3d_version", "mt3d_device_count", "mt3d_create", "mt3d_destroy", "mt3d_set_control", "mt3d_update_cond",
-           "mt3d_update_freq", "mt3d_set_formulation", "mt3d_sizes", "mt3d_interior_index", "mt3d_mult_aii",
+           "mt3d_get_cond", "mt3d_update_freq", "mt3d_set_formulation", "mt3d_sizes", "mt3d_interior_index", "mt3d_mult_aii",
            "mt3d_mult_aii_device_noalloc", "mt3d_bicg", "mt3d_fwdsolve",
            "mt3d_fwdsolve_batch", "mt3d_fwdsolve_batch_device", "mt3d_set_stream", "mt3d_profile",
            "mt3d_kernel_time", "mt3d_get_diag", "mt3d_get_batch_diag", "mt3d_pmult_t", "mt3d_impedance", "mt3d_impedance_device", "mt3d_lmult_t", "mt3d_lmult_t_device", "mt3d_launch_counter", "mt3d_last_error"]
@@ -56,6 +56,7 @@ def load(path: str = LIB_PATH):
     L.mt3d_destroy.argtypes = [P]
     L.mt3d_set_control.argtypes = [P, I, I, I, C.c_double, C.c_double, C.c_double, I, I]
     L.mt3d_update_cond.argtypes = [P, D, C.c_double]
+    L.mt3d_get_cond.argtypes = [P, D, D, D]
     L.mt3d_update_freq.argtypes = [P, C.c_double]
     L.mt3d_set_formulation.argtypes = [P, I]
     L.mt3d_sizes.argtypes = [P, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
@@ -143,6 +144,12 @@ class Solver:
     def update_cond(self, m_earth, air_cond):
         m = np.ascontiguousarray(m_earth, np.float64)
         self._check(self.L.mt3d_update_cond(self.h, _d(m), float(air_cond)))
+
+    def get_cond(self):
+        """(sigma_e [nE], divcorr [7, nN], node_w [nN]) as mt3d_get_cond returns them."""
+        sig, coef, w = np.zeros(self.nE), np.zeros(7 * self.nN), np.zeros(self.nN)
+        self._check(self.L.mt3d_get_cond(self.h, _d(sig), _d(coef), _d(w)))
+        return sig, coef.reshape(7, self.nN), w
 
     def update_freq(self, omega):
         self._check(self.L.mt3d_update_freq(self.h, float(omega)))

@@ -61,6 +61,32 @@ def test_mult_aii_matches_oracle(prob):
         assert relerr(y, yref) < 1e-13
 
 
+def test_operator_setup_matches_oracle(prob):
+    """Sigma_E and the DivCorrSetUp coefficients that update_cond builds on the
+    device against the oracle's UpdateCond (relative 1e-14: the cell
+    exponentials may differ in the last bit)."""
+    g, m, omega, o, s = prob
+    sig, coef, _ = s.get_cond()
+    assert np.max(np.abs(sig - o.sigE) / np.maximum(np.abs(o.sigE), 1e-300)) < 1e-14
+    db1, db2, c = o.divcorr_coef()
+    nx, ny, nz = g.nx, g.ny, g.nz
+    nX, nY = nx * (ny + 1) * (nz + 1), (nx + 1) * ny * (nz + 1)
+    i, j, k = np.meshgrid(np.arange(nx + 1), np.arange(ny + 1), np.arange(nz + 1), indexing="ij")
+    i, j, k = (a.ravel(order="F") for a in (i, j, k))
+    inner = (i >= 1) & (i < nx) & (j >= 1) & (j < ny) & (k >= 1) & (k < nz)
+    ii, jj, kk = i[inner], j[inner], k[inner]
+    ex = ii + nx * (jj + (ny + 1) * kk)
+    ey = nX + ii + (nx + 1) * (jj + ny * kk)
+    ez = nX + nY + ii + (nx + 1) * (jj + (ny + 1) * kk)
+    want = np.zeros((7, s.nN))
+    for q, (arr, e) in enumerate(((db1, ex), (db2, ex), (db1, ey), (db2, ey), (db1, ez), (db2, ez))):
+        want[q, inner] = arr[e]
+    want[6] = c
+    scale = np.max(np.abs(want), axis=1, keepdims=True)
+    assert np.max(np.abs(coef - want) / scale) < 1e-14
+    assert np.all(coef[:, ~inner] == 0)
+
+
 def test_bicg_history_matches_oracle(prob):
     g, m, omega, o, s = prob
     mask = interior_edge_mask(g)
@@ -369,6 +395,17 @@ def test_ccgd_operator_matches_sp2(gprob):
     rng = np.random.default_rng(0)
     xi = rng.standard_normal(s.nEi) + 1j * rng.standard_normal(s.nEi)
     assert relerr(s.mult_aii(xi), ref.A @ xi) < 1e-12
+
+
+def test_ccgd_node_weights_match_sp2(gprob):
+    """Signed grad-div node weights built on the device against the SP2
+    restatement: -1/(sigma_N V_N) at earth nodes, 1/V_N at air nodes."""
+    g, m, omega, ref, s = gprob
+    _, _, w = s.get_cond()
+    t = ref.topo
+    want = np.where(ref.nearth, -1.0 / (ref.sig_n * t.Vnode), np.where(ref.nair, 1.0 / t.Vnode, 0.0))
+    assert np.array_equal(w < 0, ref.nearth)
+    assert np.max(np.abs(w - want) / np.max(np.abs(want))) < 1e-14
 
 
 @pytest.mark.parametrize("prec", [0, 1])
