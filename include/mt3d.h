@@ -122,6 +122,20 @@ MT3D_API int mt3d_update_cond(mt3d_handle h, const double *m_earth, double airCo
  * Any of the three may be NULL. */
 MT3D_API int mt3d_get_cond(mt3d_handle h, double *sigma_e, double *divcorr, double *node_w);
 
+/* Boundary conditions and first guess of the forward problem for one
+ * polarisation: ComputeBC -> BC_x0_WS (f90/3D_MT/FWD/modelOperator3D.f90:
+ * 268-293, f90/3D_MT/FWD/boundary_ws.f90:21-168), 2-D TE solutions on the
+ * slices of the model with 1-D TE solutions on their edges, computed on the
+ * device from the conductivity of mt3d_update_cond.  imode = 2 fills the
+ * x-edges (x-slices), imode = 1 the y-edges (y-slices).  e0 (full edge vector,
+ * nE complex) receives E0 with the tangential field of the bottom face zero:
+ * pass it to mt3d_fwdsolve as both bc (its boundary entries are the BC) and
+ * e (its interior entries are the reference's first guess).
+ * mt3d_compute_bc uses the handle's frequency and host memory;
+ * mt3d_compute_bc_device takes omega and a device pointer. */
+MT3D_API int mt3d_compute_bc(mt3d_handle h, int imode, double *e0);
+MT3D_API int mt3d_compute_bc_device(mt3d_handle h, int imode, double omega, void *e0);
+
 /* Set the angular frequency (UpdateFreq, f90/3D_MT/FWD/modelOperator3D.f90:
  * 196-204). */
 MT3D_API int mt3d_update_freq(mt3d_handle h, double omega);

@@ -143,6 +143,19 @@ int mt3d_get_cond(mt3d_handle h, double *sigma_e, double *divcorr, double *node_
     return wrap(h, [&] { return h->s.get_cond(sigma_e, divcorr, node_w); });
 }
 
+int mt3d_compute_bc(mt3d_handle h, int imode, double *e0)
+{
+    return wrap(h, [&] {
+        if (!(h->s.omega > 0)) return h->s.fail(5, "mt3d_compute_bc: frequency not set (call mt3d_update_freq)");
+        return h->s.compute_bc(imode, h->s.omega, e0, false);
+    });
+}
+
+int mt3d_compute_bc_device(mt3d_handle h, int imode, double omega, void *e0)
+{
+    return wrap(h, [&] { return h->s.compute_bc(imode, omega, reinterpret_cast<double *>(e0), true); });
+}
+
 int mt3d_update_freq(mt3d_handle h, double omega)
 {
     return wrap(h, [&] { return h->s.update_freq(omega); });

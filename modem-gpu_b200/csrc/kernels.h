@@ -130,10 +130,29 @@ void launch_update_padded(const Geo<double> &g, const OuterState *ost, size_t st
                           const float2 *d32, double2 *X, int nrhs, cudaStream_t s);
 void launch_to_padded(const Geo<double> &g, const double *src, PadLayout pl, float *dst, cudaStream_t s);
 // conductivity-dependent operator set-up from the model parameter (setupkernels.cu);
-// VC, CT: [nx*ny*nz] scratch; coef: [7][nN]
+// VC, CT, sigC: [nx*ny*nz] (cell volume, volume x conductivity, conductivity); coef: [7][nN]
 void launch_setup_cond(const Geo<double> &g, const double *m_earth, double airCond, double *VC, double *CT,
-                       double *sig, double *sigs, double *gdw, unsigned char *gde, double *gdn, double *coef,
-                       float *sig32, float *sigs32, float *gdw32, float *gdn32, cudaStream_t s);
+                       double *sigC, double *sig, double *sigs, double *gdw, unsigned char *gde, double *gdn,
+                       double *coef, float *sig32, float *sigs32, float *gdw32, float *gdn32, cudaStream_t s);
+
+// 2-D TE boundary conditions (bc2d.cu)
+struct BcArgs {
+    int imode;         // 2: x-slices, field on the x-edges; 1: y-slices, field on the y-edges
+    int nh, nz, nza;   // horizontal cells of a slice, vertical cells (air first), air cells
+    int nslice, slice0;
+    int nx, ny, nXe;   // 3-D grid; nXe = offset of the y-edges
+    double omue;       // omega mu0
+    const double *dh, *dz, *sigC;
+    double2 *side;     // [nslice][2][nz+1] side columns
+    double2 *cpr;      // [nslice][2][nz] elimination scratch of the side columns
+    double2 *bottom;   // [nslice][nh+1] bottom node of each interior column
+    double2 *U, *y;    // [chunk][n][nz], [chunk][n]: U rows and reduced right-hand side
+    double2 *W;        // [chunk][nz][nz] elimination window when it is not in shared memory
+    double2 *e0;       // full edge vector (zeroed by the caller)
+};
+size_t bc_smem_bytes(int nz, bool window_in_smem);
+void launch_bc1d(const BcArgs &a, cudaStream_t s);
+int launch_bc2d(const BcArgs &a, int nblocks, bool window_in_smem, cudaStream_t s);
 void launch_nodes_to_padded(const Geo<double> &g, const double *src, PadLayout pl, float *dst, cudaStream_t s);
 int stage_chunks(int nz, int tiles, int resident);
 template <typename T> void launch_cocg_iter(const ColArgs<T> &a, int nrhs, cudaStream_t s, cudaEvent_t *ev = nullptr);

@@ -30,8 +30,8 @@ constexpr int kT = 256;
 inline int blocks(long long n) { return (int)std::min<long long>((n + kT - 1) / kT, 148LL * 32); }
 }  // namespace
 
-// cell volume V_C and V_C sigma_C
-__global__ void ks_cells(Geo<double> g, const double *m_earth, double airCond, double *VC, double *CT)
+// cell volume V_C, V_C sigma_C and sigma_C
+__global__ void ks_cells(Geo<double> g, const double *m_earth, double airCond, double *VC, double *CT, double *sigC)
 {
     const long long nC = (long long)g.nx * g.ny * g.nz, nAir = (long long)g.nx * g.ny * g.nzAir;
     for (long long c = blockIdx.x * (long long)kT + threadIdx.x; c < nC; c += (long long)gridDim.x * kT) {
@@ -41,6 +41,7 @@ __global__ void ks_cells(Geo<double> g, const double *m_earth, double airCond, d
         const double s = c < nAir ? exp(airCond) : exp(m_earth[c - nAir]);
         VC[c] = v;
         CT[c] = v * s;
+        sigC[c] = s;
     }
 }
 
@@ -156,12 +157,12 @@ __global__ void ks_edge_final(Geo<double> g, double *sig, const double *sigs, fl
 }
 
 void launch_setup_cond(const Geo<double> &g, const double *m_earth, double airCond, double *VC, double *CT,
-                       double *sig, double *sigs, double *gdw, unsigned char *gde, double *gdn, double *coef,
+                       double *sigC, double *sig, double *sigs, double *gdw, unsigned char *gde, double *gdn, double *coef,
                        float *sig32, float *sigs32, float *gdw32, float *gdn32, cudaStream_t s)
 {
     const long long nC = (long long)g.nx * g.ny * g.nz;
     g_launch_count.fetch_add(4, std::memory_order_relaxed);
-    ks_cells<<<blocks(nC), kT, 0, s>>>(g, m_earth, airCond, VC, CT);
+    ks_cells<<<blocks(nC), kT, 0, s>>>(g, m_earth, airCond, VC, CT, sigC);
     ks_edge_sigma<<<blocks(g.nE), kT, 0, s>>>(g, VC, CT, sig, sigs);
     ks_nodes<<<blocks(g.nN), kT, 0, s>>>(g, VC, CT, sig, sigs, gdw, gde, gdn, gdw32, gdn32, coef);
     ks_edge_final<<<blocks(g.nE), kT, 0, s>>>(g, sig, sigs, sig32, sigs32);

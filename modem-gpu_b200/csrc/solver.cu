@@ -234,13 +234,13 @@ int Solver::update_cond(const double *m_earth, double airCond)
     if (sig64_.alloc(nE * sizeof(double)) || sig32_.alloc(nE * sizeof(float)) || coef_.alloc(7 * nN * sizeof(double)) ||
         sigs64_.alloc(nE * sizeof(double)) || sigs32_.alloc(nE * sizeof(float)) || gdw64_.alloc(nN * sizeof(double)) ||
         gdw32_.alloc(nN * sizeof(float)) || gde_.alloc(nN) || gdn64_.alloc(nN * sizeof(double)) ||
-        gdn32_.alloc(nN * sizeof(float)) || setup_.alloc((nEarth + 2 * nC) * sizeof(double)))
+        gdn32_.alloc(nN * sizeof(float)) || setup_.alloc((nEarth + 3 * nC) * sizeof(double)))
         return fail(8, "mt3d_update_cond: out of device memory");
-    double *m_d = setup_.as<double>(), *VC = m_d + nEarth, *CT = VC + nC;
+    double *m_d = setup_.as<double>(), *VC = m_d + nEarth, *CT = VC + nC, *sigC = CT + nC;
     if ((rc = check(cudaMemcpyAsync(m_d, m_earth, nEarth * sizeof(double), cudaMemcpyHostToDevice, stream_),
                     "copy model parameter")))
         return rc;
-    launch_setup_cond(g64_, m_d, airCond, VC, CT, sig64_.as<double>(), sigs64_.as<double>(), gdw64_.as<double>(),
+    launch_setup_cond(g64_, m_d, airCond, VC, CT, sigC, sig64_.as<double>(), sigs64_.as<double>(), gdw64_.as<double>(),
                       gde_.as<unsigned char>(), gdn64_.as<double>(), coef_.as<double>(), sig32_.as<float>(),
                       sigs32_.as<float>(), gdw32_.as<float>(), gdn32_.as<float>(), stream_);
     // sigma of both formulations and the signed node weights on the padded

@@ -77,6 +77,7 @@ class Solver {
     int profile(int enable);
     int kernel_time(int *launches, double *ms, int *precision);
     int get_cond(double *sigma_e, double *divcorr, double *node_w);
+    int compute_bc(int imode, double omega, double *e0, bool device);
     int pmult_t(int npol, const double *e0, const double *eadj, const double *m0, double *dm);
     int impedance(double omega, int nsite, const double *xyz, const double *origin, const double *e1, const double *e2,
                   double *Z, bool device);
@@ -123,7 +124,8 @@ class Solver {
     Geo<float> g32_{};
     DevBuf tab64_, tab32_, sig64_, sig32_, coef_, edgei_d_;
     DevBuf sigs64_, sigs32_, gdw64_, gdw32_, gde_, gdn64_, gdn32_;  // grad-div (SP2) data
-    DevBuf setup_;  // model parameter, V_C and V_C sigma_C of the operator set-up
+    DevBuf setup_;  // model parameter, V_C, V_C sigma_C and sigma_C of the operator set-up
+    DevBuf bcs_, bce_;  // 2-D boundary-condition scratch and host-bound output
     // padded FP32 layout of the TMA-staged kernels: sigma of both
     // formulations, signed node weights, the tensor maps and a device flag
     // that bounded waits set

@@ -3,11 +3,11 @@
 In ModEM the forward solve receives its boundary conditions from ``fwdSetup``
 (f90/3D_MT/ForwardSolver.f90:333-460), which calls ``ComputeBC`` ->
 ``BC_x0_WS`` (f90/3D_MT/FWD/boundary_ws.f90:21-168): one 2D TE solve per grid
-slice.  That set-up runs on the host before the solve and is outside the
-solver's C-ABI, which takes the boundary values as an input (a full edge
-vector whose boundary entries are used).
+slice.  The library computes that on the device (mt3d_compute_bc); the
+solve takes the boundary values as an input (a full edge vector whose
+boundary entries are used), so any other boundary data can be passed too.
 
-This module builds such boundary data from 1D plane-wave solutions: for each
+This module builds boundary data from 1D plane-wave solutions: for each
 boundary edge column the 1D finite-difference problem of that column's
 conductivity profile, discretised with exactly the z-part of the 3D curl-curl
 stencil, normalised to E = 1 at the top of the air and E = 0 at the bottom

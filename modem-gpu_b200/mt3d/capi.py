@@ -24,7 +24,7 @@ FORM_CCDC, FORM_CCGD = 0, 1
 
 #: every symbol include/mt3d.h declares
 EXPORTS = ["mt3d_version", "mt3d_device_count", "mt3d_create", "mt3d_destroy", "mt3d_set_control", "mt3d_update_cond",
-           "mt3d_get_cond", "mt3d_update_freq", "mt3d_set_formulation", "mt3d_sizes", "mt3d_interior_index", "mt3d_mult_aii",
+           "mt3d_get_cond", "mt3d_compute_bc", "mt3d_compute_bc_device", "mt3d_update_freq", "mt3d_set_formulation", "mt3d_sizes", "mt3d_interior_index", "mt3d_mult_aii",
            "mt3d_mult_aii_device_noalloc", "mt3d_bicg", "mt3d_fwdsolve",
            "mt3d_fwdsolve_batch", "mt3d_fwdsolve_batch_device", "mt3d_set_stream", "mt3d_profile",
            "mt3d_kernel_time", "mt3d_get_diag", "mt3d_get_batch_diag", "mt3d_pmult_t", "mt3d_impedance", "mt3d_impedance_device", "mt3d_lmult_t", "mt3d_lmult_t_device", "mt3d_launch_counter", "mt3d_last_error"]
@@ -57,6 +57,8 @@ def load(path: str = LIB_PATH):
     L.mt3d_set_control.argtypes = [P, I, I, I, C.c_double, C.c_double, C.c_double, I, I]
     L.mt3d_update_cond.argtypes = [P, D, C.c_double]
     L.mt3d_get_cond.argtypes = [P, D, D, D]
+    L.mt3d_compute_bc.argtypes = [P, I, D]
+    L.mt3d_compute_bc_device.argtypes = [P, I, C.c_double, C.c_void_p]
     L.mt3d_update_freq.argtypes = [P, C.c_double]
     L.mt3d_set_formulation.argtypes = [P, I]
     L.mt3d_sizes.argtypes = [P, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
@@ -150,6 +152,13 @@ class Solver:
         sig, coef, w = np.zeros(self.nE), np.zeros(7 * self.nN), np.zeros(self.nN)
         self._check(self.L.mt3d_get_cond(self.h, _d(sig), _d(coef), _d(w)))
         return sig, coef.reshape(7, self.nN), w
+
+    def compute_bc(self, imode):
+        """E0 of BC_x0_WS for polarisation imode (1 or 2) at the handle's
+        frequency: boundary entries are the BC, interior entries the first guess."""
+        e0 = np.zeros(self.nE, np.complex128)
+        self._check(self.L.mt3d_compute_bc(self.h, int(imode), _d(e0)))
+        return e0
 
     def update_freq(self, omega):
         self._check(self.L.mt3d_update_freq(self.h, float(omega)))

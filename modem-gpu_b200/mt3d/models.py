@@ -90,6 +90,36 @@ def make_grid(nx: int, ny: int, n_air: int, n_earth: int, core: float = 500.0, n
     return Grid(dx, dy, np.concatenate([air, earth]), n_air)
 
 
+def air_layers(dz_earth: np.ndarray, method: str, nz_air: int, *params: float) -> np.ndarray:
+    """Air-layer thicknesses (top down) of setup_airlayers
+    (f90/3D_MT/GridDef.f90:406-494) from the forward control line
+    (f90/3D_MT/FWD/EMsolve3D.f90:687-718; km on input):
+      "mirror" alpha min_top_dz: layer j above the surface (j = 1 next to it)
+        is alpha**(j-1) times earth layer j, the top one at least min_top_dz;
+      "fixed height" max_height: thicknesses growing log-uniformly from the
+        first earth layer to a total of max_height."""
+    dz_earth = np.asarray(dz_earth, np.float64)
+    dz = np.empty(nz_air)
+    if method.startswith("mirror"):
+        alpha, min_top = params[0], 1000.0 * params[1]
+        for iz in range(nz_air, 0, -1):
+            j = nz_air - iz + 1
+            dz[iz - 1] = (alpha ** (j - 1)) * dz_earth[j - 1]
+        if dz[0] < min_top:
+            dz[0] = min_top
+    elif method.startswith("fixed height"):
+        max_height = 1000.0 * params[0]
+        z1 = math.log10(dz_earth[0])
+        dlog = (math.log10(max_height) - z1) / nz_air
+        zl = z1
+        for iz in range(nz_air, 0, -1):
+            dz[iz - 1] = 10.0 ** (zl + dlog) - 10.0 ** zl
+            zl = zl + dlog
+    else:
+        raise ValueError(f"unknown air-layer method {method!r}")
+    return dz
+
+
 def gaussian_random_field(shape, corr_len_cells: float, seed: int) -> np.ndarray:
     """Zero-mean, unit-variance stationary Gaussian field with exponential
     covariance exp(-|h|/L) (h in cell units), sampled by circulant embedding on

@@ -8,10 +8,11 @@ The oracle restates ModEM's matrix-free 3D-MT forward solver
 (f90/3D_MT/FWD/modelOperator3D.f90, f90/3D_MT/FWD/EMsolve3D.f90,
 f90/3D_MT/FWD/solver.f90) and the sensitivity glue
 (f90/3D_MT/SolverSens.f90:63-116, f90/3D_MT/modelParam/ModelMap.inc).
-Parity unpinned: the reference (Fortran) cannot be built here and its one
-forward fixture (unit_testing/3D/CylinderModel_1per.dat, impedances) needs
-the 2-D boundary solver and the impedance functional, which are not
-restated.  The oracle is pinned instead by a closed-form layered solution,
+Pinned against the reference's forward fixture
+unit_testing/3D/CylinderModel_1per.dat: with the boundary conditions of
+oracle/bc2d.py and the impedance functional of oracle/datafunc.py it
+reproduces the file's 2501 impedance tensors to the 7 digits the file prints
+(tests/test_golden.py).  Also checked against a closed-form layered solution,
 scipy direct solves, the CC-DC/SP2 equivalence and operator identities
 (tests/test_oracle.py).
 """

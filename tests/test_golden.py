@@ -1,0 +1,112 @@
+"""The reference's own forward fixture: unit_testing/3D/CylinderModel_1per.dat.
+
+Full_Impedance at 2501 surface sites, period 1000 s, written by the
+reference's forward run on CylinderModel+QuarterSpace.rho (48 x 68 earth
+cells, a 0.1 ohm-m cylinder at 6-16 km in a 100 ohm-m / 10 ohm-m vertical
+contact; tests/golden/make_cylinder.py extracts it into
+tests/golden/cylinder_1per.npz).  The whole forward chain is exercised:
+BC_x0_WS boundary conditions and first guess, the divergence-corrected
+solve, and dataResp with the file's units ([mV/km]/[nT], i.e. SI E/B times
+1e-3) and sign convention (exp(+i omega t): the conjugate of the reference's
+internal ISIGN = -1 values).
+
+Grid: 12 air layers to 1000 km ("fixed height 12 1000", the air set-up of the
+reference's own log of this test, unit_testing/3D/CylinderModel_FWD.out, and
+of unit_testing/3D/FWD_3D.m) over the model's top 36 earth layers, whose
+base lies at 100.0 km.  The file agrees with that grid to the precision it
+prints (7 digits); with all 44 layers of the model file (base at 1000 km) it
+differs by exactly what a perfect conductor at 100 km explains (on the
+100 ohm-m side, apparent resistivity 72 ohm-m and phase 73 degrees instead of
+100 ohm-m and 45 degrees), so the data were made with the 100 km version of
+the model.
+
+Tolerances, per site relative to |Zxy|: the oracle (QMR + D-ILU, the
+reference's solver) within 1e-5; the GPU (BiCGStab, FP64 and mixed
+precision, every solve to relative residual 1e-7 like the reference's)
+within 5e-4, median within 1e-5.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from mt3d import models
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+N_EARTH = 36
+
+
+def cylinder():
+    f = np.load(os.path.join(HERE, "golden", "cylinder_1per.npz"))
+    nx, ny = f["dx"].size, f["dy"].size
+    air = models.air_layers(f["dz_earth"], "fixed height", 12, 1000.0)
+    g = models.Grid(f["dx"], f["dy"], np.concatenate([air, f["dz_earth"][:N_EARTH]]), air.size)
+    m = f["m_earth"].reshape(nx, ny, -1, order="F")[:, :, :N_EARTH]
+    model = models.Model(g, models.flat_f(m))
+    omega = 2 * models.PI_REF / float(f["period"])
+    return g, model, omega, f["sites"], f["origin"], f["Z"]
+
+
+def to_file_units(Z):
+    """SI E/B with ISIGN = -1 -> [mV/km]/[nT], exp(+i omega t)
+    (ImpUnits, f90/3D_MT/DICT/dataTypes.f90:252-315; conjugation,
+    f90/3D_MT/DataIO.f90:276-280)."""
+    return np.conj(Z) * 1e-3
+
+
+def site_errors(Z, G):
+    return np.abs(Z - G) / np.abs(G[:, 0, 1])[:, None, None]
+
+
+def test_oracle_reproduces_cylinder_fixture():
+    from oracle import bc2d, datafunc
+    from oracle.oracle import PC_DILU, QMR, Oracle
+    g, m, omega, sites, origin, G = cylinder()
+    o = Oracle(g)
+    o.update_cond(m.m_earth, m.air_cond)
+    o.update_freq(omega)
+    o.set_control(solver=QMR, precond=PC_DILU)
+    s = bc2d.sigma_cells(g, m.m_earth, m.air_cond)
+    E = []
+    for imode in (1, 2):
+        e0 = bc2d.compute_bc(g, s, omega, imode)
+        e, rc = o.fwdsolve(bc=e0, e0=e0)
+        assert rc == 0
+        E.append(e)
+    c = datafunc.coords(g.dx, g.dy, g.dz, g.nzAir, origin)
+    err = site_errors(to_file_units(datafunc.impedance(c, omega, sites, E[0], E[1])), G)
+    assert err.max() < 1e-5, err.max()
+    assert np.median(err) < 1e-6
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("formulation,solver,cycle,precision", [
+    (0, 3, 100, 0), (0, 3, 100, 1),      # curl-curl + divergence correction, BiCGStab + z-line
+    (1, 1, 1000, 0), (1, 1, 1000, 1),    # curl-curl + grad-div, BiCGStab + diagonal
+])
+def test_gpu_reproduces_cylinder_fixture(cuda, formulation, solver, cycle, precision):
+    """The device chain (mt3d_compute_bc, mt3d_fwdsolve, mt3d_impedance) on the
+    reference's fixture.  The diagonally preconditioned BiCGStab of the
+    curl-curl + divergence-correction system stalls near 1e-2 on this grid
+    (air layers up to 580 km thick over 28 m surface cells); the z-line
+    preconditioner with 100 iterations between divergence corrections, or
+    the grad-div formulation with 1000-iteration restart cycles, converge."""
+    from mt3d import capi
+    g, m, omega, sites, origin, G = cylinder()
+    s = capi.Solver(g)
+    s.set_formulation(formulation)
+    s.update_cond(m.m_earth, m.air_cond)
+    s.update_freq(omega)
+    s.set_control(IterPerDivCor=cycle, MaxDivCor=8000 // cycle, solver=solver, precision=precision)
+    E = []
+    for imode in (1, 2):
+        e0 = s.compute_bc(imode)
+        e, rc = s.fwdsolve(bc=e0, e0=e0)
+        d = s.diagnostics()
+        print("imode", imode, "iterations", d["nIterTotal"], "cycles", d["nDivCor"], "relres", d["final_relres"])
+        assert rc == 0
+        E.append(e)
+    err = site_errors(to_file_units(s.impedance(omega, sites, E[0], E[1], origin=origin)), G)
+    print("max", err.max(), "median", np.median(err))
+    assert err.max() < 5e-4, err.max()
+    assert np.median(err) < 1e-5

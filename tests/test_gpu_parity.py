@@ -87,6 +87,35 @@ def test_operator_setup_matches_oracle(prob):
     assert np.all(coef[:, ~inner] == 0)
 
 
+@pytest.mark.parametrize("imode", [1, 2])
+def test_compute_bc_matches_oracle(prob, imode):
+    """E0 of the 2-D TE boundary solver on the device (band elimination in
+    shared memory) against the oracle's sparse direct solves: relative 1e-10."""
+    from oracle import bc2d
+    g, m, omega, o, s = prob
+    e = s.compute_bc(imode)
+    want = bc2d.compute_bc(g, bc2d.sigma_cells(g, m.m_earth, m.air_cond), omega, imode)
+    assert np.max(np.abs(e - want)) < 1e-10 * np.max(np.abs(want))
+
+
+def test_compute_bc_tall_slices(cuda):
+    """72 vertical cells: the elimination window (72 x 72 complex, 81 KB) takes
+    the opted-in shared memory and 32 x 32 threads."""
+    from oracle import bc2d
+    g = models.make_grid(8, 9, 20, 52, core=500.0, n_pad=2, pad_growth=1.6, air_first=60.0, air_growth=1.3,
+                         earth_first=40.0, earth_growth=1.08)
+    m = random_model(g, seed=5)
+    omega = 2 * np.pi * 3.0
+    s = capi.Solver(g)
+    s.update_cond(m.m_earth, m.air_cond)
+    s.update_freq(omega)
+    sig = bc2d.sigma_cells(g, m.m_earth, m.air_cond)
+    for imode in (1, 2):
+        e = s.compute_bc(imode)
+        want = bc2d.compute_bc(g, sig, omega, imode)
+        assert np.max(np.abs(e - want)) < 1e-10 * np.max(np.abs(want))
+
+
 def test_bicg_history_matches_oracle(prob):
     g, m, omega, o, s = prob
     mask = interior_edge_mask(g)

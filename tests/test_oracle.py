@@ -267,3 +267,30 @@ def test_datafunc_lmult_t_is_the_derivative_of_z():
     lhs = s1 @ de1 + s2 @ de2
     rhs = np.sum(np.conj(d) * dz)
     assert abs(lhs - rhs) < 1e-7 * abs(rhs)
+
+
+def test_bc2d_layered_slices_equal_the_1d_column():
+    """For a layered earth every 2-D TE slice of BC_x0_WS reduces to the 1-D TE
+    column solution (the lateral terms cancel and the 2-D vertical terms equal
+    Fwd1D_TE's), so E0 on each x-edge column equals fwd1d_te of that column."""
+    from oracle import bc2d
+    g = small_grid()
+    rho = np.array([100.0, 30.0, 3.0, 300.0, 10.0, 10.0, 50.0, 50.0])
+    m = np.broadcast_to(-np.log(rho)[None, None, :], (g.nx, g.ny, g.nzEarth))
+    model = models.Model(g, models.flat_f(m))
+    s = bc2d.sigma_cells(g, model.m_earth, model.air_cond)
+    omega = 2 * np.pi * 0.7
+    om2 = (2 * bc2d.PI_REF) / ((2 * bc2d.PI_REF) / omega)
+    col = bc2d.fwd1d_te(om2, g.nzAir, np.asarray(g.dz, float), s[0, 0, g.nzAir:])
+    for imode in (1, 2):
+        e = bc2d.compute_bc(g, s, omega, imode)
+        nX, nY = g.nx * (g.ny + 1) * (g.nz + 1), (g.nx + 1) * g.ny * (g.nz + 1)
+        if imode == 2:
+            f = e[:nX].reshape(g.nx, g.ny + 1, g.nz + 1, order="F")
+        else:
+            f = e[nX:nX + nY].reshape(g.nx + 1, g.ny, g.nz + 1, order="F")
+        want = np.broadcast_to(col[:g.nz], f[:, :, :g.nz].shape)
+        assert np.max(np.abs(f[:, :, :g.nz] - want)) < 1e-10 * np.max(np.abs(col))
+        assert np.all(f[:, :, g.nz] == 0)  # bottom face zeroed
+        other = e[nX:] if imode == 2 else np.concatenate([e[:nX], e[nX + nY:]])
+        assert np.all(other == 0)
