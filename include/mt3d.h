@@ -280,6 +280,31 @@ MT3D_API int mt3d_lmult_t_device(mt3d_handle h, double omega, int nsite, const d
                                  double *s2_dev);
 
 /* Number of kernels the library has launched in this process (all handles). */
+/* E-field solution files in the reference's binary layout (write_solnVectorMTX
+ * / read_solnVectorMTX, f90/3D_MT/ioMod/ioAscii.f90:493-597, with
+ * FileWriteInit :188-215, FileReadInit f90/3D_MT/ioMod/ioBinary.f90:61-93,
+ * EfileWrite / EfileRead :314-368): Fortran unformatted sequential records
+ * (int32 length before and after each), a header with the grid, then per
+ * transmitter j and polarisation k a record (omega, j, k, name) and the Ex,
+ * Ey, Ez blocks of the full edge vector.  Files written by the reference on a
+ * little-endian host read here and the other way round.
+ *   mt3d_write_soln: e holds nTx * nPol full edge vectors (transmitter major)
+ *     in host memory, or device memory when device != 0; omegas[nTx];
+ *     origin[3] (grid%ox, oy, oz; may be NULL for zeros) and rotdeg go to the
+ *     header; the polarisations of a two-polarisation file are named Ex, Ey.
+ *   mt3d_read_soln: one full edge vector (transmitter iTx, polarisation iPol,
+ *     1-based) into e (host, or device when device != 0) and its omega; the
+ *     file's grid sizes must match the handle's.
+ *   mt3d_read_soln_header: the header without a handle; any output may be
+ *     NULL (dx, dy, dz take nx, ny, nz entries; nz includes the air).
+ * Field components longer than 2^31 - 1 bytes (gfortran sub-records) are
+ * refused. */
+MT3D_API int mt3d_write_soln(mt3d_handle h, const char *path, int nTx, int nPol, const double *omegas,
+                             const double *origin, double rotdeg, const double *e, int device);
+MT3D_API int mt3d_read_soln(mt3d_handle h, const char *path, int iTx, int iPol, double *omega, double *e, int device);
+MT3D_API int mt3d_read_soln_header(const char *path, int *nTx, int *nPol, int *nx, int *ny, int *nz, int *nzAir,
+                                   double *origin, double *rotdeg, double *dx, double *dy, double *dz);
+
 MT3D_API int64_t mt3d_launch_counter(void);
 
 /* Message of the last error on the handle (NUL-terminated, truncated to len). */

@@ -300,6 +300,28 @@ int mt3d_pmult_t(mt3d_handle h, int npol, const double *e0, const double *eadj, 
 
 int64_t mt3d_launch_counter(void) { return mt3d::g_launch_count.load(); }
 
+int mt3d_write_soln(mt3d_handle h, const char *path, int nTx, int nPol, const double *omegas, const double *origin,
+                    double rotdeg, const double *e, int device)
+{
+    return wrap(h, [&] { return h->s.write_soln(path, nTx, nPol, omegas, origin, rotdeg, e, device != 0); });
+}
+
+int mt3d_read_soln(mt3d_handle h, const char *path, int iTx, int iPol, double *omega, double *e, int device)
+{
+    return wrap(h, [&] { return h->s.read_soln(path, iTx, iPol, omega, e, device != 0); });
+}
+
+int mt3d_read_soln_header(const char *path, int *nTx, int *nPol, int *nx, int *ny, int *nz, int *nzAir, double *origin,
+                          double *rotdeg, double *dx, double *dy, double *dz)
+{
+    try {
+        return mt3d::read_soln_header(path, nTx, nPol, nx, ny, nz, nzAir, origin, rotdeg, dx, dy, dz, g_create_error);
+    } catch (...) {
+        g_create_error = "host out of memory";
+        return MT3D_OUT_OF_MEMORY;
+    }
+}
+
 int mt3d_last_error(mt3d_handle h, char *buf, int len)
 {
     if (!buf || len < 1) return MT3D_INVALID_ARGUMENT;

@@ -62,6 +62,10 @@ struct Workspace {
     DevBuf bst, pst, ost, parts, cnt, rerr, dcrerr;
 };
 
+// header of a solution file (solnio.cu); any output may be NULL
+int read_soln_header(const char *path, int *nTx, int *nMode, int *nx, int *ny, int *nz, int *nzAir, double *origin,
+                     double *rotdeg, double *dx, double *dy, double *dz, std::string &err);
+
 class Solver {
   public:
     ~Solver();
@@ -78,6 +82,9 @@ class Solver {
     int kernel_time(int *launches, double *ms, int *precision);
     int get_cond(double *sigma_e, double *divcorr, double *node_w);
     int compute_bc(int imode, double omega, double *e0, bool device);
+    int write_soln(const char *path, int nTx, int nPol, const double *omegas, const double *origin, double rotdeg,
+                   const double *e, bool device);
+    int read_soln(const char *path, int iTx, int iPol, double *omega, double *e, bool device);
     int pmult_t(int npol, const double *e0, const double *eadj, const double *m0, double *dm);
     int impedance(double omega, int nsite, const double *xyz, const double *origin, const double *e1, const double *e2,
                   double *Z, bool device);

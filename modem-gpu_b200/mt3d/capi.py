@@ -27,7 +27,7 @@ EXPORTS = ["mt3d_version", "mt3d_device_count", "mt3d_create", "mt3d_destroy", "
            "mt3d_get_cond", "mt3d_compute_bc", "mt3d_compute_bc_device", "mt3d_update_freq", "mt3d_set_formulation", "mt3d_sizes", "mt3d_interior_index", "mt3d_mult_aii",
            "mt3d_mult_aii_device_noalloc", "mt3d_bicg", "mt3d_fwdsolve",
            "mt3d_fwdsolve_batch", "mt3d_fwdsolve_batch_device", "mt3d_set_stream", "mt3d_profile",
-           "mt3d_kernel_time", "mt3d_get_diag", "mt3d_get_batch_diag", "mt3d_pmult_t", "mt3d_impedance", "mt3d_impedance_device", "mt3d_lmult_t", "mt3d_lmult_t_device", "mt3d_launch_counter", "mt3d_last_error"]
+           "mt3d_kernel_time", "mt3d_get_diag", "mt3d_get_batch_diag", "mt3d_pmult_t", "mt3d_impedance", "mt3d_impedance_device", "mt3d_lmult_t", "mt3d_lmult_t_device", "mt3d_write_soln", "mt3d_read_soln", "mt3d_read_soln_header", "mt3d_launch_counter", "mt3d_last_error"]
 
 _lib = None
 
@@ -80,6 +80,9 @@ def load(path: str = LIB_PATH):
     L.mt3d_get_batch_diag.argtypes = [P, I, IP, D]
     L.mt3d_pmult_t.argtypes = [P, I, D, D, D, D]
     L.mt3d_last_error.argtypes = [P, C.c_char_p, I]
+    L.mt3d_write_soln.argtypes = [P, C.c_char_p, I, I, D, D, C.c_double, C.c_void_p, I]
+    L.mt3d_read_soln.argtypes = [P, C.c_char_p, I, I, D, C.c_void_p, I]
+    L.mt3d_read_soln_header.argtypes = [C.c_char_p, IP, IP, IP, IP, IP, IP, D, D, D, D, D]
     L.mt3d_launch_counter.restype = C.c_int64
     L.mt3d_launch_counter.argtypes = []
     for name in EXPORTS:
@@ -159,6 +162,34 @@ class Solver:
         e0 = np.zeros(self.nE, np.complex128)
         self._check(self.L.mt3d_compute_bc(self.h, int(imode), _d(e0)))
         return e0
+
+    def write_soln(self, path, omegas, e, origin=(0.0, 0.0, 0.0), rotdeg=0.0):
+        """e: host array [nTx, nPol, nE] (complex128), or (device address as
+        int, nTx, nPol) for fields in device memory."""
+        om = np.ascontiguousarray(omegas, np.float64)
+        org = np.ascontiguousarray(origin, np.float64)
+        if isinstance(e, tuple):
+            ptr, ntx, npol = e
+            rc = self.L.mt3d_write_soln(self.h, os.fsencode(path), ntx, npol, _d(om), _d(org), float(rotdeg),
+                                        C.c_void_p(ptr), 1)
+        else:
+            a = np.ascontiguousarray(e, np.complex128)
+            rc = self.L.mt3d_write_soln(self.h, os.fsencode(path), a.shape[0], a.shape[1], _d(om), _d(org),
+                                        float(rotdeg), a.ctypes.data_as(C.c_void_p), 0)
+        self._check(rc)
+
+    def read_soln(self, path, itx, ipol, device_ptr=None):
+        """(omega, field) of transmitter itx, polarisation ipol (1-based); with
+        device_ptr the field goes to that device address and None is returned."""
+        om = C.c_double()
+        if device_ptr is not None:
+            self._check(self.L.mt3d_read_soln(self.h, os.fsencode(path), itx, ipol, C.byref(om),
+                                              C.c_void_p(device_ptr), 1))
+            return om.value, None
+        e = np.zeros(self.nE, np.complex128)
+        self._check(self.L.mt3d_read_soln(self.h, os.fsencode(path), itx, ipol, C.byref(om),
+                                          e.ctypes.data_as(C.c_void_p), 0))
+        return om.value, e
 
     def update_freq(self, omega):
         self._check(self.L.mt3d_update_freq(self.h, float(omega)))
@@ -302,3 +333,27 @@ class Solver:
 
 def device_count() -> int:
     return int(load().mt3d_device_count())
+
+
+def read_soln_header(path):
+    """Header of a solution file: dict with nTx, nPol, the grid (dx, dy, dz,
+    nzAir), origin and rotation."""
+    L = load()
+    v = [C.c_int() for _ in range(6)]
+    org, rot = np.zeros(3), C.c_double()
+    rc = L.mt3d_read_soln_header(os.fsencode(path), *[C.byref(x) for x in v], _d(org), C.byref(rot), None, None, None)
+    if rc:
+        raise MT3DError(rc, _last_global_error(L))
+    ntx, npol, nx, ny, nz, nza = (x.value for x in v)
+    dx, dy, dz = np.zeros(nx), np.zeros(ny), np.zeros(nz)
+    rc = L.mt3d_read_soln_header(os.fsencode(path), None, None, None, None, None, None, None, None, _d(dx), _d(dy),
+                                 _d(dz))
+    if rc:
+        raise MT3DError(rc, _last_global_error(L))
+    return dict(nTx=ntx, nPol=npol, dx=dx, dy=dy, dz=dz, nzAir=nza, origin=org, rotdeg=rot.value)
+
+
+def _last_global_error(L):
+    buf = C.create_string_buffer(512)
+    L.mt3d_last_error(None, buf, 512)
+    return buf.value.decode()
