@@ -220,11 +220,14 @@ MT3D_API int mt3d_set_stream(mt3d_handle h, void *stream);
 
 /* Kernel timing: with enable != 0 every launch of the BiCGStab stencil
  * kernels (v = A ph with the fused dot product) is bracketed by CUDA events
- * on the solver stream.  mt3d_kernel_time returns the number of timed
- * launches and their summed device time in milliseconds since the last
- * enable, and the precision (0 FP64, 1 FP32) of the last timed launch. */
+ * on the solver stream.  mt3d_kernel_time returns, for the launches of one
+ * precision (0 FP64, 1 FP32) since the last enable, their number, their
+ * summed device time in milliseconds and rhs_sweeps: the number of
+ * (launch, right-hand side) pairs in which the staged stencil kernels swept a
+ * still-running right-hand side, i.e. the stencil work in units of nE edges.
+ * Any output may be NULL. */
 MT3D_API int mt3d_profile(mt3d_handle h, int enable);
-MT3D_API int mt3d_kernel_time(mt3d_handle h, int *launches, double *ms, int *precision);
+MT3D_API int mt3d_kernel_time(mt3d_handle h, int precision, int *launches, double *ms, int64_t *rhs_sweeps);
 
 /* Solver diagnostics of the last mt3d_fwdsolve (getEMsolveDiag,
  * f90/3D_MT/FWD/EMsolve3D.f90:866-876): total Krylov iterations, number of

@@ -255,9 +255,9 @@ int mt3d_profile(mt3d_handle h, int enable)
     return wrap(h, [&] { return h->s.profile(enable); });
 }
 
-int mt3d_kernel_time(mt3d_handle h, int *launches, double *ms, int *precision)
+int mt3d_kernel_time(mt3d_handle h, int precision, int *launches, double *ms, int64_t *rhs_sweeps)
 {
-    return wrap(h, [&] { return h->s.kernel_time(launches, ms, precision); });
+    return wrap(h, [&] { return h->s.kernel_time(precision, launches, ms, rhs_sweeps); });
 }
 
 int mt3d_get_diag(mt3d_handle h, int *nIterTotal, int *nDivCor, int *failed, double *EMrelErr, int len, double *divJ,

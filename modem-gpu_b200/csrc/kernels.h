@@ -62,6 +62,9 @@ template <typename T> struct KArgs {
     PadLayout pl;
     int *err;  // set by a bounded device-side wait that gave up
     const struct TmaMaps *tma;  // host pointer: tensor maps of the padded vectors (colstencil == 3)
+    // profiling: the staged stencil kernels count one sweep per active
+    // right-hand side and launch here (nullptr when not profiling)
+    unsigned long long *sweeps;
 };
 
 // arguments of the divergence-correction kernels (FP64)

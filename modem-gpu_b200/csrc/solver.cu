@@ -54,9 +54,14 @@ int Solver::profile(int enable)
 {
     if (stream_) cudaStreamSynchronize(stream_);
     prof_ = enable != 0;
-    prof_launches_ = 0;
-    prof_ms_ = 0.0;
+    prof_launches_[0] = prof_launches_[1] = 0;
+    prof_ms_[0] = prof_ms_[1] = 0.0;
     ev_used_ = 0;
+    if (prof_) {
+        if (prof_cnt_.alloc(2 * sizeof(unsigned long long))) return fail(8, "mt3d_profile: out of device memory");
+        if (int rc = check(cudaMemset(prof_cnt_.as<void>(), 0, 2 * sizeof(unsigned long long)), "mt3d_profile"))
+            return rc;
+    }
     return 0;
 }
 
@@ -68,20 +73,22 @@ cudaEvent_t *Solver::next_events(int n)
         if (cudaEventCreate(&e) != cudaSuccess) { cudaGetLastError(); return nullptr; }
         ev_.push_back(e);
     }
+    ev_prec_.resize(ev_.size());
+    for (int q = 0; q < n; q++) ev_prec_[ev_used_ + q] = prof_cur_;
     cudaEvent_t *p = &ev_[ev_used_];
     ev_used_ += n;
     return p;
 }
 
-// sum the elapsed time of the recorded (start, stop) pairs; the stream must
-// have been synchronised
+// sum the elapsed time of the recorded (start, stop) pairs per precision; the
+// stream must have been synchronised
 void Solver::collect_events()
 {
     for (size_t i = 0; i + 1 < ev_used_; i += 2) {
         float ms = 0.f;
         if (cudaEventElapsedTime(&ms, ev_[i], ev_[i + 1]) == cudaSuccess) {
-            prof_ms_ += ms;
-            prof_launches_ += 1;
+            prof_ms_[ev_prec_[i] ? 1 : 0] += ms;
+            prof_launches_[ev_prec_[i] ? 1 : 0] += 1;
         } else {
             cudaGetLastError();
         }
@@ -89,13 +96,20 @@ void Solver::collect_events()
     ev_used_ = 0;
 }
 
-int Solver::kernel_time(int *launches, double *ms, int *precision)
+int Solver::kernel_time(int precision, int *launches, double *ms, int64_t *sweeps)
 {
+    if (precision != 0 && precision != 1) return fail(5, "mt3d_kernel_time: precision must be 0 or 1");
     if (stream_) cudaStreamSynchronize(stream_);
     collect_events();
-    if (launches) *launches = prof_launches_;
-    if (ms) *ms = prof_ms_;
-    if (precision) *precision = prof_prec_;
+    if (launches) *launches = prof_launches_[precision];
+    if (ms) *ms = prof_ms_[precision];
+    if (sweeps) {
+        unsigned long long c[2] = {0, 0};
+        if (prof_cnt_.bytes() >= sizeof c &&
+            cudaMemcpy(c, prof_cnt_.as<void>(), sizeof c, cudaMemcpyDeviceToHost) != cudaSuccess)
+            cudaGetLastError();
+        *sweeps = (int64_t)c[precision];
+    }
     return 0;
 }
 
@@ -417,6 +431,7 @@ template <> KArgs<double> Solver::kargs<double>(int nrhs, int)
 {
     KArgs<double> a{};
     Workspace &w = ws_;
+    a.sweeps = prof_ ? prof_cnt_.as<unsigned long long>() + 0 : nullptr;
     a.g = g64_;
     a.sigma = sig64_.as<double>();
     a.ost = w.ost.as<OuterState>();
@@ -454,6 +469,7 @@ template <> KArgs<float> Solver::kargs<float>(int nrhs, int)
 {
     KArgs<float> a{};
     Workspace &w = ws_;
+    a.sweeps = prof_ ? prof_cnt_.as<unsigned long long>() + 1 : nullptr;
     a.g = g32_;
     a.sigma = sig32_.as<float>();
     a.ost = w.ost.as<OuterState>();
@@ -565,7 +581,7 @@ DArgs Solver::dargs(int nrhs)
 
 int Solver::run_bicg(int nrhs, int precision, int maxit)
 {
-    if (prof_) prof_prec_ = precision;
+    prof_cur_ = precision;
     if (ctl.solver == 2) {  // Bi-CG for the complex-symmetric system (COCG) with z-line preconditioner
         if (precision == 0) {
             KArgs<double> a = kargs<double>(nrhs, 0);

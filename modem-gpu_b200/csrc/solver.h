@@ -79,7 +79,7 @@ class Solver {
               int *status, bool device = false);
     int set_stream(void *s);
     int profile(int enable);
-    int kernel_time(int *launches, double *ms, int *precision);
+    int kernel_time(int precision, int *launches, double *ms, int64_t *sweeps);
     int get_cond(double *sigma_e, double *divcorr, double *node_w);
     int compute_bc(int imode, double omega, double *e0, bool device);
     int write_soln(const char *path, int nTx, int nPol, const double *omegas, const double *origin, double rotdeg,
@@ -123,8 +123,10 @@ class Solver {
     bool prof_ = false;
     std::vector<cudaEvent_t> ev_;
     size_t ev_used_ = 0;
-    int prof_launches_ = 0, prof_prec_ = 0;
-    double prof_ms_ = 0.0;
+    int prof_launches_[2] = {0, 0}, prof_cur_ = 0;  // per precision (0 FP64, 1 FP32)
+    double prof_ms_[2] = {0.0, 0.0};
+    std::vector<int> ev_prec_;  // precision of each recorded event
+    DevBuf prof_cnt_;           // device sweep counters [FP64, FP32]
     cudaEvent_t *next_events(int n);
     void collect_events();
     Geo<double> g64_{};

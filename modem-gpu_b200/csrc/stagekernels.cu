@@ -80,6 +80,7 @@ template <typename T> __global__ void __launch_bounds__(kThreads, sizeof(T) == 4
     const int r = blockIdx.y;
     BicgState &st = a.st[r];
     if (st.status != KS_RUNNING || !a.ost[r].active) return;
+    if (a.sweeps && threadIdx.x == 0 && blockIdx.x == 0 && blockIdx.z == 0) atomicAdd(a.sweeps, 1ULL);
     int i0, j0, k0, k1;
     stage_tile(a.cmap, i0, j0);
     stage_range(a.g, k0, k1);

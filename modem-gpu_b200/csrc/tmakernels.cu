@@ -372,6 +372,7 @@ __global__ void __launch_bounds__(kThreads, 3) kct_vt(const __grid_constant__ Tm
     const int r = blockIdx.y;
     BicgState &st = a.st[r];
     if (st.status != KS_RUNNING || !a.ost[r].active) return;
+    if (a.sweeps && threadIdx.x == 0 && blockIdx.x == 0 && blockIdx.z == 0) atomicAdd(a.sweeps, 1ULL);
     int i0, j0, k0, k1;
     tma_tile(a.cmap, i0, j0);
     tma_range(a.g.nz, k0, k1);

@@ -75,7 +75,7 @@ def load(path: str = LIB_PATH):
     L.mt3d_fwdsolve_batch_device.argtypes = [P, I, D, IP, C.c_void_p, C.c_void_p, C.c_void_p, IP]
     L.mt3d_set_stream.argtypes = [P, C.c_void_p]
     L.mt3d_profile.argtypes = [P, I]
-    L.mt3d_kernel_time.argtypes = [P, IP, D, IP]
+    L.mt3d_kernel_time.argtypes = [P, I, IP, D, C.POINTER(C.c_int64)]
     L.mt3d_get_diag.argtypes = [P, IP, IP, IP, D, I, D, I, D]
     L.mt3d_get_batch_diag.argtypes = [P, I, IP, D]
     L.mt3d_pmult_t.argtypes = [P, I, D, D, D, D]
@@ -298,10 +298,12 @@ class Solver:
     def profile(self, enable=True):
         self._check(self.L.mt3d_profile(self.h, int(enable)))
 
-    def kernel_time(self):
-        n, ms, prec = C.c_int(), C.c_double(), C.c_int()
-        self._check(self.L.mt3d_kernel_time(self.h, C.byref(n), C.byref(ms), C.byref(prec)))
-        return n.value, ms.value, prec.value
+    def kernel_time(self, precision):
+        """(timed launches, device ms, right-hand-side sweeps) of the stencil
+        launches of one precision (0 FP64, 1 FP32) since profile(True)."""
+        n, ms, sw = C.c_int(), C.c_double(), C.c_int64()
+        self._check(self.L.mt3d_kernel_time(self.h, int(precision), C.byref(n), C.byref(ms), C.byref(sw)))
+        return n.value, ms.value, sw.value
 
     def diagnostics(self, maxlen=4000, maxdc=200):
         nit, ndc, fl = C.c_int(), C.c_int(), C.c_int()
