@@ -856,6 +856,10 @@ int Solver::solve(int nrhs, const double *omegas, const int *trans, const double
     // that is already small relative to the field)
     std::vector<double> prev_relres(nrhs, std::numeric_limits<double>::infinity());
     std::vector<char> hi(nrhs, 0);
+    // smallest relative residual of the last FP32 cycle's own iteration and
+    // the number of FP32 cycles in a row that did not halve the true residual
+    std::vector<double> inner_best(nrhs, 0.0);
+    std::vector<int> stalls(nrhs, 0);
     while (any_active()) {
         if (refine) {
             // true FP64 residual r64 = b - A X (into tmp); converged right-hand
@@ -876,7 +880,18 @@ int Solver::solve(int nrhs, const double *omegas, const int *trans, const double
                 if (o.relres <= o.tol) { o.active = 0; o.converged = 1; continue; }
                 if (o.nDivCor >= ctl.MaxDivCor) { o.active = 0; o.failed = 1; continue; }
                 o.tol_inner = o.tol * o.bnorm64 * o.scale;  // tol*||b|| relative to ||r64||
-                if (prec == 1 && !hi[r] && o.relres > 0.5 * prev_relres[r]) hi[r] = 1;
+                // an FP32 cycle that did not halve the true residual: when its
+                // own iteration converged well, the FP32 operator's rounding is
+                // the limit and the right-hand side moves to FP64; when the
+                // iteration itself stagnated, one more FP32 cycle restarts it
+                // from the new residual first
+                if (prec == 1 && !hi[r]) {
+                    if (o.relres > 0.5 * prev_relres[r]) {
+                        if (inner_best[r] < 0.1 || ++stalls[r] >= 2) hi[r] = 1;
+                    } else {
+                        stalls[r] = 0;
+                    }
+                }
                 prev_relres[r] = o.relres;
                 work = true;
             }
@@ -939,6 +954,11 @@ int Solver::solve(int nrhs, const double *omegas, const int *trans, const double
             double *h = &rerr[(size_t)r * (maxit + 1)];
             if (!conv) h[maxit - 1] = st.imin > 0 ? h[st.imin - 1] : h[0];
             for (int k = 0; k < niter; k++) dg[r].EMrelErr.push_back(h[k]);
+            if (prec == 1 && !hi[r]) {
+                double best = 1.0;
+                for (int k = 0; k < niter; k++) best = std::min(best, h[k]);
+                inner_best[r] = best;
+            }
             o.nIterTotal += niter;
             if (!refine) {
                 if (conv) o.converged = 1;

@@ -4,7 +4,8 @@
 // A block owns 32 x 8 node columns of one right-hand side and marches a chunk
 // of node planes, as the cp.async kernels of stagekernels.cu do.  Per plane
 // one thread issues three tensor copies into a four-slot ring in shared
-// memory, completed on an mbarrier per slot:
+// memory (separate rings for fields, sigma and node weights), completed on an
+// mbarrier per plane slot:
 //   - Ex, Ey, Ez over i0-2 .. i0+33, j0-1 .. j0+8 (one copy for the three
 //     components: box 72 floats x 10 rows x 3 components),
 //   - sigma over i0-4 .. i0+35, j0-1 .. j0+8 (box 40 x 10 x 3),
@@ -55,16 +56,23 @@ constexpr int kPhX = kTX + 1, kPhN = (kTX + 1) * (kTY + 1);
 constexpr unsigned kFBytes = 3 * kFR * kFW * 8;  // 8640
 constexpr unsigned kSBytes = 3 * kFR * kSW * 4;  // 4800
 constexpr unsigned kNBytes = kNR * kNW * 4;      // 1296
-constexpr unsigned kFOff = 0, kSOff = 8704, kNOff = 8704 + 4864, kSlot = 8704 + 4864 + 1408;  // 128-byte aligned
+// ring slots, 128-byte aligned: the fields of four planes (k-1, k, k+1 in use,
+// k+2 in flight), sigma of three (k, k+1, k+2) and the node weights of two
+// (k+1, k+2), so that four blocks fit on an SM
+constexpr unsigned kFSlot = 8704, kSSlot = 4864, kNSlot = 1408;
 constexpr int kWaitLimit = 1 << 22;
 static_assert(kTX * kTY == kThreads, "one thread per node column");
-static_assert(kSlot % 128 == 0 && kSOff % 128 == 0 && kNOff % 128 == 0, "tensor-copy destinations 128-byte aligned");
+static_assert(kFSlot % 128 == 0 && kSSlot % 128 == 0 && kNSlot % 128 == 0, "tensor-copy destinations 128-byte aligned");
+static_assert(kFSlot >= kFBytes && kSSlot >= kSBytes && kNSlot >= kNBytes, "slot sizes");
 
 struct TmaSmem {
-    alignas(128) unsigned char slot[4][kSlot];
+    alignas(128) unsigned char fld[4][kFSlot];
+    alignas(128) unsigned char sig[3][kSSlot];
+    alignas(128) unsigned char nod[2][kNSlot];
     float2 phi[2][kPhN];
     unsigned long long mbar[4];
 };
+__device__ __forceinline__ int mod3(int p) { return ((p % 3) + 3) % 3; }
 
 __device__ __forceinline__ unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void mbar_init(unsigned a, unsigned count)
@@ -116,11 +124,11 @@ __device__ __forceinline__ float2 tma_phi_node(const TmaSmem &sm, const Geo<floa
 {
     if (!(i >= 1 && i <= g.nx - 1 && j >= 1 && j <= g.ny - 1 && p >= 1 && p <= g.nz - 1)) return make_float2(0, 0);
     const int sp = p & 3, sz = (p - 1) & 3;
-    const float2 *F = reinterpret_cast<const float2 *>(sm.slot[sp] + kFOff);
-    const float2 *Fz = reinterpret_cast<const float2 *>(sm.slot[sz] + kFOff) + 2 * kFR * kFW;
-    const float *S = reinterpret_cast<const float *>(sm.slot[sp] + kSOff);
-    const float *Sz = reinterpret_cast<const float *>(sm.slot[sz] + kSOff) + 2 * kFR * kSW;
-    const float wn = reinterpret_cast<const float *>(sm.slot[sp] + kNOff)[nj * kNW + ni];
+    const float2 *F = reinterpret_cast<const float2 *>(sm.fld[sp]);
+    const float2 *Fz = reinterpret_cast<const float2 *>(sm.fld[sz]) + 2 * kFR * kFW;
+    const float *S = reinterpret_cast<const float *>(sm.sig[p % 3]);
+    const float *Sz = reinterpret_cast<const float *>(sm.sig[(p - 1) % 3]) + 2 * kFR * kSW;
+    const float wn = reinterpret_cast<const float *>(sm.nod[p & 1])[nj * kNW + ni];
     const int h = (nj + 1) * kFW + ni + 2, hs = (nj + 1) * kSW + ni + 4;
     const int cf = kFR * kFW, cs = kFR * kSW;
     const float dfa0 = dY * dZ, dfa1 = dX * dZ, dfa2 = dX * dY;
@@ -163,7 +171,7 @@ __device__ __forceinline__ bool tma_march(TmaSmem &sm, const TmaParams &tp, cons
     const int pxy = pl.Px * pl.Py, pc = pl.Pz * pxy;
     const int col = min(i, pl.Px - 1) + pl.Px * min(j, pl.Py - 1);  // (i, j) in a plane of the padded layout
     const bool issuer = threadIdx.x == 0;
-    const unsigned tx_bytes = kFBytes + kSBytes + (gd ? kNBytes : 0u);
+    const unsigned tx_bytes = kFBytes + kSBytes;
     // halo potentials: threads 0..31 the row j0 + 8, the next 9 the column i0 + 32
     const bool hasH = threadIdx.x < kTX + kTY + 1;
     const int hni = threadIdx.x < kTX ? threadIdx.x : kTX;
@@ -172,7 +180,7 @@ __device__ __forceinline__ bool tma_march(TmaSmem &sm, const TmaParams &tp, cons
     const float hdX = (hasH && hi <= g.nx) ? g.delX[hi] : 0.f, hdY = (hasH && hj <= g.ny) ? g.delY[hj] : 0.f;
 
     // tensor-copy destinations must be 128-byte aligned: refuse otherwise
-    if (smem_addr(sm.slot[0]) & 127u) {
+    if ((smem_addr(sm.fld[0]) | smem_addr(sm.sig[0]) | smem_addr(sm.nod[0])) & 127u) {
         if (issuer) atomicExch(err, 2);
         return false;
     }
@@ -182,14 +190,18 @@ __device__ __forceinline__ bool tma_march(TmaSmem &sm, const TmaParams &tp, cons
     }
     __syncthreads();
     unsigned phase = 0;
+    // the copies of plane p complete on the mbarrier of its field slot; the
+    // node weights of plane k0 - 1 are not needed (no potential is formed
+    // there) and would share a slot with plane k0 + 1
     auto issue = [&](int p) {
         if (!issuer) return;
         const int s = p & 3;
+        const bool node = gd && p >= k0;
         const unsigned mb = smem_addr(&sm.mbar[s]);
-        mbar_expect(mb, tx_bytes);
-        tma_load4(smem_addr(sm.slot[s] + kFOff), &tp.in, 2 * (i0 - 2), j0 - 1, p, 3 * r, mb);
-        tma_load4(smem_addr(sm.slot[s] + kSOff), &tp.sig, i0 - 4, j0 - 1, p, 0, mb);
-        if (gd) tma_load3(smem_addr(sm.slot[s] + kNOff), &tp.node, i0, j0, p, mb);
+        mbar_expect(mb, tx_bytes + (node ? kNBytes : 0u));
+        tma_load4(smem_addr(sm.fld[s]), &tp.in, 2 * (i0 - 2), j0 - 1, p, 3 * r, mb);
+        tma_load4(smem_addr(sm.sig[mod3(p)]), &tp.sig, i0 - 4, j0 - 1, p, 0, mb);
+        if (node) tma_load3(smem_addr(sm.nod[p & 1]), &tp.node, i0, j0, p, mb);
     };
     // returns false after setting err: the issuer then waits (bounded) for
     // the copies it still has in flight so that none lands after the exit
@@ -232,10 +244,10 @@ __device__ __forceinline__ bool tma_march(TmaSmem &sm, const TmaParams &tp, cons
         if (gd) phi_plane(k + 1);
         __syncthreads();
         if (live) {
-            const float2 *Fm = reinterpret_cast<const float2 *>(sm.slot[(k - 1) & 3] + kFOff);
-            const float2 *F0 = reinterpret_cast<const float2 *>(sm.slot[k & 3] + kFOff);
-            const float2 *Fp = reinterpret_cast<const float2 *>(sm.slot[(k + 1) & 3] + kFOff);
-            const float *S0 = reinterpret_cast<const float *>(sm.slot[k & 3] + kSOff);
+            const float2 *Fm = reinterpret_cast<const float2 *>(sm.fld[(k - 1) & 3]);
+            const float2 *F0 = reinterpret_cast<const float2 *>(sm.fld[k & 3]);
+            const float2 *Fp = reinterpret_cast<const float2 *>(sm.fld[(k + 1) & 3]);
+            const float *S0 = reinterpret_cast<const float *>(sm.sig[k % 3]);
             const float2 *Xm = Fm, *X0 = F0, *Xp = Fp;
             const float2 *Ym = Fm + cf, *Y0 = F0 + cf, *Yp = Fp + cf;
             const float2 *Zm = Fm + 2 * cf, *Z0 = F0 + 2 * cf;
@@ -335,7 +347,7 @@ __device__ __forceinline__ TmaSmem &tma_smem()
 }
 
 // start of a call: r = b - A x0, rt = r; |b|^2, |r|^2
-__global__ void __launch_bounds__(kThreads, 3) kct_init(const __grid_constant__ TmaParams tp, KArgs<float> a)
+__global__ void __launch_bounds__(kThreads, 4) kct_init(const __grid_constant__ TmaParams tp, KArgs<float> a)
 {
     const int r = blockIdx.y;
     if (!a.ost[r].active) return;
@@ -367,7 +379,7 @@ __global__ void __launch_bounds__(kThreads, 3) kct_init(const __grid_constant__ 
 
 // v = A ph ; rtv = rt . v ; alpha   (which = 0)
 // t = A sh ; ts = t . s, tt = t . t ; omega   (which = 1)
-__global__ void __launch_bounds__(kThreads, 3) kct_vt(const __grid_constant__ TmaParams tp, KArgs<float> a, int which)
+__global__ void __launch_bounds__(kThreads, 4) kct_vt(const __grid_constant__ TmaParams tp, KArgs<float> a, int which)
 {
     const int r = blockIdx.y;
     BicgState &st = a.st[r];
