@@ -237,6 +237,9 @@ __device__ __forceinline__ bool tma_march(TmaSmem &sm, const TmaParams &tp, cons
     issue(k0 + 1);
     if (!wait(k0 - 1, k0 + 1) || !wait(k0, k0 + 1)) return false;
     if (gd) phi_plane(k0);
+    // plane k0 + 2 goes into the sigma slot of plane k0 - 1 and the node slot
+    // of plane k0, which the potentials of plane k0 have just read
+    __syncthreads();
     for (int k = k0; k < k1; k++) {
         const int last = k + 2 <= k1 ? k + 2 : k + 1;
         if (k + 2 <= k1) issue(k + 2);
