@@ -12,6 +12,7 @@
 //             column with the area-averaged conductivity; one thread per
 //             column, tridiagonal elimination (the 1-D matrix is diagonally
 //             dominant, so no pivoting is needed);
+//   k_bc_coef the operator coefficients and right-hand side per unknown;
 //   k_bc2d    the 2-D TE system of SetupA_TE / FormAII / MulAibWithXb /
 //             Fwd2DsolveTE (WSfwd2Dmod.f90:32-127, 325-418; FwdTEmod.f90:
 //             104-157): (nh-1)(nz-1) interior nodes, bandwidth m = nz-1.  One
@@ -205,6 +206,26 @@ struct Op2d {
 };
 }  // namespace
 
+// Coefficients of the 2-D operators and right-hand sides of the slices of a
+// launch chunk, one thread per unknown: the diagonal, A(r, r+1), A(r, r+m)
+// and -A_ib x_b, so that the elimination reads them instead of forming them
+// on its critical path.
+__global__ void k_bc_coef(BcArgs a, int nslices)
+{
+    const int m = a.nz - 1, n = (a.nh - 1) * m;
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)nslices * n) return;
+    const int q = (int)(t / n), r = (int)(t % n), s = a.slice0 + q;
+    const Slice sl(a, s);
+    const Op2d op(a, sl);
+    const double2 *left = a.side + (size_t)s * 2 * (a.nz + 1), *right = left + (a.nz + 1);
+    const double2 *bottom = a.bottom + (size_t)s * (a.nh + 1);
+    a.cd[t] = op.diag(r);
+    a.czc[t] = op.zc(r);
+    a.cyc[t] = op.yc(r);
+    a.cb[t] = op.rhs(r, left, right, bottom);
+}
+
 // One block (32 x BY threads) per slice of the launch chunk.
 __global__ void __launch_bounds__(1024) k_bc2d(BcArgs a, int smem_window)
 {
@@ -220,6 +241,19 @@ __global__ void __launch_bounds__(1024) k_bc2d(BcArgs a, int smem_window)
     const double2 *left = a.side + (size_t)s * 2 * (a.nz + 1), *right = left + (a.nz + 1);
     const double2 *bottom = a.bottom + (size_t)s * (a.nh + 1);
     const int tx = threadIdx.x, ty = threadIdx.y, nt = blockDim.x * blockDim.y, tid = ty * blockDim.x + tx;
+    const double2 *cd = a.cd + (size_t)blockIdx.x * n, *cb = a.cb + (size_t)blockIdx.x * n;
+    const double *czc = a.czc + (size_t)blockIdx.x * n, *cyc = a.cyc + (size_t)blockIdx.x * n;
+    // A(r, c) of the slice from the coefficient arrays
+    auto at = [&](int r, int c) -> double2 {
+        if (r >= n || c >= n) return c2(0, 0);
+        const int d = c - r;
+        if (d == 0) return cd[r];
+        if (d == 1) return c2(czc[r], 0);
+        if (d == -1) return c2(czc[c], 0);
+        if (d == m) return c2(cyc[r], 0);
+        if (d == -m) return c2(cyc[c], 0);
+        return c2(0, 0);
+    };
 
     // boundary nodes of E0: side columns, 1 along the top; the bottom row stays zero
     for (int k = tid; k < a.nz; k += nt) {
@@ -231,13 +265,20 @@ __global__ void __launch_bounds__(1024) k_bc2d(BcArgs a, int smem_window)
     // window of step 0: rows and columns 0..m
     for (int q = tid; q < M * M; q += nt) {
         const int r = q / M, c = q % M;
-        W[r * M + c] = op.at(r, c);
+        W[r * M + c] = at(r, c);
     }
-    for (int r = tid; r < M; r += nt) rw[r] = op.rhs(r, left, right, bottom);
+    for (int r = tid; r < M; r += nt) rw[r] = r < n ? cb[r] : c2(0, 0);
     __syncthreads();
 
     for (int j = 0; j < n; j++) {
         const int s0 = j % M;
+        // the row and column rn = j + M that enter at the end of this step hold
+        // three nonzeros, A(rn, rn) and the symmetric pairs A(rn - 1, rn),
+        // A(rn - m, rn); their loads are issued here, ahead of their use
+        const int rn = j + M;
+        const bool newrow = rn < n;
+        const double2 nd = newrow ? cd[rn] : c2(0, 0), nb = newrow ? cb[rn] : c2(0, 0);
+        const double nz1 = newrow ? czc[rn - 1] : 0.0, nym = newrow ? cyc[rn - m] : 0.0;
         const double2 piv = W[s0 * M + s0];
         const double2 rp = cdv(c2(1.0, 0.0), piv);
         // rows j+a, columns j+b, a, b = 1..m
@@ -271,19 +312,19 @@ __global__ void __launch_bounds__(1024) k_bc2d(BcArgs a, int smem_window)
         }
         if (tid == 0) y[j] = rw[s0];
         __syncthreads();
-        // slot s0 now takes row j+M (columns j+1..j+M) and column j+M (rows j+1..j+M-1)
-        const int rn = j + M;
+        // slot s0 now takes row rn (columns j+1..j+M) and column rn (rows
+        // j+1..j+M-1): column j+1 = rn - m, column rn - 1 and the diagonal
         for (int bi = 1 + tid; bi <= M; bi += nt) {
             int cb = s0 + bi;
             if (cb >= M) cb -= M;
-            W[s0 * M + cb] = op.at(rn, j + bi);
+            W[s0 * M + cb] = bi == M ? nd : c2(bi == 1 ? nym : bi == M - 1 ? nz1 : 0.0, 0.0);
         }
         for (int ai = 1 + tid; ai < M; ai += nt) {
             int ra = s0 + ai;
             if (ra >= M) ra -= M;
-            W[ra * M + s0] = op.at(j + ai, rn);
+            W[ra * M + s0] = c2(ai == 1 ? nym : ai == M - 1 ? nz1 : 0.0, 0.0);
         }
-        if (tid == 0) rw[s0] = op.rhs(rn, left, right, bottom);
+        if (tid == 0) rw[s0] = nb;
         __syncthreads();
     }
 
@@ -317,6 +358,13 @@ size_t bc_smem_bytes(int nz, bool window_in_smem)
 {
     const size_t M = (size_t)nz;
     return (window_in_smem ? M * M + M : M) * sizeof(double2);
+}
+
+void launch_bc_coef(const BcArgs &a, int nslices, cudaStream_t s)
+{
+    g_launch_count.fetch_add(1, std::memory_order_relaxed);
+    const long long nt = (long long)nslices * (a.nh - 1) * (a.nz - 1);
+    k_bc_coef<<<(unsigned)((nt + 255) / 256), 256, 0, s>>>(a, nslices);
 }
 
 void launch_bc1d(const BcArgs &a, cudaStream_t s)
@@ -356,7 +404,10 @@ int Solver::compute_bc(int imode, double om, double *e0, bool device)
     int optin = 0;
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev_);
     const bool smem = bc_smem_bytes(nz, true) <= (size_t)optin;
-    const size_t per_slice = ((size_t)n * M + n + (smem ? 0 : (size_t)M * M)) * sizeof(double2);
+    // per slice: U rows (n x M), reduced right-hand side (n), diagonal (n),
+    // operator right-hand side (n), the two couplings (2n doubles = n double2),
+    // the window when it is not in shared memory (M x M)
+    const size_t per_slice = ((size_t)n * M + 4 * (size_t)n + (smem ? 0 : (size_t)M * M)) * sizeof(double2);
     const size_t cap = (size_t)8 << 30;
     const int chunk = (int)std::max<size_t>(1, std::min<size_t>(nslice, cap / per_slice));
     const size_t fixed = ((size_t)nslice * 2 * (nz + 1) + (size_t)nslice * 2 * nz + (size_t)nslice * (nh + 1));
@@ -383,6 +434,11 @@ int Solver::compute_bc(int imode, double om, double *e0, bool device)
     a.bottom = p; p += (size_t)nslice * (nh + 1);
     a.U = p; p += (size_t)chunk * n * M;
     a.y = p; p += (size_t)chunk * n;
+    a.cd = p; p += (size_t)chunk * n;
+    a.cb = p; p += (size_t)chunk * n;
+    a.czc = reinterpret_cast<double *>(p);
+    a.cyc = a.czc + (size_t)chunk * n;
+    p += (size_t)chunk * n;
     a.W = smem ? nullptr : p;
     a.e0 = device ? reinterpret_cast<double2 *>(e0) : bce_.as<double2>();
     int rc;
@@ -390,6 +446,7 @@ int Solver::compute_bc(int imode, double om, double *e0, bool device)
     launch_bc1d(a, stream_);
     for (int s0 = 0; s0 < nslice; s0 += chunk) {
         a.slice0 = s0;
+        launch_bc_coef(a, std::min(chunk, nslice - s0), stream_);
         if ((rc = check((cudaError_t)launch_bc2d(a, std::min(chunk, nslice - s0), smem, stream_), "mt3d_compute_bc")))
             return rc;
     }

@@ -150,11 +150,14 @@ struct BcArgs {
     double2 *cpr;      // [nslice][2][nz] elimination scratch of the side columns
     double2 *bottom;   // [nslice][nh+1] bottom node of each interior column
     double2 *U, *y;    // [chunk][n][nz], [chunk][n]: U rows and reduced right-hand side
+    double2 *cd, *cb;  // [chunk][n] operator diagonal and right-hand side
+    double *czc, *cyc; // [chunk][n] couplings A(r, r+1) and A(r, r+nz-1)
     double2 *W;        // [chunk][nz][nz] elimination window when it is not in shared memory
     double2 *e0;       // full edge vector (zeroed by the caller)
 };
 size_t bc_smem_bytes(int nz, bool window_in_smem);
 void launch_bc1d(const BcArgs &a, cudaStream_t s);
+void launch_bc_coef(const BcArgs &a, int nslices, cudaStream_t s);
 int launch_bc2d(const BcArgs &a, int nblocks, bool window_in_smem, cudaStream_t s);
 void launch_nodes_to_padded(const Geo<double> &g, const double *src, PadLayout pl, float *dst, cudaStream_t s);
 int stage_chunks(int nz, int tiles, int resident);
