@@ -122,6 +122,17 @@ int mt3d_set_control(mt3d_handle h, int IterPerDivCor, int MaxDivCor, int MaxIte
     return MT3D_OK;
 }
 
+int mt3d_set_restart(mt3d_handle h, int restart)
+{
+    if (!h) return MT3D_INVALID_ARGUMENT;
+    if (restart < 0) {
+        h->s.last_error = "mt3d_set_restart: restart length must be >= 0";
+        return MT3D_INVALID_ARGUMENT;
+    }
+    h->s.ctl.restart = restart;
+    return MT3D_OK;
+}
+
 int mt3d_set_formulation(mt3d_handle h, int formulation)
 {
     if (!h) return MT3D_INVALID_ARGUMENT;

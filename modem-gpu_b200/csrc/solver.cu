@@ -461,7 +461,7 @@ template <> KArgs<double> Solver::kargs<double>(int nrhs, int)
         a.gde = gde_.as<unsigned char>();
         a.gdn = gdn64_.as<double>();
         a.phi = w.phi64.as<double2>();
-        a.restart = 120;
+        a.restart = ctl.restart;
     }
     return a;
 }
@@ -508,7 +508,7 @@ template <> KArgs<float> Solver::kargs<float>(int nrhs, int)
         a.gde = gde_.as<unsigned char>();
         a.gdn = gdn32_.as<float>();
         a.phi = w.phi32.as<float2>();
-        a.restart = 120;
+        a.restart = ctl.restart;
     }
     return a;
 }

@@ -18,6 +18,7 @@ struct Control {
     int solver = 1;     // 1: BiCGStab (reference BICG) + diagonal; 2: Bi-CG/COCG + z-line
     int precision = 0;  // 0 FP64, 1 mixed
     int formulation = 0;  // 0 curl-curl + divergence correction (MF), 1 curl-curl + grad-div (SP2)
+    int restart = 120;    // grad-div formulation: BiCGStab restart length (cuBiCG's 120; 0 never)
 };
 
 struct Diag {

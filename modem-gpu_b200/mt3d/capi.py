@@ -24,7 +24,7 @@ FORM_CCDC, FORM_CCGD = 0, 1
 
 #: every symbol include/mt3d.h declares
 EXPORTS = ["mt3d_version", "mt3d_device_count", "mt3d_create", "mt3d_destroy", "mt3d_set_control", "mt3d_update_cond",
-           "mt3d_get_cond", "mt3d_compute_bc", "mt3d_compute_bc_device", "mt3d_update_freq", "mt3d_set_formulation", "mt3d_sizes", "mt3d_interior_index", "mt3d_mult_aii",
+           "mt3d_get_cond", "mt3d_compute_bc", "mt3d_compute_bc_device", "mt3d_update_freq", "mt3d_set_formulation", "mt3d_set_restart", "mt3d_sizes", "mt3d_interior_index", "mt3d_mult_aii",
            "mt3d_mult_aii_device_noalloc", "mt3d_bicg", "mt3d_fwdsolve",
            "mt3d_fwdsolve_batch", "mt3d_fwdsolve_batch_device", "mt3d_set_stream", "mt3d_profile",
            "mt3d_kernel_time", "mt3d_get_diag", "mt3d_get_batch_diag", "mt3d_pmult_t", "mt3d_impedance", "mt3d_impedance_device", "mt3d_lmult_t", "mt3d_lmult_t_device", "mt3d_write_soln", "mt3d_read_soln", "mt3d_read_soln_header", "mt3d_launch_counter", "mt3d_last_error"]
@@ -61,6 +61,7 @@ def load(path: str = LIB_PATH):
     L.mt3d_compute_bc_device.argtypes = [P, I, C.c_double, C.c_void_p]
     L.mt3d_update_freq.argtypes = [P, C.c_double]
     L.mt3d_set_formulation.argtypes = [P, I]
+    L.mt3d_set_restart.argtypes = [P, I]
     L.mt3d_sizes.argtypes = [P, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     L.mt3d_interior_index.argtypes = [P, C.POINTER(C.c_int32)]
     L.mt3d_mult_aii.argtypes = [P, I, D, D]
@@ -145,6 +146,9 @@ class Solver:
 
     def set_formulation(self, formulation):
         self._check(self.L.mt3d_set_formulation(self.h, int(formulation)))
+
+    def set_restart(self, restart):
+        self._check(self.L.mt3d_set_restart(self.h, int(restart)))
 
     def update_cond(self, m_earth, air_cond):
         m = np.ascontiguousarray(m_earth, np.float64)

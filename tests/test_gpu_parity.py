@@ -472,6 +472,27 @@ def test_ccgd_sources_match_sp2(gprob):
         assert relerr(eg[mask], er[mask]) < 1e-5
 
 
+def test_restart_length_gives_the_same_solution(gprob):
+    """The grad-div formulation without cuBiCG's 120-iteration restarts
+    (restart only at cycle starts) converges to the same field."""
+    g, m, omega, ref, s = gprob
+    oms = np.array([omega, omega])
+    bcs = np.stack([mbc.boundary_1d(m, omega, md) for md in (1, 2)])
+    s.set_control(IterPerDivCor=300, MaxDivCor=20, precision=capi.PREC_MIXED)
+    e120, st120, _ = s.fwdsolve_batch(oms, bc=bcs)
+    s.set_restart(0)
+    e0, st0, _ = s.fwdsolve_batch(oms, bc=bcs)
+    it0, rr0 = s.batch_diagnostics(2)
+    s.set_restart(120)
+    s.set_control(IterPerDivCor=120, MaxDivCor=20, precision=capi.PREC_FP64)
+    assert np.all(st120 == 0) and np.all(st0 == 0) and np.all(rr0 <= 1e-7)
+    mask = earth_mask(g, m)
+    for r in range(2):
+        assert relerr(e0[r][mask], e120[r][mask]) < 1e-5
+    with pytest.raises(capi.MT3DError):
+        s.set_restart(-1)
+
+
 def test_mixed_cycles_fall_back_to_fp64(gprob):
     """Mixed precision with short (8-iteration) FP32 cycles, which do not
     always halve the FP64 residual, so right-hand sides may continue with FP64
