@@ -98,6 +98,20 @@ def test_compute_bc_matches_oracle(prob, imode):
     assert np.max(np.abs(e - want)) < 1e-10 * np.max(np.abs(want))
 
 
+def test_compute_bc_device_matches_host(prob):
+    """mt3d_compute_bc_device (explicit omega, device output) gives the same E0
+    as the host entry point at the handle's frequency."""
+    import torch
+    g, m, omega, o, s = prob
+    for imode in (1, 2):
+        out = torch.zeros(2 * s.nE, dtype=torch.float64, device="cuda")
+        s._check(s.L.mt3d_compute_bc_device(s.h, imode, float(omega), capi.C.c_void_p(out.data_ptr())))
+        torch.cuda.synchronize()
+        assert np.array_equal(out.cpu().numpy().view(np.complex128), s.compute_bc(imode))
+    with pytest.raises(capi.MT3DError):
+        s._check(s.L.mt3d_compute_bc_device(s.h, 3, float(omega), capi.C.c_void_p(out.data_ptr())))
+
+
 def test_compute_bc_tall_slices(cuda):
     """72 vertical cells: the elimination window (72 x 72 complex, 81 KB) takes
     the opted-in shared memory and 32 x 32 threads."""
