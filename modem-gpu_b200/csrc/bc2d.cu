@@ -20,8 +20,8 @@
 //             right-hand side carried along.  The active (m+1) x (m+1) window
 //             lives in shared memory as a circular buffer; each step writes
 //             the finished row of U out and loads the one new row and column
-//             of A, which no earlier step has touched.  One warp then
-//             back-substitutes.  The matrix is column diagonally dominant
+//             of A, which no earlier step has touched;
+//   k_bc_back the back substitution, one warp per slice.  The matrix is column diagonally dominant
 //             (the off-diagonal entries are real and sum to minus the real
 //             part of the diagonal), so elimination without row exchanges is
 //             stable; the reference's LAPACK band LU agrees with it to
@@ -282,26 +282,67 @@ __global__ void __launch_bounds__(1024) k_bc2d(BcArgs a, int smem_window)
         const double2 piv = W[s0 * M + s0];
         const double2 rp = cdv(c2(1.0, 0.0), piv);
         // rows j+a, columns j+b, a, b = 1..m
-        for (int ai = 1 + ty; ai <= m; ai += blockDim.y) {
-            int ra = s0 + ai;
-            if (ra >= M) ra -= M;
-            const double2 l = cm(W[ra * M + s0], rp);
-            if (l.x == 0.0 && l.y == 0.0) continue;
+        if (m <= 4 * (int)blockDim.y) {
+            // up to four rows per thread: their multipliers in registers, each
+            // entry of the pivot row read once per column
+            int ras[4];
+            double2 ls[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int ai = 1 + ty + q * blockDim.y;
+                int ra = s0 + ai;
+                if (ra >= M) ra -= M;
+                ras[q] = ra;
+                ls[q] = ai <= m ? cm(W[ra * M + s0], rp) : c2(0, 0);
+            }
             for (int bi = 1 + tx; bi <= m; bi += blockDim.x) {
                 int cb = s0 + bi;
                 if (cb >= M) cb -= M;
                 const double2 u = W[s0 * M + cb];
-                double2 w = W[ra * M + cb];
-                w.x -= l.x * u.x - l.y * u.y;
-                w.y -= l.x * u.y + l.y * u.x;
-                W[ra * M + cb] = w;
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    const double2 l = ls[q];
+                    if (l.x == 0.0 && l.y == 0.0) continue;
+                    double2 w = W[ras[q] * M + cb];
+                    w.x -= l.x * u.x - l.y * u.y;
+                    w.y -= l.x * u.y + l.y * u.x;
+                    W[ras[q] * M + cb] = w;
+                }
             }
             if (tx == 0) {
                 const double2 r0 = rw[s0];
-                double2 w = rw[ra];
-                w.x -= l.x * r0.x - l.y * r0.y;
-                w.y -= l.x * r0.y + l.y * r0.x;
-                rw[ra] = w;
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    const double2 l = ls[q];
+                    if (l.x == 0.0 && l.y == 0.0) continue;
+                    double2 w = rw[ras[q]];
+                    w.x -= l.x * r0.x - l.y * r0.y;
+                    w.y -= l.x * r0.y + l.y * r0.x;
+                    rw[ras[q]] = w;
+                }
+            }
+        } else {
+            for (int ai = 1 + ty; ai <= m; ai += blockDim.y) {
+                int ra = s0 + ai;
+                if (ra >= M) ra -= M;
+                const double2 l = cm(W[ra * M + s0], rp);
+                if (l.x == 0.0 && l.y == 0.0) continue;
+                for (int bi = 1 + tx; bi <= m; bi += blockDim.x) {
+                    int cb = s0 + bi;
+                    if (cb >= M) cb -= M;
+                    const double2 u = W[s0 * M + cb];
+                    double2 w = W[ra * M + cb];
+                    w.x -= l.x * u.x - l.y * u.y;
+                    w.y -= l.x * u.y + l.y * u.x;
+                    W[ra * M + cb] = w;
+                }
+                if (tx == 0) {
+                    const double2 r0 = rw[s0];
+                    double2 w = rw[ra];
+                    w.x -= l.x * r0.x - l.y * r0.y;
+                    w.y -= l.x * r0.y + l.y * r0.x;
+                    rw[ra] = w;
+                }
             }
         }
         // the finished row of U and of the reduced right-hand side
@@ -327,30 +368,68 @@ __global__ void __launch_bounds__(1024) k_bc2d(BcArgs a, int smem_window)
         if (tid == 0) rw[s0] = nb;
         __syncthreads();
     }
+}
 
-    // back substitution by warp 0: x_j = (y_j - sum_b U[j][b] x_{j+b}) / U[j][0]
-    if (ty == 0) {
-        double2 *xs = rw;  // circular buffer of the last M solution values
-        for (int j = n - 1; j >= 0; j--) {
-            double2 acc = c2(0, 0);
-            for (int bi = 1 + tx; bi <= m && j + bi < n; bi += 32) {
-                const double2 u = U[(size_t)j * M + bi];
-                const double2 xv = xs[(j + bi) % M];
-                acc.x += u.x * xv.x - u.y * xv.y;
-                acc.y += u.x * xv.y + u.y * xv.x;
-            }
-            for (int o = 16; o > 0; o >>= 1) {
-                acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
-                acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
-            }
-            const double2 xj = cdv(c2(y[j].x - acc.x, y[j].y - acc.y), U[(size_t)j * M]);
-            __syncwarp();
-            if (tx == 0) {
-                xs[j % M] = xj;
-                a.e0[sl.edge(j / m + 1, j % m + 1)] = xj;
-            }
-            __syncwarp();
+// Back substitution, one warp per slice: x_j = (y_j - sum_b U[j][b] x_{j+b}) /
+// U[j][0] from j = n-1 down.  Each lane holds up to kBackP entries of a U row
+// (columns lane + 32 p), and the row of step j - 1 is loaded while step j is
+// reduced, so the chain waits on shuffles and not on memory.  The last M
+// values of x live in shared memory as a circular buffer.
+constexpr int kBackP = 8;
+__global__ void __launch_bounds__(32) k_bc_back(BcArgs a)
+{
+    extern __shared__ double2 xs[];
+    const int q = blockIdx.x, s = a.slice0 + q;
+    const int m = a.nz - 1, n = (a.nh - 1) * m, M = a.nz;
+    const Slice sl(a, s);
+    const double2 *U = a.U + (size_t)q * n * M, *y = a.y + (size_t)q * n;
+    const int tx = threadIdx.x;
+    double2 u[kBackP], un[kBackP];
+    auto load = [&](int j, double2 *dst) {
+#pragma unroll
+        for (int p = 0; p < kBackP; p++) {
+            const int bi = tx + 32 * p;
+            dst[p] = bi < M ? U[(size_t)j * M + bi] : c2(0, 0);
         }
+    };
+    load(n - 1, u);
+    double2 yj = y[n - 1];
+    for (int j = n - 1; j >= 0; j--) {
+        double2 yn = c2(0, 0);
+        if (j > 0) {
+            load(j - 1, un);
+            yn = y[j - 1];
+        }
+        double2 acc = c2(0, 0);
+#pragma unroll
+        for (int p = 0; p < kBackP; p++) {
+            const int bi = tx + 32 * p;
+            if (bi >= 1 && bi < M && j + bi < n) {
+                const double2 xv = xs[(j + bi) % M];
+                acc.x += u[p].x * xv.x - u[p].y * xv.y;
+                acc.y += u[p].x * xv.y + u[p].y * xv.x;
+            }
+        }
+        for (int bi = tx + 32 * kBackP; bi < M && j + bi < n; bi += 32) {  // rows longer than 32 kBackP
+            const double2 uv = U[(size_t)j * M + bi], xv = xs[(j + bi) % M];
+            acc.x += uv.x * xv.x - uv.y * xv.y;
+            acc.y += uv.x * xv.y + uv.y * xv.x;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
+            acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
+        }
+        const double2 dg = c2(__shfl_sync(0xffffffffu, u[0].x, 0), __shfl_sync(0xffffffffu, u[0].y, 0));
+        const double2 xj = cdv(c2(yj.x - acc.x, yj.y - acc.y), dg);
+        __syncwarp();
+        if (tx == 0) {
+            xs[j % M] = xj;
+            a.e0[sl.edge(j / m + 1, j % m + 1)] = xj;
+        }
+        __syncwarp();
+#pragma unroll
+        for (int p = 0; p < kBackP; p++) u[p] = un[p];
+        yj = yn;
     }
 }
 
@@ -365,6 +444,14 @@ void launch_bc_coef(const BcArgs &a, int nslices, cudaStream_t s)
     g_launch_count.fetch_add(1, std::memory_order_relaxed);
     const long long nt = (long long)nslices * (a.nh - 1) * (a.nz - 1);
     k_bc_coef<<<(unsigned)((nt + 255) / 256), 256, 0, s>>>(a, nslices);
+}
+
+void launch_bc_back(const BcArgs &a, int nslices, cudaStream_t s)
+{
+    const size_t smem = (size_t)a.nz * sizeof(double2);
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k_bc_back, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    g_launch_count.fetch_add(1, std::memory_order_relaxed);
+    k_bc_back<<<nslices, 32, smem, s>>>(a);
 }
 
 void launch_bc1d(const BcArgs &a, cudaStream_t s)
@@ -449,6 +536,7 @@ int Solver::compute_bc(int imode, double om, double *e0, bool device)
         launch_bc_coef(a, std::min(chunk, nslice - s0), stream_);
         if ((rc = check((cudaError_t)launch_bc2d(a, std::min(chunk, nslice - s0), smem, stream_), "mt3d_compute_bc")))
             return rc;
+        launch_bc_back(a, std::min(chunk, nslice - s0), stream_);
     }
     if (!device &&
         (rc = check(cudaMemcpyAsync(e0, a.e0, nE * sizeof(double2), cudaMemcpyDeviceToHost, stream_), "copy E0")))

@@ -158,6 +158,7 @@ struct BcArgs {
 size_t bc_smem_bytes(int nz, bool window_in_smem);
 void launch_bc1d(const BcArgs &a, cudaStream_t s);
 void launch_bc_coef(const BcArgs &a, int nslices, cudaStream_t s);
+void launch_bc_back(const BcArgs &a, int nslices, cudaStream_t s);
 int launch_bc2d(const BcArgs &a, int nblocks, bool window_in_smem, cudaStream_t s);
 void launch_nodes_to_padded(const Geo<double> &g, const double *src, PadLayout pl, float *dst, cudaStream_t s);
 int stage_chunks(int nz, int tiles, int resident);
