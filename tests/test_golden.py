@@ -110,3 +110,17 @@ def test_gpu_reproduces_cylinder_fixture(cuda, formulation, solver, cycle, preci
     print("max", err.max(), "median", np.median(err))
     assert err.max() < 5e-4, err.max()
     assert np.median(err) < 1e-5
+
+
+def test_air_layers_match_the_reference_log():
+    """setup_airlayers 'fixed height 12 1000' on this model: the reference's
+    log of the cylinder test prints 'The top of the air layers is at
+    999.972 km' (unit_testing/3D/CylinderModel_FWD.out); the thicknesses grow
+    log-uniformly from the first earth layer."""
+    f = np.load(os.path.join(HERE, "golden", "cylinder_1per.npz"))
+    air = models.air_layers(f["dz_earth"], "fixed height", 12, 1000.0)
+    assert round(air.sum() / 1000, 3) == 999.972
+    ratios = air[:-1] / air[1:]
+    assert np.allclose(ratios, ratios[0], rtol=1e-9) and ratios[0] > 1
+    mirror = models.air_layers(f["dz_earth"], "mirror", 10, 3.0, 30.0)
+    assert np.isclose(mirror[-1], f["dz_earth"][0]) and np.isclose(mirror[-2], 3.0 * f["dz_earth"][1])
