@@ -98,6 +98,25 @@ def test_compute_bc_matches_oracle(prob, imode):
     assert np.max(np.abs(e - want)) < 1e-10 * np.max(np.abs(want))
 
 
+def test_compute_bc_window_in_global_memory(cuda):
+    """130 vertical cells: the elimination window (130 x 130 complex, 270 KB)
+    no longer fits in shared memory and lives in global memory, and the rows
+    exceed four per thread (the generic update loop)."""
+    from oracle import bc2d
+    g = models.make_grid(6, 7, 30, 100, core=500.0, n_pad=1, pad_growth=1.6, air_first=60.0, air_growth=1.12,
+                         earth_first=40.0, earth_growth=1.03)
+    m = random_model(g, seed=7)
+    omega = 2 * np.pi * 0.3
+    s = capi.Solver(g)
+    s.update_cond(m.m_earth, m.air_cond)
+    s.update_freq(omega)
+    sig = bc2d.sigma_cells(g, m.m_earth, m.air_cond)
+    for imode in (1, 2):
+        e = s.compute_bc(imode)
+        want = bc2d.compute_bc(g, sig, omega, imode)
+        assert np.max(np.abs(e - want)) < 1e-10 * np.max(np.abs(want))
+
+
 def test_compute_bc_device_matches_host(prob):
     """mt3d_compute_bc_device (explicit omega, device output) gives the same E0
     as the host entry point at the handle's frequency."""
