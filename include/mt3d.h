@@ -317,7 +317,9 @@ MT3D_API int mt3d_read_soln_header(const char *path, int *nTx, int *nPol, int *n
 
 MT3D_API int64_t mt3d_launch_counter(void);
 
-/* Message of the last error on the handle (NUL-terminated, truncated to len). */
+/* Message of the last error on the handle (NUL-terminated, truncated to len).
+ * With h = NULL: the last error of this thread's calls that take no handle
+ * (mt3d_create, mt3d_read_soln_header). */
 MT3D_API int mt3d_last_error(mt3d_handle h, char *buf, int len);
 
 #ifdef __cplusplus
