@@ -315,6 +315,8 @@ MT3D_API int mt3d_read_soln(mt3d_handle h, const char *path, int iTx, int iPol, 
 MT3D_API int mt3d_read_soln_header(const char *path, int *nTx, int *nPol, int *nx, int *ny, int *nz, int *nzAir,
                                    double *origin, double *rotdeg, double *dx, double *dy, double *dz);
 
+/* Number of kernel launches the library has issued in this process, over all
+ * handles (no counterpart in the reference; for launch accounting). */
 MT3D_API int64_t mt3d_launch_counter(void);
 
 /* Message of the last error on the handle (NUL-terminated, truncated to len).
