@@ -67,3 +67,28 @@ def test_library_writes_the_oracle_bytes_and_reads_them_back(cuda, tmp_path):
         other.read_soln(str(ref), 1, 1)
     with pytest.raises(capi.MT3DError):
         s.read_soln(str(ref), 3, 1)
+
+
+@pytest.mark.gpu
+def test_entry_points_reject_bad_arguments(cuda, tmp_path):
+    """Invalid arguments of the boundary, profiling and file entry points come
+    back as MT3D_INVALID_ARGUMENT with a message, not as a crash."""
+    import ctypes as C
+    g = small_grid()
+    s = capi.Solver(g)
+    m_earth = np.full(g.nx * g.ny * g.nzEarth, -np.log(100.0))
+    s.update_cond(m_earth, -23.0)
+    e = np.zeros(g.n_edges, np.complex128)
+    for imode, om in ((0, 1.0), (3, 1.0), (1, 0.0), (1, float("nan"))):
+        rc = s.L.mt3d_compute_bc_device(s.h, imode, om, e.ctypes.data_as(C.c_void_p))
+        assert rc == 5 and s._err(s.h)
+    n, ms, sw = C.c_int(), C.c_double(), C.c_int64()
+    assert s.L.mt3d_kernel_time(s.h, 2, C.byref(n), C.byref(ms), C.byref(sw)) == 5
+    with pytest.raises(capi.MT3DError):
+        s.write_soln(str(tmp_path / "x.soln"), [], np.zeros((0, 2, g.n_edges), np.complex128))
+    s.write_soln(str(tmp_path / "y.soln"), [1.0], np.zeros((1, 2, g.n_edges), np.complex128))
+    for itx, ipol in ((0, 1), (1, 0), (2, 1), (1, 3)):
+        with pytest.raises(capi.MT3DError):
+            s.read_soln(str(tmp_path / "y.soln"), itx, ipol)
+    with pytest.raises(capi.MT3DError):
+        s.read_soln(str(tmp_path / "missing.soln"), 1, 1)
