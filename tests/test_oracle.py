@@ -294,3 +294,22 @@ def test_bc2d_layered_slices_equal_the_1d_column():
         assert np.all(f[:, :, g.nz] == 0)  # bottom face zeroed
         other = e[nX:] if imode == 2 else np.concatenate([e[:nX], e[nX + nY:]])
         assert np.all(other == 0)
+
+
+def test_bc1d_halfspace_impedance():
+    """Fwd1D_TE restated (oracle/bc2d.py) against the halfspace's analytic
+    impedance: with E linear in the air, E / (dE/dz) at the surface times
+    omega is sqrt(omega / (mu0 sigma)) in magnitude with a 45 degree phase."""
+    from oracle import bc2d
+    nza = 6
+    air = 60.0 * 1.5 ** np.arange(nza)[::-1]
+    earth = 10.0 * 1.08 ** np.arange(90)
+    dz = np.concatenate([air, earth])
+    sigma, f = 0.01, 1.0
+    omega = 2 * np.pi * f
+    e = bc2d.fwd1d_te(omega, nza, dz, np.full(earth.size, sigma))
+    dedz = (e[nza] - e[nza - 1]) / dz[nza - 1]
+    z = -omega * e[nza] / dedz  # z down: E decays with depth
+    want = np.sqrt(omega / (bc2d.MU_0 * sigma))
+    assert abs(abs(z) / want - 1) < 0.01
+    assert abs(abs(np.degrees(np.angle(z))) - 45.0) < 1.0
