@@ -313,3 +313,25 @@ def test_bc1d_halfspace_impedance():
     want = np.sqrt(omega / (bc2d.MU_0 * sigma))
     assert abs(abs(z) / want - 1) < 0.01
     assert abs(abs(np.degrees(np.angle(z))) - 45.0) < 1.0
+
+
+def test_bc2d_contact_far_field_is_1d():
+    """A 2-D TE slice with a vertical contact (0.1 S/m | 0.01 S/m): columns
+    many skin depths away from the contact carry the 1-D solution of their own
+    side (within 1e-3 of the surface field)."""
+    from oracle import bc2d
+    nza = 6
+    dz = np.concatenate([60.0 * 1.5 ** np.arange(nza)[::-1], 20.0 * 1.12 ** np.arange(60)])
+    dy = np.full(60, 2000.0)
+    cond = np.empty((60, dz.size))
+    cond[:30] = 0.1
+    cond[30:] = 0.01
+    omega = 2 * np.pi * 1.0
+    e = bc2d.fwd2d_te(omega, nza, dy, dz, cond)
+    for col, s in ((5, 0.1), (55, 0.01)):
+        want = bc2d.fwd1d_te(omega, nza, dz, np.full(dz.size - nza, s))
+        assert np.max(np.abs(e[col] - want)) < 1e-3 * abs(want[nza])
+    # at the contact the field is neither side's 1-D one
+    for s in (0.1, 0.01):
+        want = bc2d.fwd1d_te(omega, nza, dz, np.full(dz.size - nza, s))
+        assert abs(e[30, nza] - want[nza]) > 0.05 * abs(want[nza])
