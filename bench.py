@@ -8,7 +8,9 @@ data) and adjoint (transposed) solves (synthetic receiver sources on a 20x20
 array) -- 64 right-hand sides.  One step solves 8 of them in one batched call
 of the C ABI: frequencies f and f+8 (f = step mod 8) x 2 polarisations x
 {forward, adjoint}, each to a relative residual of 1e-7 of the FP64 system;
-8 steps cover all 64.  The metric is solves/s over all ranks.
+8 steps cover all 64.  The metric is solves/s over all ranks.  The solver:
+curl-curl + grad-div, diagonal preconditioner, FP32 BiCGStab cycles of 300
+iterations (restarted only at cycle starts) under FP64 residual refinement.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--workload combined|precision|batch|small]
@@ -45,10 +47,9 @@ from mt3d import models  # noqa: E402
 
 METRIC = "fwd+adjoint solves/s, mixed-precision batched vs plain FP64 GPU at 1e-7 residual"
 TOL = 1e-7
-# refinement cycle: FP32 BiCGStab iterations between FP64 residual updates
-# (the shadow residual is still restarted every 120 iterations, as cuBiCG
-# does); shorter cycles stall the low-frequency forward solves of the
-# 200x200x100 model, 300 converges all 64 right-hand sides
+# refinement cycle: FP32 BiCGStab iterations between FP64 residual updates;
+# cycles of 40-120 stall the low-frequency forward solves of the 200x200x100
+# model, 300 converges all 64 right-hand sides
 CYCLE = 300
 # BiCGStab restarts only at cycle starts (each cycle begins from the true
 # residual); cuBiCG's 120-iteration restarts cost 14 % more iterations here
