@@ -5,8 +5,8 @@
  * The library replaces the solver calls of ModEM's 3D-MT forward problem:
  * the model-operator set-up (modelOperator3D), the Krylov call BICG/cuBiCG
  * and the driver FWDsolve3D with its divergence correction SdivCorr.  The
- * Fortran host keeps its types; a thin ISO_C_BINDING shim
- * flattens them with getCVector and calls the functions below.
+ * Fortran host keeps its types; a thin ISO_C_BINDING shim flattens them
+ * with getCVector and calls the functions below.
  *
  * Conventions
  *  - Complex arrays are interleaved (re, im) doubles, i.e. the memory layout
@@ -109,6 +109,18 @@ MT3D_API int mt3d_set_formulation(mt3d_handle h, int formulation);
  * 200 x 200 x 100 random-field benchmark 0 takes 14 % fewer iterations. */
 MT3D_API int mt3d_set_restart(mt3d_handle h, int restart);
 
+/* The FP32 iteration of the mixed-precision BiCGStab (MT3D_PREC_MIXED with
+ * MT3D_SOLVER_BICG).  on != 0 (default): the iteration runs in
+ * preconditioned variables (u = D^-1 p, D^-1 r, D^-1 v, ...) with the
+ * diagonal preconditioner fused into the operator kernels and a fixed
+ * pseudo-random shadow vector, 147 bytes of memory traffic per edge and
+ * iteration; 0: the kernels that keep the reference's variables (rt = r0,
+ * the preconditioned vectors formed in separate passes), 211 bytes.  Both
+ * are BiCGStab with the diagonal preconditioner of BICG
+ * (f90/3D_MT/FWD/solver.f90:346-555); they differ in the shadow vector and
+ * rounding.  No counterpart in the reference. */
+MT3D_API int mt3d_set_fused(mt3d_handle h, int on);
+
 /* Set the conductivity model (UpdateCond, f90/3D_MT/FWD/modelOperator3D.f90:
  * 211-232): ModelParamToEdge (LOGE, ModelMap.inc:88-188) and DivCorrSetUp. */
 MT3D_API int mt3d_update_cond(mt3d_handle h, const double *m_earth, double airCond);
@@ -156,8 +168,10 @@ MT3D_API int mt3d_interior_index(mt3d_handle h, int32_t *edgei);
 
 /* y = A x on interior vectors, A = V_E (curl curl + ISIGN i omega mu0 sigma)
  * (Mult_Aii, f90/3D_MT/FWD_SP2/modelOperator3D.f90:415-436; the same
- * operator as MultA_N, f90/3D_MT/FWD/modelOperator3D.f90:879-918).  With
- * adjt != 0 the conjugate-transposed operator is applied. */
+ * operator as MultA_N, f90/3D_MT/FWD/modelOperator3D.f90:879-918), plus the
+ * grad-div term in MT3D_FORM_CCGD.  With adjt != 0 the conjugate-transposed
+ * operator is applied: AAii^T x - i ISIGN VomegaMuSig x as Mult_Aii(adjt)
+ * forms it, including the transpose of the (unsymmetric) grad-div term. */
 MT3D_API int mt3d_mult_aii(mt3d_handle h, int adjt, const double *x, double *y);
 
 /* The product of mt3d_mult_aii on DEVICE vectors, allocating no device
@@ -173,11 +187,14 @@ MT3D_API int mt3d_mult_aii(mt3d_handle h, int adjt, const double *x, double *y);
  * this point.  The scratch (two full edge vectors, the grad-div node
  * potentials and a state record) is one fixed 16 MiB device array per
  * device: grids whose 256 + 16 * (2 nE + nN) bytes exceed it (about 52^3
- * cells) are rejected with MT3D_INVALID_ARGUMENT.  The first call on a
- * device looks up the scratch address (cudaGetSymbolAddress); make that first
- * call before any stream capture.  The scratch is shared by all handles on a
- * device, so calls whose GPU work overlaps in time (different streams,
- * handles or host threads) race; calls on one stream are safe. */
+ * cells) are rejected with MT3D_INVALID_ARGUMENT.  The first mt3d_create on
+ * a device looks up the scratch address (cudaGetSymbolAddress), which is
+ * what commits the array's 16 MiB, and loads the kernels of this entry, so
+ * this entry takes no device memory on any call; create the handle before a
+ * memory pool takes the device's free memory.  The scratch is shared by all
+ * handles on a device, so calls whose GPU work overlaps in time (different
+ * streams, handles or host threads) race; calls on one stream are safe.
+ * With adjt != 0 the product is the conjugate transpose, as mt3d_mult_aii's. */
 MT3D_API int mt3d_mult_aii_device_noalloc(mt3d_handle h, int adjt, const double *x, double *y);
 
 /* One Krylov call on the interior system A x = b: BICG(b, x, KSSiter,
@@ -224,6 +241,28 @@ MT3D_API int mt3d_fwdsolve_batch_device(mt3d_handle h, int nrhs, const double *o
 /* Run the handle's work on a caller-owned CUDA stream (a cudaStream_t passed
  * as void*); NULL restores the handle's own stream. */
 MT3D_API int mt3d_set_stream(mt3d_handle h, void *stream);
+
+/* Polls of one bounded device-side wait (the mbarrier waits of the FP32
+ * stencil kernels) before it gives up and the call returns
+ * MT3D_DEVICE_TIMEOUT; default 4194304.  0 makes every such wait give up at
+ * once (the copies in flight are still waited for, under the default
+ * limit, before a block exits).  No counterpart in the reference: a small
+ * limit lets a caller check its handling of that status without any device
+ * fault. */
+MT3D_API int mt3d_set_wait_limit(mt3d_handle h, int polls);
+
+/* y = A x on FULL edge vectors in host memory through one of the library's
+ * internal operator kernels, for checking the kernels against each other and
+ * against an independent operator (no counterpart in the reference; the
+ * operator is the one of mt3d_mult_aii at the handle's formulation and
+ * frequency, boundary entries of y zero):
+ *   kernel 0  the FP64 edge-parallel apply behind mt3d_mult_aii;
+ *   kernel 1  the shared-memory staged FP64 stencil of the FP64 BiCGStab;
+ *   kernel 2  the TMA-staged FP32 stencil of the mixed-precision BiCGStab
+ *             on its padded layout (x is rounded to complex FP32 first);
+ *   kernel 3  the operator kernel of the fused FP32 iteration
+ *             (mt3d_set_fused): y = D^-1 A x, D = diag(A), x rounded to FP32. */
+MT3D_API int mt3d_apply_kernel(mt3d_handle h, int kernel, const double *x, double *y);
 
 /* Kernel timing: with enable != 0 every launch of the BiCGStab stencil
  * kernels (v = A ph with the fused dot product) is bracketed by CUDA events
@@ -289,7 +328,6 @@ MT3D_API int mt3d_lmult_t_device(mt3d_handle h, double omega, int nsite, const d
                                  const double *e1_dev, const double *e2_dev, const double *d, double *s1_dev,
                                  double *s2_dev);
 
-/* Number of kernels the library has launched in this process (all handles). */
 /* E-field solution files in the reference's binary layout (write_solnVectorMTX
  * / read_solnVectorMTX, f90/3D_MT/ioMod/ioAscii.f90:493-597, with
  * FileWriteInit :188-215, FileReadInit f90/3D_MT/ioMod/ioBinary.f90:61-93,
@@ -315,9 +353,38 @@ MT3D_API int mt3d_read_soln(mt3d_handle h, const char *path, int iTx, int iPol, 
 MT3D_API int mt3d_read_soln_header(const char *path, int *nTx, int *nPol, int *nx, int *ny, int *nz, int *nzAir,
                                    double *origin, double *rotdeg, double *dx, double *dy, double *dz);
 
+/* J^T d for one transmitter (one frequency, both polarisations) and the
+ * Full_Impedance functional: JmultT_TX (f90/SENS/SensComp.f90:408-488) from
+ * saved background fields, i.e. LmultT (as mt3d_lmult_t) of the data weights
+ * d at the sites, the transposed solves of both polarisations (sensSolve with
+ * TRN; as mt3d_fwdsolve_batch with trans = 1, zero first guess, under the
+ * handle's control) and PmultT (as mt3d_pmult_t) at the background model
+ * m0_earth.  The impedance functional does not depend on the conductivity, so
+ * JmultT_TX's QmultT term is zero.  e0 holds the background fields of
+ * polarisations 1 and 2 (two full edge vectors) at angular frequency omega;
+ * xyz, origin and d are as for mt3d_lmult_t.  dm receives nx*ny*nzEarth
+ * values (the real part, as JmultT_TX keeps); eadj (two full edge vectors,
+ * may be NULL) the adjoint fields.  Returns MT3D_NOT_CONVERGED (with dm
+ * formed from the best iterates) when a transposed solve reached its limits.
+ * The misfit gradient of an inversion (gradient, f90/INV/INVcore.f90:141-206)
+ * is -2/Ndata times the sum over transmitters of J^T applied to the
+ * error-weighted residuals (d - dHat)/err^2. */
+MT3D_API int mt3d_jmult_t(mt3d_handle h, double omega, int nsite, const double *xyz, const double *origin,
+                          const double *e0, const double *d, const double *m0_earth, double *dm, double *eadj);
+/* As mt3d_jmult_t with e0, dm and eadj in device memory of the handle's
+ * device (xyz, origin, d and m0_earth on the host). */
+MT3D_API int mt3d_jmult_t_device(mt3d_handle h, double omega, int nsite, const double *xyz, const double *origin,
+                                 const double *e0_dev, const double *d, const double *m0_earth, double *dm_dev,
+                                 double *eadj_dev);
+
 /* Number of kernel launches the library has issued in this process, over all
  * handles (no counterpart in the reference; for launch accounting). */
 MT3D_API int64_t mt3d_launch_counter(void);
+
+/* Number of device allocations (cudaMalloc) the library has made in this
+ * process, over all handles (no counterpart in the reference; for checking
+ * which calls allocate). */
+MT3D_API int64_t mt3d_alloc_counter(void);
 
 /* Message of the last error on the handle (NUL-terminated, truncated to len).
  * With h = NULL: the last error of this thread's calls that take no handle

@@ -11,6 +11,7 @@
 
 namespace mt3d {
 extern std::atomic<long long> g_launch_count;
+extern std::atomic<long long> g_alloc_count;
 }
 
 struct mt3d_solver {
@@ -50,7 +51,11 @@ template <typename F> int wrap(mt3d_handle h, F &&f)
 
 extern "C" {
 
-const char *mt3d_version(void) { return "mt3d-b200 0.1 (sm_100a)"; }
+#ifndef MT3D_SRC_HASH
+#define MT3D_SRC_HASH "unknown"
+#endif
+// the source hash of build.py follows "mt3d-src-"
+const char *mt3d_version(void) { return "mt3d-b200 0.2 (sm_100a) mt3d-src-" MT3D_SRC_HASH; }
 
 int mt3d_device_count(void)
 {
@@ -261,6 +266,36 @@ int mt3d_set_stream(mt3d_handle h, void *stream)
     return wrap(h, [&] { return h->s.set_stream(stream); });
 }
 
+int mt3d_jmult_t(mt3d_handle h, double omega, int nsite, const double *xyz, const double *origin, const double *e0,
+                 const double *d, const double *m0_earth, double *dm, double *eadj)
+{
+    return wrap(h, [&] { return h->s.jmult_t(omega, nsite, xyz, origin, e0, d, m0_earth, dm, eadj, false); });
+}
+
+int mt3d_jmult_t_device(mt3d_handle h, double omega, int nsite, const double *xyz, const double *origin,
+                        const double *e0_dev, const double *d, const double *m0_earth, double *dm_dev,
+                        double *eadj_dev)
+{
+    return wrap(h, [&] {
+        return h->s.jmult_t(omega, nsite, xyz, origin, e0_dev, d, m0_earth, dm_dev, eadj_dev, true);
+    });
+}
+
+int mt3d_set_fused(mt3d_handle h, int on)
+{
+    return wrap(h, [&] { return h->s.set_fused(on); });
+}
+
+int mt3d_set_wait_limit(mt3d_handle h, int polls)
+{
+    return wrap(h, [&] { return h->s.set_wait_limit(polls); });
+}
+
+int mt3d_apply_kernel(mt3d_handle h, int kernel, const double *x, double *y)
+{
+    return wrap(h, [&] { return h->s.apply_kernel(kernel, x, y); });
+}
+
 int mt3d_profile(mt3d_handle h, int enable)
 {
     return wrap(h, [&] { return h->s.profile(enable); });
@@ -310,6 +345,8 @@ int mt3d_pmult_t(mt3d_handle h, int npol, const double *e0, const double *eadj, 
 }
 
 int64_t mt3d_launch_counter(void) { return mt3d::g_launch_count.load(); }
+
+int64_t mt3d_alloc_counter(void) { return mt3d::g_alloc_count.load(); }
 
 int mt3d_write_soln(mt3d_handle h, const char *path, int nTx, int nPol, const double *omegas, const double *origin,
                     double rotdeg, const double *e, int device)

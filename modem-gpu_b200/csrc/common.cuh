@@ -213,6 +213,7 @@ enum KStatus : int { KS_IDLE = 0, KS_RUNNING = 1, KS_CONVERGED = 2, KS_BREAKDOWN
 struct BicgState {
     cd rho, rho1, alpha, omega, beta;
     double bnorm, btol, rnorm, rnormin;
+    double rn2;  // fused FP32 iteration: ||s - omega t||^2 from the inner products of t = A sh
     int iter;    // iterations completed in this call
     int maxit;
     int status;  // KStatus

@@ -1,0 +1,562 @@
+// hatkernels.cu -- the FP32 BiCGStab iteration of the mixed-precision solve
+// with the diagonal preconditioner fused into the operator kernels.
+//
+// BiCGStab right-preconditioned with D = diag(A) (BICG, f90/3D_MT/FWD/
+// solver.f90:346-555, as the unfused kernels run it) is carried in
+// preconditioned variables: u = D^-1 p, vh = D^-1 v, rh = D^-1 r,
+// sh = D^-1 s, th = D^-1 t.  Then every vector update is a plain axpy, the
+// preconditioner is one division at the output edge of the operator kernels
+// (vh = D^-1 A u, th = D^-1 A sh), and no vector of D^-1 exists:
+//
+//   kh_u     u  = rh + beta (u - omega vh)   (u = rh on the first iteration)
+//   kh_vt 0  vh = D^-1 A u,       (z, vh)                  -> alpha
+//   kh_s     sh = rh - alpha vh
+//   kh_vt 1  th = D^-1 A sh,      (t, s), (t, t), (s, s)   -> omega, ||r||
+//   kh_xr    x += alpha u + omega sh,  rh = sh - omega th,  (z, rh) -> beta
+//
+// 147 bytes per edge and iteration instead of the 211 of the unfused
+// kernels (kb_p, kct_vt, kb_s, kct_vt, kb_xr).  The inner products of the
+// method in the original variables follow from the hat ones:
+//   - the shadow residual is rt = D^-H z, so (rt, r) = (z, rh) and
+//     (rt, v) = (z, vh); z is a fixed pseudo-random vector of entries
+//     +-1 +- i generated from the edge index, so it costs no memory traffic
+//     (any shadow with (rt, r0) != 0 is a valid BiCGStab shadow; a random one
+//     converges like rt = r0);
+//   - with W = |D|^2 per edge, computed in the operator kernel where D is,
+//     (t, s) = sum W conj(th) sh, (t, t) = sum W |th|^2, and the true
+//     residual norm of the new iterate follows without another pass:
+//     ||s - omega t||^2 = ||s||^2 - 2 Re(conj(omega) (t, s)) + |omega|^2 ||t||^2.
+// The iterates, step lengths and residual norms are those of the unfused
+// kernels up to the shadow vector and rounding.
+//
+// The operator kernels stage u or sh with the tensor copies of tma.cuh.  D =
+// V_E xXO-diagonal of the curl-curl term (col_ccdiag) + the grad-div diagonal
+// DFA^2 (w_s c_s + w_e c_e) + i omega mu0 sigma V_E, from the staged sigma
+// and signed node weights (the weights of the thread's three nodes at plane
+// k are kept in registers from the previous plane, so the node ring keeps
+// two slots).  kh_cast computes the same D from the global tables.
+#include <atomic>
+
+#include "finalize.cuh"
+#include "tma.cuh"
+
+namespace mt3d {
+
+extern std::atomic<long long> g_launch_count;
+static inline void counted(int n) { g_launch_count.fetch_add(n, std::memory_order_relaxed); }
+
+// shadow vector entry of padded index e: +-1 +- i from a 32-bit integer hash
+// (the "lowbias32" mixer of C. Wellons' hash-prospector)
+__device__ __forceinline__ float2 shadow_z(unsigned e)
+{
+    unsigned h = e;
+    h ^= h >> 16;
+    h *= 0x7feb352du;
+    h ^= h >> 15;
+    h *= 0x846ca68bu;
+    h ^= h >> 16;
+    return make_float2((h & 1u) ? 1.f : -1.f, (h & 2u) ? 1.f : -1.f);
+}
+
+// diagonal of A at an interior edge: dr + i di
+__device__ __forceinline__ void hat_diag(int comp, const ColGeo<float> &cg, const PlaneGeo<float> &pg, float wmu,
+                                         float sig, bool gd, float wns, float wne, float &dr, float &di)
+{
+    float ve, dfa;
+    if (comp == 0) {
+        ve = cg.dxi * (cg.delYj * pg.delZk);
+        dfa = cg.delYj * pg.delZk;
+    } else if (comp == 1) {
+        ve = cg.dyj * (cg.delXi * pg.delZk);
+        dfa = cg.delXi * pg.delZk;
+    } else {
+        ve = pg.dzk * (cg.delXi * cg.delYj);
+        dfa = cg.delXi * cg.delYj;
+    }
+    dr = col_ccdiag(comp, cg, pg);
+    if (gd) {
+        const float cs = wns < 0.f ? sig : 1.f, ce = wne < 0.f ? sig : 1.f;
+        dr += dfa * dfa * (fabsf(wns) * cs + fabsf(wne) * ce);
+    }
+    di = wmu * sig * ve;
+}
+
+// y / D and |D|^2
+__device__ __forceinline__ float2 hat_div(float2 y, float dr, float di, float &W)
+{
+    W = dr * dr + di * di;
+    const float inv = 1.f / W;
+    return make_float2((y.x * dr + y.y * di) * inv, (y.y * dr - y.x * di) * inv);
+}
+
+// ---------------------------------------------------------------------------
+// start of an FP32 cycle: rh = D^-1 b with b = r64 scale on the padded
+// layout, x = 0; ||b||^2 and rho = (z, rh).  The first guess is zero, so
+// r = b and no operator pass is needed.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads) kh_cast(KArgs<float> a, const double2 *r64, size_t stride64)
+{
+    const int r = blockIdx.y;
+    if (!a.ost[r].active) return;
+    const Geo<float> &g = a.g;
+    const size_t off = (size_t)r * stride64, offp = (size_t)r * a.stride;
+    const double sc = a.ost[r].scale;
+    const float wmu = (float)(a.dsgn * a.ost[r].omega * kMu0);
+    double u[3] = {0.0, 0.0, 0.0};
+    for (int e = blockIdx.x * kThreads + threadIdx.x; e < g.nE; e += gridDim.x * kThreads) {
+        const EdgeIdx q = edge_decode(g, e);
+        const int pe = a.pl.idx(q.c, q.i, q.j, q.k);
+        const double2 v = r64[off + e];
+        const float2 b = make_float2((float)(v.x * sc), (float)(v.y * sc));
+        float2 rh = make_float2(0.f, 0.f);
+        if (edge_interior(g, q)) {
+            const ColGeo<float> cg = col_geo(g, q.i, q.j);
+            const PlaneGeo<float> pg = plane_geo(g, q.k);
+            float wns = 0.f, wne = 0.f;
+            if (a.gd) {
+                const int ns = iN(g, q.i, q.j, q.k);
+                wns = a.gdn[ns];
+                wne = a.gdn[q.c == 0 ? ns + 1 : q.c == 1 ? ns + g.nx + 1 : ns + (g.nx + 1) * (g.ny + 1)];
+            }
+            float dr, di, W;
+            hat_diag(q.c, cg, pg, wmu, a.sigma[e], a.gd != 0, wns, wne, dr, di);
+            rh = hat_div(b, dr, di, W);
+            const float2 z = shadow_z((unsigned)pe);
+            u[0] += (double)b.x * b.x + (double)b.y * b.y;
+            u[1] += (double)z.x * rh.x + (double)z.y * rh.y;  // conj(z) rh
+            u[2] += (double)z.x * rh.y - (double)z.y * rh.x;
+        }
+        a.r[offp + pe] = rh;
+        a.x0[offp + pe] = make_float2(0.f, 0.f);
+    }
+    double tot[3];
+    if (block_reduce_last<3>(u, a.parts, a.cnt, r, blockIdx.x, gridDim.x, tot) && threadIdx.x == 0) {
+        const double t2[2] = {tot[0], tot[0]};
+        BicgState &st = a.st[r];
+        fin_init(st, t2, a.rerr + (size_t)r * a.rerr_stride, a.maxit, a.ost[r].tol_inner);
+        st.rho = {tot[1], tot[2]};
+        if (st.status == KS_RUNNING && cd_zero(st.rho)) st.status = KS_BREAKDOWN;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// elementwise kernels (two complex entries per thread and step)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float4 c2mul2(float2 c, float4 v)
+{
+    return make_float4(c.x * v.x - c.y * v.y, c.x * v.y + c.y * v.x, c.x * v.z - c.y * v.w, c.x * v.w + c.y * v.z);
+}
+__device__ __forceinline__ float4 add4(float4 a, float4 b) { return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w); }
+__device__ __forceinline__ float4 sub4(float4 a, float4 b) { return make_float4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w); }
+
+#define HAT_PAIRS(a)                                                                 \
+    const int n2 = (a).len / 2, c2 = (a).chunk / 2;                                  \
+    const int q1 = min((int)(blockIdx.x + 1) * c2, n2);                              \
+    for (int q = blockIdx.x * c2 + threadIdx.x; q < q1; q += kThreads)
+
+// u = rh + beta (u - omega vh); u = rh on the first iteration of a cycle or
+// after a restart
+__global__ void __launch_bounds__(kThreads) kh_u(KArgs<float> a)
+{
+    const int r = blockIdx.y;
+    const BicgState &st = a.st[r];
+    if (st.status != KS_RUNNING || !a.ost[r].active) return;
+    const size_t off = (size_t)r * a.stride / 2;
+    const float4 *RH = reinterpret_cast<const float4 *>(a.r) + off;
+    const float4 *VH = reinterpret_cast<const float4 *>(a.v) + off;
+    float4 *U = reinterpret_cast<float4 *>(a.ph) + off;
+    if (st.first) {
+        HAT_PAIRS(a) U[q] = RH[q];
+        return;
+    }
+    const float2 be = make_float2((float)st.beta.re, (float)st.beta.im);
+    const float2 om = make_float2((float)st.omega.re, (float)st.omega.im);
+    HAT_PAIRS(a) U[q] = add4(RH[q], c2mul2(be, sub4(U[q], c2mul2(om, VH[q]))));
+}
+
+// sh = rh - alpha vh
+__global__ void __launch_bounds__(kThreads) kh_s(KArgs<float> a)
+{
+    const int r = blockIdx.y;
+    const BicgState &st = a.st[r];
+    if (st.status != KS_RUNNING || !a.ost[r].active) return;
+    const size_t off = (size_t)r * a.stride / 2;
+    const float4 *RH = reinterpret_cast<const float4 *>(a.r) + off;
+    const float4 *VH = reinterpret_cast<const float4 *>(a.v) + off;
+    float4 *SH = reinterpret_cast<float4 *>(a.sh) + off;
+    const float2 al = make_float2((float)st.alpha.re, (float)st.alpha.im);
+    HAT_PAIRS(a) SH[q] = sub4(RH[q], c2mul2(al, VH[q]));
+}
+
+// x += alpha u + omega sh (into the buffer that does not hold the best
+// iterate); rh = sh - omega th; rho = (z, rh).  The true residual norm of the
+// new iterate comes from the inner products of kh_vt 1 (BicgState::rn2).
+__global__ void __launch_bounds__(kThreads) kh_xr(KArgs<float> a)
+{
+    const int r = blockIdx.y;
+    BicgState &st = a.st[r];
+    if (st.status != KS_RUNNING || !a.ost[r].active) return;
+    const size_t off = (size_t)r * a.stride / 2;
+    const float2 al = make_float2((float)st.alpha.re, (float)st.alpha.im);
+    const float2 om = make_float2((float)st.omega.re, (float)st.omega.im);
+    const int cur = st.xcur, dst = (st.xcur == st.xbest) ? 1 - st.xcur : st.xcur;
+    const float4 *XS = reinterpret_cast<const float4 *>(cur == 0 ? a.x0 : a.x1) + off;
+    float4 *XD = reinterpret_cast<float4 *>(dst == 0 ? a.x0 : a.x1) + off;
+    const float4 *U = reinterpret_cast<const float4 *>(a.ph) + off;
+    const float4 *SH = reinterpret_cast<const float4 *>(a.sh) + off;
+    const float4 *TH = reinterpret_cast<const float4 *>(a.t) + off;
+    float4 *RH = reinterpret_cast<float4 *>(a.r) + off;
+    double u[2] = {0.0, 0.0};
+    HAT_PAIRS(a)
+    {
+        const float4 sh = SH[q];
+        XD[q] = add4(add4(XS[q], c2mul2(al, U[q])), c2mul2(om, sh));
+        const float4 rn = sub4(sh, c2mul2(om, TH[q]));
+        RH[q] = rn;
+        const float2 z0 = shadow_z(2u * q), z1 = shadow_z(2u * q + 1u);
+        u[0] += (double)(z0.x * rn.x + z0.y * rn.y) + (double)(z1.x * rn.z + z1.y * rn.w);
+        u[1] += (double)(z0.x * rn.y - z0.y * rn.x) + (double)(z1.x * rn.w - z1.y * rn.z);
+    }
+    double tot[2];
+    if (block_reduce_last<2>(u, a.parts, a.cnt, r, blockIdx.x, gridDim.x, tot) && threadIdx.x == 0) {
+        double *rerr = a.rerr + (size_t)r * a.rerr_stride;
+        const double rnorm = sqrt(st.rn2);
+        st.iter += 1;
+        st.xcur = dst;
+        st.first = 0;
+        st.rnorm = rnorm;
+        rerr[st.iter - 1] = rnorm / st.bnorm;
+        if (!isfinite(rnorm) || !isfinite(tot[0]) || !isfinite(tot[1])) { st.status = KS_NAN; return; }
+        if (rnorm < st.btol) {
+            st.status = KS_CONVERGED;
+            st.xbest = dst;
+            return;
+        }
+        if (rnorm < st.rnormin) {
+            st.rnormin = rnorm;
+            st.xbest = dst;
+            st.imin = st.iter;
+        }
+        if (st.iter >= st.maxit) {
+            st.status = KS_MAXIT;
+            return;
+        }
+        const cd rho_new = {tot[0], tot[1]};
+        if (a.restart > 0 && st.iter % a.restart == 0) {
+            // restart towards steepest descent: p = r, omega = 1 (the shadow
+            // vector is kept)
+            st.first = 1;
+            st.rho = rho_new;
+            st.omega = {1.0, 0.0};
+            if (cd_zero(st.rho)) st.status = KS_BREAKDOWN;
+            return;
+        }
+        st.rho1 = st.rho;
+        st.rho = rho_new;
+        if (cd_zero(st.rho)) { st.status = KS_BREAKDOWN; return; }
+        st.beta = cd_mul(cd_div(st.rho, st.rho1), cd_div(st.alpha, st.omega));
+        if (cd_zero(st.beta)) st.status = KS_BREAKDOWN;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// the operator kernels: the staged stencil of tmakernels.cu with the output
+// divided by D at the edge
+// ---------------------------------------------------------------------------
+
+// March planes [k0, k1) of tile (i0, j0), right-hand side r, calling
+// f(e, interior, yhat, x_e, W) for every existing edge of the thread's node
+// column: yhat = D^-1 (A x)_e and W = |D_e|^2 at interior edges (zero
+// otherwise), e the padded index.  Returns false (all threads of the block
+// alike) when a wait gave up.
+template <typename F>
+__device__ __forceinline__ bool hat_march(TmaSmem &sm, const TmaParams &tp, const Geo<float> &g, PadLayout pl, int r,
+                                          bool gd, float wmu, int i0, int j0, int k0, int k1, int *err, int limit,
+                                          F &&f)
+{
+    const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
+    const int i = i0 + tx, j = j0 + ty;
+    const bool live = i <= g.nx && j <= g.ny;
+    const ColGeo<float> cg = col_geo(g, min(i, g.nx), min(j, g.ny));
+    const int hf = (ty + 1) * kFW + tx + 2;  // own column in a field plane of the tile
+    const int hs = (ty + 1) * kSW + tx + 4;  // own column in a sigma plane
+    const int hn = ty * kPhX + tx;           // own node in a potential plane
+    const int hw = ty * kNW + tx;            // own node in a node-weight plane
+    const int cf = kFR * kFW, cs = kFR * kSW;
+    const int pxy = pl.Px * pl.Py, pc = pl.Pz * pxy;
+    const int col = min(i, pl.Px - 1) + pl.Px * min(j, pl.Py - 1);
+    const bool issuer = threadIdx.x == 0;
+    const unsigned tx_bytes = kFBytes + kSBytes;
+    const bool hasH = threadIdx.x < kTX + kTY + 1;
+    const int hni = threadIdx.x < kTX ? threadIdx.x : kTX;
+    const int hnj = threadIdx.x < kTX ? kTY : threadIdx.x - kTX;
+    const int hi = i0 + hni, hj = j0 + hnj;
+    const float hdX = (hasH && hi <= g.nx) ? g.delX[hi] : 0.f, hdY = (hasH && hj <= g.ny) ? g.delY[hj] : 0.f;
+
+    if ((smem_addr(sm.fld[0]) | smem_addr(sm.sig[0]) | smem_addr(sm.nod[0])) & 127u) {
+        if (issuer) atomicExch(err, 2);
+        return false;
+    }
+    if (issuer) {
+        for (int q = 0; q < 4; q++) mbar_init(smem_addr(&sm.mbar[q]), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    __syncthreads();
+    unsigned phase = 0;
+    // node weights are staged for planes k0 .. k1 (the diagonal and the
+    // potentials need them), in slot p & 1
+    auto issue = [&](int p) {
+        if (!issuer) return;
+        const int s = p & 3;
+        const bool node = gd && p >= k0;
+        const unsigned mb = smem_addr(&sm.mbar[s]);
+        mbar_expect(mb, tx_bytes + (node ? kNBytes : 0u));
+        tma_load4(smem_addr(sm.fld[s]), &tp.in, 2 * (i0 - 2), j0 - 1, p, 3 * r, mb);
+        tma_load4(smem_addr(sm.sig[mod3(p)]), &tp.sig, i0 - 4, j0 - 1, p, 0, mb);
+        if (node) tma_load3(smem_addr(sm.nod[p & 1]), &tp.node, i0, j0, p, mb);
+    };
+    auto wait = [&](int p) -> bool {
+        const int s = p & 3;
+        if (mbar_wait(smem_addr(&sm.mbar[s]), (phase >> s) & 1u, limit)) {
+            phase ^= 1u << s;
+            return true;
+        }
+        return false;
+    };
+    auto give_up = [&](int first, int last) {
+        if (!issuer) return;
+        atomicExch(err, 1);
+        for (int q = first; q <= last; q++)
+            if (mbar_wait(smem_addr(&sm.mbar[q & 3]), (phase >> (q & 3)) & 1u, kWaitLimit)) phase ^= 1u << (q & 3);
+    };
+    auto phi_plane = [&](int p) {
+        const float dZ = (p >= 0 && p <= g.nz) ? g.delZ[p] : 0.f;
+        sm.phi[p & 1][hn] = tma_phi_node(sm, g, i, j, p, tx, ty, cg.delXi, cg.delYj, dZ);
+        if (hasH) sm.phi[p & 1][hnj * kPhX + hni] = tma_phi_node(sm, g, hi, hj, p, hni, hnj, hdX, hdY, dZ);
+    };
+    const float2 zero = make_float2(0.f, 0.f);
+    // signed node weights of the thread's nodes (i, j), (i+1, j), (i, j+1) at
+    // the plane being computed
+    float wS = 0.f, wX = 0.f, wY = 0.f;
+    auto node_w = [&](int p, float &s, float &x, float &y) {
+        const float *N = reinterpret_cast<const float *>(sm.nod[p & 1]);
+        s = N[hw];
+        x = N[hw + 1];
+        y = N[hw + kNW];
+    };
+
+    issue(k0 - 1);
+    issue(k0);
+    issue(k0 + 1);
+    {
+        const bool w0 = wait(k0 - 1), w1 = w0 && wait(k0);
+        if (w1 && gd) {
+            phi_plane(k0);
+            node_w(k0, wS, wX, wY);
+        }
+        if (!__syncthreads_and(w1)) {
+            give_up(w1 ? k0 + 1 : w0 ? k0 : k0 - 1, k0 + 1);
+            return false;
+        }
+    }
+    for (int k = k0; k < k1; k++) {
+        const int last = k + 2 <= k1 ? k + 2 : k + 1;
+        if (k + 2 <= k1) issue(k + 2);
+        const bool ok = wait(k + 1);
+        float nS = 0.f, nX = 0.f, nY = 0.f;  // plane k + 1
+        if (ok && gd) {
+            phi_plane(k + 1);
+            node_w(k + 1, nS, nX, nY);
+        }
+        if (!__syncthreads_and(ok)) {
+            give_up(ok ? k + 2 : k + 1, last);
+            return false;
+        }
+        if (live) {
+            const float2 *Fm = reinterpret_cast<const float2 *>(sm.fld[(k - 1) & 3]);
+            const float2 *F0 = reinterpret_cast<const float2 *>(sm.fld[k & 3]);
+            const float2 *Fp = reinterpret_cast<const float2 *>(sm.fld[(k + 1) & 3]);
+            const float *S0 = reinterpret_cast<const float *>(sm.sig[k % 3]);
+            const float2 *Xm = Fm, *X0 = F0, *Xp = Fp;
+            const float2 *Ym = Fm + cf, *Y0 = F0 + cf, *Yp = Fp + cf;
+            const float2 *Zm = Fm + 2 * cf, *Z0 = F0 + 2 * cf;
+            const float2 *P0 = sm.phi[k & 1], *P1 = sm.phi[(k + 1) & 1];
+            const PlaneGeo<float> pg = plane_geo(g, k);
+            const bool kin = k >= 1 && k <= g.nz - 1;
+            const int h = hf;
+            const int eb = col + pxy * k;
+            // ---- Ex(i, j, k)
+            if (cg.hasX) {
+                const float2 X1 = X0[h];
+                const float sg = S0[hs];
+                float2 out = zero;
+                float W = 0.f;
+                const bool in = cg.intX && kin;
+                if (in) {
+                    float dr, di;
+                    hat_diag(0, cg, pg, wmu, sg, gd, wS, wX, dr, di);
+                    const float2 yy = csub(cadd(csub(Y0[h + 1], Y0[h]), Y0[h - kFW]), Y0[h + 1 - kFW]);
+                    const float2 zz = csub(cadd(csub(Z0[h + 1], Z0[h]), Zm[h]), Zm[h + 1]);
+                    const float2 fyp = cscale(csub(X0[h + kFW], X1), cg.rdyj);
+                    const float2 fym = cscale(csub(X1, X0[h - kFW]), cg.rdyjm1);
+                    const float2 fzp = cscale(csub(Xp[h], X1), pg.rdzk);
+                    const float2 fzm = cscale(csub(X1, Xm[h]), pg.rdzkm1);
+                    out = cadd(cscale(yy, pg.delZk), cscale(zz, cg.delYj));
+                    out = csub(out, cscale(csub(fyp, fym), cg.dxi * pg.delZk));
+                    out = csub(out, cscale(csub(fzp, fzm), cg.dxi * cg.delYj));
+                    out.x -= di * X1.y;
+                    out.y += di * X1.x;
+                    if (gd) out = cadd(out, cscale(csub(P0[hn + 1], P0[hn]), cg.delYj * pg.delZk));
+                    out = hat_div(out, dr, di, W);
+                }
+                f(eb, in, out, X1, W);
+            }
+            // ---- Ey(i, j, k)
+            if (cg.hasY) {
+                const float2 Y1 = Y0[h];
+                const float sg = S0[cs + hs];
+                float2 out = zero;
+                float W = 0.f;
+                const bool in = cg.intY && kin;
+                if (in) {
+                    float dr, di;
+                    hat_diag(1, cg, pg, wmu, sg, gd, wS, wY, dr, di);
+                    const float2 zz = csub(cadd(csub(Z0[h + kFW], Z0[h]), Zm[h]), Zm[h + kFW]);
+                    const float2 xx = csub(cadd(csub(X0[h + kFW], X0[h]), X0[h - 1]), X0[h - 1 + kFW]);
+                    const float2 fzp = cscale(csub(Yp[h], Y1), pg.rdzk);
+                    const float2 fzm = cscale(csub(Y1, Ym[h]), pg.rdzkm1);
+                    const float2 fxp = cscale(csub(Y0[h + 1], Y1), cg.rdxi);
+                    const float2 fxm = cscale(csub(Y1, Y0[h - 1]), cg.rdxim1);
+                    out = cadd(cscale(zz, cg.delXi), cscale(xx, pg.delZk));
+                    out = csub(out, cscale(csub(fzp, fzm), cg.dyj * cg.delXi));
+                    out = csub(out, cscale(csub(fxp, fxm), cg.dyj * pg.delZk));
+                    out.x -= di * Y1.y;
+                    out.y += di * Y1.x;
+                    if (gd) out = cadd(out, cscale(csub(P0[hn + kPhX], P0[hn]), cg.delXi * pg.delZk));
+                    out = hat_div(out, dr, di, W);
+                }
+                f(pc + eb, in, out, Y1, W);
+            }
+            // ---- Ez(i, j, k)
+            if (k < g.nz) {
+                const float2 Z1 = Z0[h];
+                const float sg = S0[2 * cs + hs];
+                float2 out = zero;
+                float W = 0.f;
+                const bool in = cg.intZ;
+                if (in) {
+                    float dr, di;
+                    hat_diag(2, cg, pg, wmu, sg, gd, wS, nS, dr, di);
+                    const float2 xx = csub(cadd(csub(Xp[h], X0[h]), X0[h - 1]), Xp[h - 1]);
+                    const float2 yy = csub(cadd(csub(Yp[h], Y0[h]), Y0[h - kFW]), Yp[h - kFW]);
+                    const float2 fxp = cscale(csub(Z0[h + 1], Z1), cg.rdxi);
+                    const float2 fxm = cscale(csub(Z1, Z0[h - 1]), cg.rdxim1);
+                    const float2 fyp = cscale(csub(Z0[h + kFW], Z1), cg.rdyj);
+                    const float2 fym = cscale(csub(Z1, Z0[h - kFW]), cg.rdyjm1);
+                    out = cadd(cscale(xx, cg.delYj), cscale(yy, cg.delXi));
+                    out = csub(out, cscale(csub(fxp, fxm), pg.dzk * cg.delYj));
+                    out = csub(out, cscale(csub(fyp, fym), pg.dzk * cg.delXi));
+                    out.x -= di * Z1.y;
+                    out.y += di * Z1.x;
+                    if (gd) out = cadd(out, cscale(csub(P1[hn], P0[hn]), cg.delXi * cg.delYj));
+                    out = hat_div(out, dr, di, W);
+                }
+                f(2 * pc + eb, in, out, Z1, W);
+            }
+        }
+        wS = nS;
+        wX = nX;
+        wY = nY;
+        __syncthreads();
+    }
+    return true;
+}
+
+// vh = D^-1 A u, (z, vh) -> alpha   (which = 0)
+// th = D^-1 A sh, (t, s)_W, (t, t)_W, (s, s)_W -> omega, ||r_new||   (which = 1)
+__global__ void __launch_bounds__(kThreads, 4) kh_vt(const __grid_constant__ TmaParams tp, KArgs<float> a, int which)
+{
+    const int r = blockIdx.y;
+    BicgState &st = a.st[r];
+    if (st.status != KS_RUNNING || !a.ost[r].active) return;
+    if (a.sweeps && threadIdx.x == 0 && blockIdx.x == 0 && blockIdx.z == 0) atomicAdd(a.sweeps, 1ULL);
+    int i0, j0, k0, k1;
+    tma_tile(a.cmap, i0, j0);
+    tma_range(a.g.nz, k0, k1);
+    const size_t off = (size_t)r * a.stride;
+    float2 *out = (which ? a.t : a.v) + off;
+    double u[4] = {0.0, 0.0, 0.0, 0.0};
+    const bool ok = hat_march(tma_smem(), tp, a.g, a.pl, r, a.gd != 0, (float)(a.dsgn * a.ost[r].omega * kMu0), i0,
+                              j0, k0, k1, a.err, a.wait_limit, [&](int e, bool inn, float2 y, float2 x, float W) {
+                                  if (inn) {
+                                      if (which == 0) {
+                                          const float2 z = shadow_z((unsigned)e);
+                                          u[0] += (double)(z.x * y.x + z.y * y.y);  // conj(z) vh
+                                          u[1] += (double)(z.x * y.y - z.y * y.x);
+                                      } else {
+                                          u[0] += (double)(W * (y.x * x.x + y.y * x.y));  // conj(t) s
+                                          u[1] += (double)(W * (y.x * x.y - y.y * x.x));
+                                          u[2] += (double)(W * (y.x * y.x + y.y * y.y));
+                                          u[3] += (double)(W * (x.x * x.x + x.y * x.y));
+                                      }
+                                  }
+                                  out[e] = y;
+                              });
+    if (!ok) return;
+    double tot[4];
+    if (block_reduce_last<4>(u, a.parts, a.cnt, r, blockIdx.x + gridDim.x * blockIdx.z, gridDim.x * gridDim.z, tot) &&
+        threadIdx.x == 0) {
+        if (which == 0) {
+            fin_v(st, tot);
+        } else {
+            fin_t(st, tot);
+            if (st.status == KS_RUNNING) {
+                const cd ts = {tot[0], tot[1]}, om = st.omega;
+                const double rn2 = tot[3] - 2.0 * (om.re * ts.re + om.im * ts.im) + (om.re * om.re + om.im * om.im) * tot[2];
+                st.rn2 = rn2 > 0.0 ? rn2 : 0.0;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+static int hat_grid(long n) { return (int)std::min<long>((n + kThreads - 1) / kThreads, 148L * 16); }
+
+void launch_hat_cast(const KArgs<float> &a, const double2 *r64, size_t stride64, int nrhs, cudaStream_t s)
+{
+    counted(1);
+    kh_cast<<<dim3(hat_grid(a.g.nE), nrhs), kThreads, 0, s>>>(a, r64, stride64);
+}
+
+static void launch_hat_vt(const KArgs<float> &a, const TmaMaps *m, int which, int nrhs, cudaStream_t s)
+{
+    counted(1);
+    TmaParams tp;
+    tp.in = which ? m->sh : m->ph;
+    tp.sig = m->sig;
+    tp.node = m->node;
+    const size_t sm = sizeof(TmaSmem);
+    const int res = tma_resident(kh_vt, sm, 2);
+    kh_vt<<<dim3(a.cmap.tiles, nrhs, stage_chunks(a.g.nz, a.cmap.tiles, res)), kThreads, sm, s>>>(tp, a, which);
+}
+
+void launch_hat_iter(const KArgs<float> &a, int nrhs, cudaStream_t s, cudaEvent_t *ev)
+{
+    counted(3);
+    const dim3 grid(a.nblk, nrhs);
+    kh_u<<<grid, kThreads, 0, s>>>(a);
+    if (ev) cudaEventRecord(ev[0], s);
+    launch_hat_vt(a, a.tma, 0, nrhs, s);
+    if (ev) cudaEventRecord(ev[1], s);
+    kh_s<<<grid, kThreads, 0, s>>>(a);
+    if (ev) cudaEventRecord(ev[2], s);
+    launch_hat_vt(a, a.tma, 1, nrhs, s);
+    if (ev) cudaEventRecord(ev[3], s);
+    kh_xr<<<grid, kThreads, 0, s>>>(a);
+}
+
+void launch_hat_apply(const KArgs<float> &a, int nrhs, cudaStream_t s) { launch_hat_vt(a, a.tma, 0, nrhs, s); }
+
+}  // namespace mt3d

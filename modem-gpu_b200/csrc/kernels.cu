@@ -66,6 +66,17 @@ __device__ __forceinline__ C2<T> gd_edge(const Geo<T> &g, const EdgeIdx &q, cons
     edge_nodes(g, q, ns, ne);
     return cscale(csub(phi[ne], phi[ns]), dual_face_area(g, q));
 }
+// (GD^T x)_e from the potentials phi of mode 2 below: the transposed term
+// scales each node's potential by the edge's own c_en (GD_e'e = DFA_e' sum_n
+// G_e'n w_n G_en c_en DFA_e, so GD^T moves c_en to the outer side)
+template <typename T>
+__device__ __forceinline__ C2<T> gd_edge_t(const KArgs<T> &a, const EdgeIdx &q, T sig_e, const C2<T> *__restrict__ phi)
+{
+    int ns, ne;
+    edge_nodes(a.g, q, ns, ne);
+    const T cs = a.gde[ns] ? sig_e : T(1), ce = a.gde[ne] ? sig_e : T(1);
+    return cscale(csub(cscale(phi[ne], ce), cscale(phi[ns], cs)), dual_face_area(a.g, q));
+}
 // GD_ee (diagonal of the grad-div term)
 template <typename T>
 __device__ __forceinline__ T gd_diag(const KArgs<T> &a, const EdgeIdx &q, T sig_e)
@@ -79,13 +90,15 @@ __device__ __forceinline__ T gd_diag(const KArgs<T> &a, const EdgeIdx &q, T sig_
 
 // phi = W G^T (C DFA x) on interior nodes (mode 0: operator; mode 1: the
 // source-correction operator V_E GD2 of GradDivSetup2, earth nodes only and
-// c = 1).  For mode 1 the input is the source scaled per right-hand side by
-// 1 / (i ISIGN omega mu0), divided by V_E for transposed problems.
+// c = 1; mode 2: the potentials of the transposed operator, W G^T DFA x with
+// c = 1, which gd_edge_t completes).  For mode 1 the input is the source
+// scaled per right-hand side by 1 / (i ISIGN omega mu0), divided by V_E for
+// transposed problems.
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_gd_phi(KArgs<T> a, const C2<T> *x, C2<T> *phi, int mode)
 {
     const int r = blockIdx.y;
-    if (!a.ost[r].active && mode == 0) return;
+    if (!a.ost[r].active && mode != 1) return;
     const Geo<T> &g = a.g;
     const size_t eo = (size_t)r * a.stride, no = (size_t)r * g.nN;
     C2<T> scl = mk<T>(1, 0);
@@ -140,8 +153,9 @@ __global__ void __launch_bounds__(kThreads) k_gd_add(KArgs<T> a, C2<T> *b, const
 }
 
 // ---------------------------------------------------------------------------
-// operator apply: y = A x (interior; boundary of y set to zero).  Optional
-// mode 1: y = b - A x with reduction of |y|^2 into parts (no finalisation).
+// operator apply: y = A x (interior; boundary of y set to zero); neg != 0
+// negates.  use_gd = 1 adds the grad-div term GD x from the potentials in
+// a.phi (mode 0), use_gd = 2 its transpose GD^T x (potentials of mode 2).
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_apply(KArgs<T> a, const C2<T> *x, C2<T> *y, int neg, int use_gd)
@@ -155,8 +169,10 @@ __global__ void __launch_bounds__(kThreads) k_apply(KArgs<T> a, const C2<T> *x, 
         EdgeIdx q = edge_decode(g, e);
         C2<T> out = mk<T>(0, 0);
         if (edge_interior(g, q)) {
-            out = stencil(g, x + off, q, dterm_of(g, q, wmu, a.sigma[e]));
-            if (use_gd) out = cadd(out, gd_edge(g, q, a.phi + (size_t)r * g.nN));
+            const T sg = a.sigma[e];
+            out = stencil(g, x + off, q, dterm_of(g, q, wmu, sg));
+            if (use_gd == 1) out = cadd(out, gd_edge(g, q, a.phi + (size_t)r * g.nN));
+            if (use_gd == 2) out = cadd(out, gd_edge_t(a, q, sg, a.phi + (size_t)r * g.nN));
             if (neg) { out.x = -out.x; out.y = -out.y; }
         }
         y[off + e] = out;
@@ -1083,11 +1099,20 @@ __global__ void __launch_bounds__(kThreads) k_gather_interior(int nEi, const int
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
+cudaError_t preload_apply_kernels()
+{
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, k_apply<double>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_gd_phi<double>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_scatter_interior);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_gather_interior);
+    return e;
+}
 template <typename T>
 void launch_apply(const KArgs<T> &a, const C2<T> *x, C2<T> *y, int neg, int nrhs, cudaStream_t s, int use_gd)
 {
     counted(1);
-    if (use_gd) launch_gd_phi(a, x, a.phi, 0, nrhs, s);
+    if (use_gd) launch_gd_phi(a, x, a.phi, use_gd == 2 ? 2 : 0, nrhs, s);
     k_apply<T><<<dim3(a.nblk, nrhs), kThreads, 0, s>>>(a, x, y, neg, use_gd);
 }
 template <typename T> void launch_gd_phi(const KArgs<T> &a, const C2<T> *x, C2<T> *phi, int mode, int nrhs, cudaStream_t s)

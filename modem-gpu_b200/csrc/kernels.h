@@ -60,7 +60,8 @@ template <typename T> struct KArgs {
     int len;
     int padded;
     PadLayout pl;
-    int *err;  // set by a bounded device-side wait that gave up
+    int *err;        // set by a bounded device-side wait that gave up
+    int wait_limit;  // polls of one bounded wait before it gives up
     const struct TmaMaps *tma;  // host pointer: tensor maps of the padded vectors (colstencil == 3)
     // profiling: the staged stencil kernels count one sweep per active
     // right-hand side and launch here (nullptr when not profiling)
@@ -127,6 +128,10 @@ TmaMaps *tma_maps_new();
 void tma_maps_free(TmaMaps *m);
 void launch_tma_init(const KArgs<float> &a, const TmaMaps *m, int nrhs, cudaStream_t s);
 void launch_tma_vt(const KArgs<float> &a, const TmaMaps *m, int which, int nrhs, cudaStream_t s);
+// the fused FP32 BiCGStab iteration in preconditioned variables (hatkernels.cu)
+void launch_hat_cast(const KArgs<float> &a, const double2 *r64, size_t stride64, int nrhs, cudaStream_t s);
+void launch_hat_iter(const KArgs<float> &a, int nrhs, cudaStream_t s, cudaEvent_t *ev = nullptr);
+void launch_hat_apply(const KArgs<float> &a, int nrhs, cudaStream_t s);
 void launch_cast_padded(const Geo<double> &g, const OuterState *ost, size_t stride64, const double2 *r64,
                         PadLayout pl, float2 *b32, float2 *x32, int nrhs, cudaStream_t s);
 void launch_update_padded(const Geo<double> &g, const OuterState *ost, size_t stride64, PadLayout pl,
@@ -192,6 +197,8 @@ void launch_pmult_t(const Geo<double> &g, int npol, const double2 *e0, const dou
                     double *dm, cudaStream_t s);
 void launch_nonzero(const double2 *v, size_t stride, int n, int *flags, int nrhs, cudaStream_t s);
 void launch_scatter_interior(int nEi, const int *edgei, const double2 *vi, double2 *vf, cudaStream_t s);
+// load the modules of the FP64 operator-apply kernels (cudaFuncGetAttributes)
+cudaError_t preload_apply_kernels();
 void launch_gather_interior(int nEi, const int *edgei, const double2 *vf, double2 *vi, cudaStream_t s);
 
 }  // namespace mt3d

@@ -6,10 +6,13 @@
 //
 // The scratch is one array per device, shared by every handle on that
 // device.  Its address is looked up once per device (cudaGetSymbolAddress,
-// with that device current) on the first call; later calls only enqueue
-// work.  Two calls whose GPU work overlaps in time on one device (different
-// streams, handles or host threads) use the same scratch and race; calls
-// enqueued on one stream run one after the other and are safe.
+// with that device current) when mt3d_create makes the first handle there:
+// under CUDA's lazy module loading that look-up is what commits the array's
+// 16 MiB, and the kernels this entry launches are loaded at the same time, so
+// the entry itself takes no device memory, on its first call or later.  Two
+// calls whose GPU work overlaps in time on one device (different streams,
+// handles or host threads) use the same scratch and race; calls enqueued on
+// one stream run one after the other and are safe.
 #include <atomic>
 #include <cstdint>
 #include <cstdio>
@@ -64,6 +67,24 @@ __global__ void k_noalloc_state(OuterState *st, double omega)
     *st = s;
 }
 
+// set-up at handle creation, with device `dev` current: the scratch address
+// (committing the array) and the kernels of the entry (loading their modules)
+int noalloc_prepare(int dev, std::string &err)
+{
+    void *p = nullptr;
+    int rc = noalloc_scratch(dev, &p, err);
+    if (rc) return rc;
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, k_noalloc_state);
+    if (e == cudaSuccess) e = preload_apply_kernels();
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        err = std::string("loading the operator kernels failed: ") + cudaGetErrorString(e);
+        return 4;
+    }
+    return 0;
+}
+
 extern std::atomic<long long> g_launch_count;
 
 static bool device_vector(const void *p, int dev)
@@ -116,7 +137,7 @@ int Solver::mult_aii_noalloc(int adjt, const double *x, double *y)
     a.ost = st;
     a.phi = phi;
     a.dsgn = adjt ? 1.0 : -1.0;
-    launch_apply(a, xf, yf, 0, 1, stream_, gd);
+    launch_apply(a, xf, yf, 0, 1, stream_, gd ? (adjt ? 2 : 1) : 0);
     launch_gather_interior((int)nEi, edgei_d_.as<int>(), yf, reinterpret_cast<double2 *>(y), stream_);
     return check(cudaGetLastError(), who);
 }

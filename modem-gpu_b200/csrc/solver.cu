@@ -5,6 +5,7 @@
 // per-right-hand-side scalar state once per outer (divergence-correction)
 // cycle.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <limits>
 #include <cstdio>
@@ -14,11 +15,14 @@
 
 namespace mt3d {
 
+std::atomic<long long> g_alloc_count{0};
+
 int DevBuf::alloc(size_t bytes)
 {
     if (bytes <= bytes_ && ptr_) return 0;
     release();
     if (bytes == 0) return 0;
+    g_alloc_count.fetch_add(1, std::memory_order_relaxed);
     cudaError_t e = cudaMalloc(&ptr_, bytes);
     if (e != cudaSuccess) {
         ptr_ = nullptr;
@@ -47,6 +51,19 @@ int Solver::set_stream(void *s)
 {
     if (stream_) cudaStreamSynchronize(stream_);
     stream_ = s ? (cudaStream_t)s : own_stream_;
+    return 0;
+}
+
+int Solver::set_fused(int on)
+{
+    ctl.fused = on != 0;
+    return 0;
+}
+
+int Solver::set_wait_limit(int polls)
+{
+    if (polls < 0) return fail(5, "mt3d_set_wait_limit: the limit must not be negative");
+    wait_limit_ = polls;
     return 0;
 }
 
@@ -228,6 +245,8 @@ int Solver::create(int dev, int nx_, int ny_, int nz_, int nzAir_, const double 
     if ((rc = check(cudaMemcpy(edgei_d_.as<void>(), edgei.data(), edgei.size() * sizeof(int32_t), cudaMemcpyHostToDevice),
                     "copy edge list")))
         return rc;
+    std::string err;
+    if ((rc = noalloc_prepare(dev_, err))) return fail(rc, "mt3d_create: " + err);
     return 0;
 }
 
@@ -311,6 +330,9 @@ int Solver::check_device_error(const char *what)
     cudaMemcpy(&e, errf_.as<void>(), sizeof(int), cudaMemcpyDeviceToHost);
     if (!e) return 0;
     cudaMemset(errf_.as<void>(), 0, sizeof(int));
+    // the blocks that gave up skipped their reductions: clear the counters
+    // of the last-block detection for the next call
+    if (ws_.cnt.bytes()) cudaMemset(ws_.cnt.as<void>(), 0, ws_.cnt.bytes());
     return fail(6, std::string(what) + ": a bounded device-side wait gave up");
 }
 
@@ -485,6 +507,7 @@ template <> KArgs<float> Solver::kargs<float>(int nrhs, int)
     a.stride = nE;
     a.len = (int)nE;
     a.err = errf_.as<int>();
+    a.wait_limit = wait_limit_;
     if (w.padded) {
         // padded layout: the elementwise kernels sweep the padded length and
         // the stencil runs on the TMA-staged kernels
@@ -631,6 +654,20 @@ int Solver::run_bicg(int nrhs, int precision, int maxit)
     return check(cudaGetLastError(), "BiCG launch");
 }
 
+// one FP32 cycle of the fused BiCGStab (hatkernels.cu) on the normalised
+// FP64 residual in tmp: x = 0, rh = D^-1 b, maxit iterations; the returned
+// iterate ends in f_x0
+int Solver::run_hat(int nrhs, int maxit)
+{
+    prof_cur_ = 1;
+    KArgs<float> a = kargs<float>(nrhs, 1);
+    a.maxit = maxit;
+    launch_hat_cast(a, ws_.tmp.as<double2>(), nE, nrhs, stream_);
+    for (int it = 0; it < maxit; it++) launch_hat_iter(a, nrhs, stream_, next_events(4));
+    launch_bicg_finish(a, nrhs, stream_);
+    return check(cudaGetLastError(), "fused BiCGStab launch");
+}
+
 int Solver::run_divcorr(int nrhs)
 {
     DArgs a = dargs(nrhs);
@@ -660,10 +697,62 @@ int Solver::mult_aii(int adjt, const double *x, double *y)
     launch_scatter_interior((int)nEi, edgei_d_.as<int>(), xi, xf, stream_);
     KArgs<double> a = kargs<double>(1, 0);
     a.dsgn = adjt ? 1.0 : -1.0;
-    launch_apply(a, xf, yf, 0, 1, stream_, ctl.formulation == 1);
+    // grad-div formulation: the transposed product needs GD^T (GD is not symmetric)
+    launch_apply(a, xf, yf, 0, 1, stream_, ctl.formulation == 1 ? (adjt ? 2 : 1) : 0);
     launch_gather_interior((int)nEi, edgei_d_.as<int>(), yf, xi, stream_);
     cudaMemcpyAsync(y, xi, nEi * sizeof(double2), cudaMemcpyDeviceToHost, stream_);
     return sync("mt3d_mult_aii");
+}
+
+// ---------------------------------------------------------------------------
+// y = A x on full edge vectors through one internal operator kernel: 0 the
+// flat FP64 apply, 1 the staged FP64 BiCGStab stencil (kcs_vt), 2 the
+// TMA-staged FP32 BiCGStab stencil on the padded layout (kct_vt); 3: y =
+// D^-1 A x through the fused FP32 iteration's stencil (kh_vt)
+// ---------------------------------------------------------------------------
+int Solver::apply_kernel(int kernel, const double *x, double *y)
+{
+    const char *who = "mt3d_apply_kernel";
+    if (!cond_set) return fail(5, std::string(who) + ": conductivity not set (call mt3d_update_cond)");
+    if (!(omega > 0)) return fail(5, std::string(who) + ": frequency not set (call mt3d_update_freq)");
+    if (!x || !y || kernel < 0 || kernel > 3) return fail(5, std::string(who) + ": invalid arguments");
+    if (kernel >= 2 && ctl.solver != 1)
+        return fail(5, std::string(who) + ": the FP32 stencil belongs to the BiCGStab + diagonal solver");
+    int rc;
+    if ((rc = ensure_workspace(1, kernel >= 2 ? 1 : 0))) return rc;
+    Workspace &w = ws_;
+    OuterState os{};
+    os.omega = omega;
+    os.active = 1;
+    os.scale = 1.0;
+    BicgState bs{};
+    bs.status = KS_RUNNING;
+    cudaMemcpyAsync(w.ost.as<void>(), &os, sizeof os, cudaMemcpyHostToDevice, stream_);
+    cudaMemcpyAsync(w.bst.as<void>(), &bs, sizeof bs, cudaMemcpyHostToDevice, stream_);
+    double2 *X = w.tmp.as<double2>(), *Y = w.bc.as<double2>();
+    cudaMemcpyAsync(X, x, nE * sizeof(double2), cudaMemcpyHostToDevice, stream_);
+    if (kernel == 0) {
+        KArgs<double> a = kargs<double>(1, 0);
+        launch_apply(a, X, Y, 0, 1, stream_, ctl.formulation == 1);
+    } else if (kernel == 1) {
+        KArgs<double> a = kargs<double>(1, 0);
+        cudaMemcpyAsync(a.ph, X, nE * sizeof(double2), cudaMemcpyDeviceToDevice, stream_);
+        launch_stage_vt(a, 0, 1, stream_);
+        cudaMemcpyAsync(Y, a.v, nE * sizeof(double2), cudaMemcpyDeviceToDevice, stream_);
+    } else {
+        if ((rc = tma_ready())) return rc;
+        // x to FP32 on the padded layout (scale 1), through the stencil, back
+        launch_cast_padded(g64_, w.ost.as<OuterState>(), nE, X, pl_, w.f_ph.as<float2>(), w.f_x0.as<float2>(), 1,
+                           stream_);
+        KArgs<float> a = kargs<float>(1, 1);
+        if (kernel == 2) launch_tma_vt(a, tma_, 0, 1, stream_);
+        else launch_hat_apply(a, 1, stream_);
+        cudaMemsetAsync(Y, 0, nE * sizeof(double2), stream_);
+        launch_update_padded(g64_, w.ost.as<OuterState>(), nE, pl_, w.f_v.as<float2>(), Y, 1, stream_);
+    }
+    cudaMemcpyAsync(y, Y, nE * sizeof(double2), cudaMemcpyDeviceToHost, stream_);
+    if ((rc = sync(who))) return rc;
+    return check_device_error(who);
 }
 
 // ---------------------------------------------------------------------------
@@ -912,15 +1001,20 @@ int Solver::solve(int nrhs, const double *omegas, const int *trans, const double
                 for (int r = 0; r < nrhs; r++) grp[r].active = os[r].active && !hi[r];
                 cudaMemcpyAsync(w.ost.as<void>(), grp.data(), nrhs * sizeof(OuterState), cudaMemcpyHostToDevice,
                                 stream_);
-                if (w.padded) {
+                if (w.padded && ctl.fused) {
+                    // FP32 cycle in preconditioned variables from a zero first guess
+                    if ((rc = tma_ready())) return rc;
+                    if ((rc = run_hat(nrhs, ctl.IterPerDivCor))) return rc;
+                } else if (w.padded) {
                     if ((rc = tma_ready())) return rc;
                     launch_cast_padded(g64_, w.ost.as<OuterState>(), nE, w.tmp.as<double2>(), pl_, w.f_b.as<float2>(),
                                        w.f_x0.as<float2>(), nrhs, stream_);
+                    if ((rc = run_bicg(nrhs, 1, ctl.IterPerDivCor))) return rc;
                 } else {
                     launch_cast(w.ost.as<OuterState>(), (int)nE, nE, w.tmp.as<double2>(), w.f_b.as<float2>(),
                                 w.f_x0.as<float2>(), nrhs, stream_);
+                    if ((rc = run_bicg(nrhs, 1, ctl.IterPerDivCor))) return rc;
                 }
-                if ((rc = run_bicg(nrhs, 1, ctl.IterPerDivCor))) return rc;
                 if (w.padded)
                     launch_update_padded(g64_, w.ost.as<OuterState>(), nE, pl_, w.f_x0.as<float2>(), X, nrhs, stream_);
                 else

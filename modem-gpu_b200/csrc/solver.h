@@ -19,6 +19,7 @@ struct Control {
     int precision = 0;  // 0 FP64, 1 mixed
     int formulation = 0;  // 0 curl-curl + divergence correction (MF), 1 curl-curl + grad-div (SP2)
     int restart = 120;    // grad-div formulation: BiCGStab restart length (cuBiCG's 120; 0 never)
+    int fused = 1;        // mixed precision: FP32 iteration in preconditioned variables (hatkernels.cu)
 };
 
 struct Diag {
@@ -63,6 +64,10 @@ struct Workspace {
     DevBuf bst, pst, ost, parts, cnt, rerr, dcrerr;
 };
 
+// fixed scratch of mt3d_mult_aii_device_noalloc (noalloc.cu): resolved and
+// committed once per device at handle creation
+int noalloc_prepare(int dev, std::string &err);
+
 // header of a solution file (solnio.cu); any output may be NULL
 int read_soln_header(const char *path, int *nTx, int *nMode, int *nx, int *ny, int *nz, int *nzAir, double *origin,
                      double *rotdeg, double *dx, double *dy, double *dz, std::string &err);
@@ -75,10 +80,13 @@ class Solver {
     int update_freq(double omega);
     int mult_aii(int adjt, const double *x, double *y);
     int mult_aii_noalloc(int adjt, const double *x, double *y);  // device vectors, fixed scratch
+    int apply_kernel(int kernel, const double *x, double *y);   // one internal operator kernel
     int bicg(const double *b, double *x, int maxit, double tol, int *niter, double *rerr, int *failed);
     int solve(int nrhs, const double *omegas, const int *trans, const double *bc, const double *src, double *e,
               int *status, bool device = false);
     int set_stream(void *s);
+    int set_wait_limit(int polls);
+    int set_fused(int on);
     int profile(int enable);
     int kernel_time(int precision, int *launches, double *ms, int64_t *sweeps);
     int get_cond(double *sigma_e, double *divcorr, double *node_w);
@@ -91,6 +99,8 @@ class Solver {
                   double *Z, bool device);
     int lmult_t(double omega, int nsite, const double *xyz, const double *origin, const double *e1, const double *e2,
                 const double *d, double *s1, double *s2, bool device);
+    int jmult_t(double omega, int nsite, const double *xyz, const double *origin, const double *e0, const double *d,
+                const double *m0, double *dm, double *eadj, bool device);
     int data_functional(double omega, int nsite, const double *xyz, const double *origin, const double *e1,
                         const double *e2, const double *d, double *Z, double *s1, double *s2, bool device);
 
@@ -111,6 +121,7 @@ class Solver {
     int ensure_fp64_krylov(int nrhs);
     int run_bicg(int nrhs, int precision, int maxit);
     int run_divcorr(int nrhs);
+    int run_hat(int nrhs, int maxit);
     template <typename T> KArgs<T> kargs(int nrhs, int precision_ws);
     template <typename T> ColArgs<T> cargs();
     DArgs dargs(int nrhs);
@@ -142,6 +153,7 @@ class Solver {
     PadLayout pl_{};
     DevBuf sigP32_, sigsP32_, gdnP32_, errf_;
     TmaMaps *tma_ = nullptr;
+    int wait_limit_ = 1 << 22;  // polls of a bounded device-side wait
     bool tma_stale_ = true;
     int tma_ready();
     int check_device_error(const char *what);

@@ -16,149 +16,33 @@
 // plane k + 2 are issued before plane k is computed, so the threads only
 // wait for data and no longer spend instructions on moving it.
 //
-// Every wait on an mbarrier is bounded: after kWaitLimit polls the kernel
-// sets *err, lets the issuing thread wait (bounded again) for its copies in
-// flight, and returns; the host reports MT3D_DEVICE_TIMEOUT.
-#include <cuda.h>
-#include <cudaTypedefs.h>
-
+// Every wait on an mbarrier is bounded: a thread polls at most `limit` times
+// (KArgs::wait_limit).  The block then decides together, in the barrier that
+// follows every wait (__syncthreads_and), so either every thread goes on or
+// every thread leaves: on a timeout the issuing thread sets *err and waits
+// (bounded by kWaitLimit) for its copies still in flight, so none lands after
+// the block has exited, and the host reports MT3D_DEVICE_TIMEOUT.
 #include <algorithm>
 #include <atomic>
 #include <cstring>
 #include <mutex>
 
-#include "colstencil.cuh"
 #include "finalize.cuh"
-#include "kernels.h"
+#include "tma.cuh"
 
 namespace mt3d {
 
 extern std::atomic<long long> g_launch_count;
 static inline void counted(int n) { g_launch_count.fetch_add(n, std::memory_order_relaxed); }
 
-struct TmaMaps {
-    CUtensorMap x0, ph, sh;  // input vectors [nrhs][3][Pz][Py][2 Px] (float)
-    CUtensorMap sig;         // sigma [3][Pz][Py][Px] (float)
-    CUtensorMap node;        // signed node weights [Pz][Py][Px] (float)
-    int ok;
-};
-struct alignas(64) TmaParams {
-    CUtensorMap in, sig, node;
-};
-
-constexpr int kTX = 32, kTY = 8;
-constexpr int kFW = 36;   // field tile columns (float2): i0-2 .. i0+33
-constexpr int kSW = 40;   // sigma tile columns: i0-4 .. i0+35
-constexpr int kNW = 36;   // node tile columns: i0 .. i0+35
-constexpr int kFR = 10;   // field / sigma rows: j0-1 .. j0+8
-constexpr int kNR = 9;    // node rows: j0 .. j0+8
-constexpr int kPhX = kTX + 1, kPhN = (kTX + 1) * (kTY + 1);
-constexpr unsigned kFBytes = 3 * kFR * kFW * 8;  // 8640
-constexpr unsigned kSBytes = 3 * kFR * kSW * 4;  // 4800
-constexpr unsigned kNBytes = kNR * kNW * 4;      // 1296
-// ring slots, 128-byte aligned: the fields of four planes (k-1, k, k+1 in use,
-// k+2 in flight), sigma of three (k, k+1, k+2) and the node weights of two
-// (k+1, k+2), so that four blocks fit on an SM
-constexpr unsigned kFSlot = 8704, kSSlot = 4864, kNSlot = 1408;
-constexpr int kWaitLimit = 1 << 22;
-static_assert(kTX * kTY == kThreads, "one thread per node column");
-static_assert(kFSlot % 128 == 0 && kSSlot % 128 == 0 && kNSlot % 128 == 0, "tensor-copy destinations 128-byte aligned");
-static_assert(kFSlot >= kFBytes && kSSlot >= kSBytes && kNSlot >= kNBytes, "slot sizes");
-
-struct TmaSmem {
-    alignas(128) unsigned char fld[4][kFSlot];
-    alignas(128) unsigned char sig[3][kSSlot];
-    alignas(128) unsigned char nod[2][kNSlot];
-    float2 phi[2][kPhN];
-    unsigned long long mbar[4];
-};
-__device__ __forceinline__ int mod3(int p) { return ((p % 3) + 3) % 3; }
-
-__device__ __forceinline__ unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ void mbar_init(unsigned a, unsigned count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(a), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect(unsigned a, unsigned bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(a), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool mbar_try(unsigned a, unsigned parity)
-{
-    unsigned done;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(done)
-        : "r"(a), "r"(parity)
-        : "memory");
-    return done != 0;
-}
-__device__ __forceinline__ bool mbar_wait(unsigned a, unsigned parity)
-{
-    for (int it = 0; it < kWaitLimit; it++)
-        if (mbar_try(a, parity)) return true;
-    return false;
-}
-__device__ __forceinline__ void tma_load4(unsigned dst, const CUtensorMap *m, int c0, int c1, int c2, int c3,
-                                          unsigned mb)
-{
-    asm volatile(
-        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
-        "%5}], [%6];\n" ::"r"(dst),
-        "l"(m), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(mb)
-        : "memory");
-}
-__device__ __forceinline__ void tma_load3(unsigned dst, const CUtensorMap *m, int c0, int c1, int c2, unsigned mb)
-{
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
-        "[%5];\n" ::"r"(dst),
-        "l"(m), "r"(c0), "r"(c1), "r"(c2), "r"(mb)
-        : "memory");
-}
-
-// grad-div potential of node (ni, nj) of the tile (global i, j) at plane p:
-// the sums of k_gd_phi (mode 0) in the same order, from the staged planes
-__device__ __forceinline__ float2 tma_phi_node(const TmaSmem &sm, const Geo<float> &g, int i, int j, int p, int ni,
-                                               int nj, float dX, float dY, float dZ)
-{
-    if (!(i >= 1 && i <= g.nx - 1 && j >= 1 && j <= g.ny - 1 && p >= 1 && p <= g.nz - 1)) return make_float2(0, 0);
-    const int sp = p & 3, sz = (p - 1) & 3;
-    const float2 *F = reinterpret_cast<const float2 *>(sm.fld[sp]);
-    const float2 *Fz = reinterpret_cast<const float2 *>(sm.fld[sz]) + 2 * kFR * kFW;
-    const float *S = reinterpret_cast<const float *>(sm.sig[p % 3]);
-    const float *Sz = reinterpret_cast<const float *>(sm.sig[(p - 1) % 3]) + 2 * kFR * kSW;
-    const float wn = reinterpret_cast<const float *>(sm.nod[p & 1])[nj * kNW + ni];
-    const int h = (nj + 1) * kFW + ni + 2, hs = (nj + 1) * kSW + ni + 4;
-    const int cf = kFR * kFW, cs = kFR * kSW;
-    const float dfa0 = dY * dZ, dfa1 = dX * dZ, dfa2 = dX * dY;
-    float2 acc;
-    if (wn < 0.f) {  // earth node: C = sigma_E
-        acc = cscale(F[h - 1], dfa0 * S[hs - 1]);                       // Ex(i-1, j, p)
-        acc = csub(acc, cscale(F[h], dfa0 * S[hs]));                     // Ex(i, j, p)
-        acc = cadd(acc, cscale(F[cf + h - kFW], dfa1 * S[cs + hs - kSW]));  // Ey(i, j-1, p)
-        acc = csub(acc, cscale(F[cf + h], dfa1 * S[cs + hs]));           // Ey(i, j, p)
-        acc = cadd(acc, cscale(Fz[h], dfa2 * Sz[hs]));                   // Ez(i, j, p-1)
-        acc = csub(acc, cscale(F[2 * cf + h], dfa2 * S[2 * cs + hs]));   // Ez(i, j, p)
-        return cscale(acc, -wn);
-    }
-    acc = cscale(F[h - 1], dfa0);
-    acc = csub(acc, cscale(F[h], dfa0));
-    acc = cadd(acc, cscale(F[cf + h - kFW], dfa1));
-    acc = csub(acc, cscale(F[cf + h], dfa1));
-    acc = cadd(acc, cscale(Fz[h], dfa2));
-    acc = csub(acc, cscale(F[2 * cf + h], dfa2));
-    return cscale(acc, wn);
-}
-
 // March planes [k0, k1) of tile (i0, j0), right-hand side r (tensor
 // coordinate 3 r), calling f(comp, e, interior, Ax, x_e, aux_e) for every
 // existing edge of the thread's node column; e indexes the padded layout.
-// Returns false (all threads) when a wait gave up.
+// Returns false (all threads of the block alike) when a wait gave up.
 template <typename F>
 __device__ __forceinline__ bool tma_march(TmaSmem &sm, const TmaParams &tp, const Geo<float> &g, PadLayout pl,
                                           int r, const float2 *__restrict__ aux, bool gd, float wmu, int i0, int j0,
-                                          int k0, int k1, int *err, F &&f)
+                                          int k0, int k1, int *err, int limit, F &&f)
 {
     const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
     const int i = i0 + tx, j = j0 + ty;
@@ -203,18 +87,23 @@ __device__ __forceinline__ bool tma_march(TmaSmem &sm, const TmaParams &tp, cons
         tma_load4(smem_addr(sm.sig[mod3(p)]), &tp.sig, i0 - 4, j0 - 1, p, 0, mb);
         if (node) tma_load3(smem_addr(sm.nod[p & 1]), &tp.node, i0, j0, p, mb);
     };
-    // returns false after setting err: the issuer then waits (bounded) for
-    // the copies it still has in flight so that none lands after the exit
-    auto wait = [&](int p, int last_issued) -> bool {
+    // this thread's bounded wait for the copies of plane p
+    auto wait = [&](int p) -> bool {
         const int s = p & 3;
-        if (mbar_wait(smem_addr(&sm.mbar[s]), (phase >> s) & 1u)) {
+        if (mbar_wait(smem_addr(&sm.mbar[s]), (phase >> s) & 1u, limit)) {
             phase ^= 1u << s;
             return true;
         }
-        atomicExch(err, 1);
-        if (issuer)
-            for (int q = p + 1; q <= last_issued; q++) mbar_wait(smem_addr(&sm.mbar[q & 3]), ((phase >> (q & 3)) & 1u));
         return false;
+    };
+    // the block gave up: the issuer records it and waits (bounded) for its
+    // copies of planes first .. last, which no thread has seen complete, so
+    // that none lands in shared memory after the block has exited
+    auto give_up = [&](int first, int last) {
+        if (!issuer) return;
+        atomicExch(err, 1);
+        for (int q = first; q <= last; q++)
+            if (mbar_wait(smem_addr(&sm.mbar[q & 3]), (phase >> (q & 3)) & 1u, kWaitLimit)) phase ^= 1u << (q & 3);
     };
     auto phi_plane = [&](int p) {
         const float dZ = (p >= 0 && p <= g.nz) ? g.delZ[p] : 0.f;
@@ -235,17 +124,25 @@ __device__ __forceinline__ bool tma_march(TmaSmem &sm, const TmaParams &tp, cons
     issue(k0 - 1);
     issue(k0);
     issue(k0 + 1);
-    if (!wait(k0 - 1, k0 + 1) || !wait(k0, k0 + 1)) return false;
-    if (gd) phi_plane(k0);
-    // plane k0 + 2 goes into the sigma slot of plane k0 - 1 and the node slot
-    // of plane k0, which the potentials of plane k0 have just read
-    __syncthreads();
+    {
+        const bool w0 = wait(k0 - 1), w1 = w0 && wait(k0);
+        if (w1 && gd) phi_plane(k0);
+        // plane k0 + 2 goes into the sigma slot of plane k0 - 1 and the node
+        // slot of plane k0, which the potentials of plane k0 have just read
+        if (!__syncthreads_and(w1)) {
+            give_up(w1 ? k0 + 1 : w0 ? k0 : k0 - 1, k0 + 1);
+            return false;
+        }
+    }
     for (int k = k0; k < k1; k++) {
         const int last = k + 2 <= k1 ? k + 2 : k + 1;
         if (k + 2 <= k1) issue(k + 2);
-        if (!wait(k + 1, last)) return false;
-        if (gd) phi_plane(k + 1);
-        __syncthreads();
+        const bool ok = wait(k + 1);
+        if (ok && gd) phi_plane(k + 1);
+        if (!__syncthreads_and(ok)) {
+            give_up(ok ? k + 2 : k + 1, last);
+            return false;
+        }
         if (live) {
             const float2 *Fm = reinterpret_cast<const float2 *>(sm.fld[(k - 1) & 3]);
             const float2 *F0 = reinterpret_cast<const float2 *>(sm.fld[k & 3]);
@@ -332,23 +229,6 @@ __device__ __forceinline__ bool tma_march(TmaSmem &sm, const TmaParams &tp, cons
     return true;
 }
 
-__device__ __forceinline__ void tma_tile(const ColMap &m, int &i0, int &j0)
-{
-    i0 = (blockIdx.x % m.tiles_x) * kTX;
-    j0 = (blockIdx.x / m.tiles_x) * kTY;
-}
-__device__ __forceinline__ void tma_range(int nz, int &k0, int &k1)
-{
-    const int kc = (nz + 1 + gridDim.z - 1) / gridDim.z;
-    k0 = blockIdx.z * kc;
-    k1 = min(k0 + kc, nz + 1);
-}
-__device__ __forceinline__ TmaSmem &tma_smem()
-{
-    extern __shared__ __align__(128) unsigned char tma_raw[];
-    return *reinterpret_cast<TmaSmem *>(tma_raw);
-}
-
 // start of a call: r = b - A x0, rt = r; |b|^2, |r|^2
 __global__ void __launch_bounds__(kThreads, 4) kct_init(const __grid_constant__ TmaParams tp, KArgs<float> a)
 {
@@ -363,7 +243,7 @@ __global__ void __launch_bounds__(kThreads, 4) kct_init(const __grid_constant__ 
     float2 *R = a.r + off, *RT = a.rt + off;
     double u[2] = {0.0, 0.0};
     const bool ok = tma_march(tma_smem(), tp, a.g, a.pl, r, b, a.gd != 0, (float)(a.dsgn * a.ost[r].omega * kMu0),
-                              i0, j0, k0, k1, a.err, [&](int, int e, bool in, float2 ax, float2, float2 bb) {
+                              i0, j0, k0, k1, a.err, a.wait_limit, [&](int, int e, bool in, float2 ax, float2, float2 bb) {
                                   float2 res = make_float2(0.f, 0.f);
                                   if (in) {
                                       res = csub(bb, ax);
@@ -396,7 +276,7 @@ __global__ void __launch_bounds__(kThreads, 4) kct_vt(const __grid_constant__ Tm
     float2 *out = (which ? a.t : a.v) + off;
     double u[3] = {0.0, 0.0, 0.0};
     const bool ok = tma_march(tma_smem(), tp, a.g, a.pl, r, w, a.gd != 0, (float)(a.dsgn * a.ost[r].omega * kMu0),
-                              i0, j0, k0, k1, a.err, [&](int, int e, bool inn, float2 y, float2, float2 q) {
+                              i0, j0, k0, k1, a.err, a.wait_limit, [&](int, int e, bool inn, float2 y, float2, float2 q) {
                                   if (inn) {
                                       if (which == 0) {
                                           u[0] += (double)q.x * y.x + (double)q.y * y.y;  // conj(rt) v
@@ -477,26 +357,6 @@ int tma_maps_build(TmaMaps *m, const float2 *x0, const float2 *ph, const float2 
         return 1;
     m->ok = 1;
     return 0;
-}
-
-// the chunk count of stagekernels.cu, for the resident blocks of these kernels
-template <typename K> static int tma_resident(K kern, size_t smem, int slot)
-{
-    static std::mutex mu;
-    static int occ[64][4] = {};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev < 0 || dev >= 64) dev = 0;
-    std::lock_guard<std::mutex> lock(mu);
-    if (!occ[dev][slot]) {
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-        int n = 0, sms = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, kThreads, smem);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        occ[dev][slot] = std::max(1, n) * std::max(1, sms);
-    }
-    return occ[dev][slot];
 }
 
 void launch_tma_init(const KArgs<float> &a, const TmaMaps *m, int nrhs, cudaStream_t s)

@@ -26,8 +26,10 @@ FORM_CCDC, FORM_CCGD = 0, 1
 EXPORTS = ["mt3d_version", "mt3d_device_count", "mt3d_create", "mt3d_destroy", "mt3d_set_control", "mt3d_update_cond",
            "mt3d_get_cond", "mt3d_compute_bc", "mt3d_compute_bc_device", "mt3d_update_freq", "mt3d_set_formulation", "mt3d_set_restart", "mt3d_sizes", "mt3d_interior_index", "mt3d_mult_aii",
            "mt3d_mult_aii_device_noalloc", "mt3d_bicg", "mt3d_fwdsolve",
-           "mt3d_fwdsolve_batch", "mt3d_fwdsolve_batch_device", "mt3d_set_stream", "mt3d_profile",
-           "mt3d_kernel_time", "mt3d_get_diag", "mt3d_get_batch_diag", "mt3d_pmult_t", "mt3d_impedance", "mt3d_impedance_device", "mt3d_lmult_t", "mt3d_lmult_t_device", "mt3d_write_soln", "mt3d_read_soln", "mt3d_read_soln_header", "mt3d_launch_counter", "mt3d_last_error"]
+           "mt3d_fwdsolve_batch", "mt3d_fwdsolve_batch_device", "mt3d_set_stream", "mt3d_set_wait_limit", "mt3d_set_fused",
+           "mt3d_apply_kernel", "mt3d_profile",
+           "mt3d_kernel_time", "mt3d_get_diag", "mt3d_get_batch_diag", "mt3d_pmult_t", "mt3d_impedance", "mt3d_impedance_device", "mt3d_lmult_t", "mt3d_lmult_t_device", "mt3d_jmult_t", "mt3d_jmult_t_device", "mt3d_write_soln", "mt3d_read_soln", "mt3d_read_soln_header", "mt3d_launch_counter", "mt3d_alloc_counter",
+           "mt3d_last_error"]
 
 _lib = None
 
@@ -75,6 +77,11 @@ def load(path: str = LIB_PATH):
     L.mt3d_fwdsolve_batch.argtypes = [P, I, D, IP, D, D, D, IP]
     L.mt3d_fwdsolve_batch_device.argtypes = [P, I, D, IP, C.c_void_p, C.c_void_p, C.c_void_p, IP]
     L.mt3d_set_stream.argtypes = [P, C.c_void_p]
+    L.mt3d_set_wait_limit.argtypes = [P, I]
+    L.mt3d_set_fused.argtypes = [P, I]
+    L.mt3d_jmult_t.argtypes = [P, C.c_double, I, D, D, D, D, D, D, D]
+    L.mt3d_jmult_t_device.argtypes = [P, C.c_double, I, D, D, C.c_void_p, D, D, C.c_void_p, C.c_void_p]
+    L.mt3d_apply_kernel.argtypes = [P, I, D, D]
     L.mt3d_profile.argtypes = [P, I]
     L.mt3d_kernel_time.argtypes = [P, I, IP, D, C.POINTER(C.c_int64)]
     L.mt3d_get_diag.argtypes = [P, IP, IP, IP, D, I, D, I, D]
@@ -84,10 +91,11 @@ def load(path: str = LIB_PATH):
     L.mt3d_write_soln.argtypes = [P, C.c_char_p, I, I, D, D, C.c_double, C.c_void_p, I]
     L.mt3d_read_soln.argtypes = [P, C.c_char_p, I, I, D, C.c_void_p, I]
     L.mt3d_read_soln_header.argtypes = [C.c_char_p, IP, IP, IP, IP, IP, IP, D, D, D, D, D]
-    L.mt3d_launch_counter.restype = C.c_int64
-    L.mt3d_launch_counter.argtypes = []
+    for name in ("mt3d_launch_counter", "mt3d_alloc_counter"):
+        getattr(L, name).restype = C.c_int64
+        getattr(L, name).argtypes = []
     for name in EXPORTS:
-        if name not in ("mt3d_version", "mt3d_launch_counter"):
+        if name not in ("mt3d_version", "mt3d_launch_counter", "mt3d_alloc_counter"):
             getattr(L, name).restype = I
     _lib = L
     return L
@@ -254,6 +262,33 @@ class Solver:
         self._check(self.L.mt3d_lmult_t_device(self.h, float(omega), len(xyz), _d(xyz), _d(org), C.c_void_p(e1_ptr),
                                                C.c_void_p(e2_ptr), _d(dd), C.c_void_p(s1_ptr), C.c_void_p(s2_ptr)))
 
+    def jmult_t(self, omega, sites, e1, e2, d, m0_earth, origin=(0.0, 0.0, 0.0), want_eadj=False):
+        """J^T d of one frequency (JmultT_TX) from the background fields e1, e2
+        (host arrays) and data weights d [nsite, 2, 2]: returns (dm, status)
+        or (dm, eadj [2, nE], status)."""
+        xyz = np.ascontiguousarray(sites, np.float64).reshape(-1, 3)
+        org = np.ascontiguousarray(origin, np.float64)
+        dd = np.ascontiguousarray(d, np.complex128).reshape(-1)
+        e0 = np.ascontiguousarray(np.stack([np.asarray(e1), np.asarray(e2)]), np.complex128)
+        m0 = np.ascontiguousarray(m0_earth, np.float64)
+        g = self.grid
+        dm = np.zeros(g.nx * g.ny * g.nzEarth)
+        ea = np.zeros((2, self.nE), np.complex128) if want_eadj else None
+        rc = self._check(self.L.mt3d_jmult_t(self.h, float(omega), len(xyz), _d(xyz), _d(org), _d(e0), _d(dd),
+                                             _d(m0), _d(dm), _d(ea) if ea is not None else None), allow=(0, 1))
+        return (dm, ea, rc) if want_eadj else (dm, rc)
+
+    def jmult_t_device(self, omega, sites, e0_ptr, d, m0_earth, dm_ptr, eadj_ptr=None, origin=(0.0, 0.0, 0.0)):
+        """mt3d_jmult_t_device: e0_ptr (two full edge fields), dm_ptr and
+        eadj_ptr are device addresses."""
+        xyz = np.ascontiguousarray(sites, np.float64).reshape(-1, 3)
+        org = np.ascontiguousarray(origin, np.float64)
+        dd = np.ascontiguousarray(d, np.complex128).reshape(-1)
+        m0 = np.ascontiguousarray(m0_earth, np.float64)
+        return self._check(self.L.mt3d_jmult_t_device(self.h, float(omega), len(xyz), _d(xyz), _d(org),
+                                                      C.c_void_p(e0_ptr), _d(dd), _d(m0), C.c_void_p(dm_ptr),
+                                                      C.c_void_p(eadj_ptr) if eadj_ptr else None), allow=(0, 1))
+
     def bicg(self, b, x0, maxit, tol):
         b = np.ascontiguousarray(b, np.complex128)
         x = np.array(x0, np.complex128)
@@ -298,6 +333,21 @@ class Solver:
 
     def set_stream(self, stream_handle):
         self._check(self.L.mt3d_set_stream(self.h, stream_handle))
+
+    def set_fused(self, on: bool = True):
+        self._check(self.L.mt3d_set_fused(self.h, int(bool(on))))
+
+    def set_wait_limit(self, polls: int):
+        self._check(self.L.mt3d_set_wait_limit(self.h, int(polls)))
+
+    def apply_kernel(self, kernel: int, x: np.ndarray) -> np.ndarray:
+        """A x on full edge vectors through internal kernel 0 (FP64 apply),
+        1 (staged FP64 stencil) or 2 (TMA-staged FP32 stencil); D^-1 A x
+        through kernel 3 (the fused FP32 iteration's stencil)."""
+        x = np.ascontiguousarray(x, dtype=np.complex128)
+        y = np.zeros(self.nE, np.complex128)
+        self._check(self.L.mt3d_apply_kernel(self.h, int(kernel), _d(x), _d(y)))
+        return y
 
     def profile(self, enable=True):
         self._check(self.L.mt3d_profile(self.h, int(enable)))
