@@ -414,7 +414,30 @@ def main():
         d_e = torch.zeros((nmax, s.nE), dtype=torch.complex128, device=dev)
         solvers.append((s, batches, d_e, m))
 
+    multi = len(solvers) > 1
+    zchunks = None
+    if multi:
+        # models of uneven size in one call per step (mt3d_fwdsolve_multi);
+        # the per-grid stencil chunking tuned once and cached
+        from mt3d import tune
+        b0 = [batches[0] for _, batches, _, _ in solvers]
+        zchunks = tune.tune([s for s, *_ in solvers], [b[0] for b in b0],
+                            [d_e[:len(b[0])].data_ptr() for (_, _, d_e, _), b in zip(solvers, b0)],
+                            [b[1].data_ptr() for b in b0], [b[2].data_ptr() for b in b0], [b[3] for b in b0],
+                            lambda: torch.cuda.synchronize(dev),
+                            cache_path=os.environ.get("MT3D_TUNE_CACHE",
+                                                      os.path.join(tempfile.gettempdir(), "mt3d_tune.json")))
+
     def step(k):
+        if multi:
+            bs = [batches[k % len(batches)] for _, batches, _, _ in solvers]
+            es = [d_e[:len(b[0])] for (_, _, d_e, _), b in zip(solvers, bs)]
+            for e in es:
+                e.zero_()
+            capi.fwdsolve_multi([s for s, *_ in solvers], [b[0] for b in bs], [e.data_ptr() for e in es],
+                                trans=[b[3] for b in bs], bc=[b[1].data_ptr() for b in bs],
+                                src=[b[2].data_ptr() for b in bs], zchunks=zchunks, device=True)
+            return
         for s, batches, d_e, _ in solvers:
             om, d_bc, d_src, tr = batches[k % len(batches)]
             e = d_e[:len(om)]
@@ -508,7 +531,37 @@ def main():
 
     # end to end through the C ABI with pinned host buffers, copies inside the timed region
     e2e = None
-    if not args.no_e2e:
+    if not args.no_e2e and multi:
+        ke = min(args.steps, 2)
+        h2d = d2h = 0
+        pinned = []
+        for k in range(ke):
+            per = []
+            for s, batches, d_e, _ in solvers:
+                om, d_bc, d_src, tr = batches[k % len(batches)]
+                hb = torch.empty(tuple(d_bc.shape), dtype=torch.complex128).pin_memory()
+                hs_ = torch.empty_like(hb).pin_memory()
+                he = torch.empty_like(hb).pin_memory()
+                hb.copy_(d_bc.cpu())
+                hs_.copy_(d_src.cpu())
+                per.append((om, hb.numpy(), hs_.numpy(), he.numpy(), tr))
+            pinned.append(per)
+        barrier()
+        t0 = time.perf_counter()
+        for per in pinned:
+            for p in per:
+                p[3][:] = 0
+            capi.fwdsolve_multi([s for s, *_ in solvers], [p[0] for p in per], [p[3] for p in per],
+                                trans=[p[4] for p in per], bc=[p[1] for p in per], src=[p[2] for p in per],
+                                zchunks=zchunks)
+            h2d += sum(p[1].nbytes + p[2].nbytes + p[3].nbytes for p in per)
+            d2h += sum(p[3].nbytes for p in per)
+        barrier()
+        e2e_s = max_over_ranks(time.perf_counter() - t0)
+        e2e = {"value": world * sum(per_step[:ke]) / e2e_s, "unit": "solves/s", "steps": ke,
+               "h2d_bytes_per_step": h2d // ke, "d2h_bytes_per_step": d2h // ke, "entry": "mt3d_fwdsolve_multi"}
+        del pinned
+    elif not args.no_e2e:
         ke = min(args.steps, 2)
         pinned = []
         for s, batches, d_e, _ in solvers:
@@ -579,6 +632,9 @@ def main():
                 "iterations_per_solve": {"mean": float(its.mean()), "min": int(its.min()), "max": int(its.max())},
                 "fp64": fp64, "parity": parity, "e2e": e2e, "roofline": roofline, "cpu_baseline": cb, "clocks": ck,
                 "gpu_launches": launches}
+        if multi:
+            line["config"]["multi_grid"] = {"entry": "mt3d_fwdsolve_multi_device, one call per step",
+                                            "zchunks": zchunks}
         print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()

@@ -238,6 +238,30 @@ MT3D_API int mt3d_fwdsolve_batch(mt3d_handle h, int nrhs, const double *omegas, 
 MT3D_API int mt3d_fwdsolve_batch_device(mt3d_handle h, int nrhs, const double *omegas, const int *trans,
                                         const double *bc_dev, const double *src_dev, double *e_dev, int *status);
 
+/* FWDsolve3D over several grids at once: handle hs[i] (its own grid, model
+ * and control) solves nrhs[i] right-hand sides with omegas[i], trans[i],
+ * bc[i], src[i] and e[i] as mt3d_fwdsolve_batch takes them (bc, src, trans
+ * or any entry may be NULL), status[i] receives their statuses.  Replaces the
+ * reference's farm of (transmitter, polarisation) solves over MPI ranks
+ * (f90/MPI/Main_MPI.f90:1444-1649) for models of uneven size on one GPU:
+ * the handles' FWDsolve3D phases run in lockstep on the first handle's
+ * stream and the FP32 iterations of all grids share their launches (five per
+ * iteration for the whole batch).  Every handle must be on one device, in
+ * mixed precision with MT3D_SOLVER_BICG and the fused FP32 iteration
+ * (mt3d_set_fused), with the same IterPerDivCor; 1 to 8 handles.  zchunks
+ * (nh entries, may be NULL; 0 = the occupancy-based default) sets how many
+ * chunks of node planes each grid's stencil blocks split the column into --
+ * the knob mt3d/tune.py tunes.  Errors are reported by mt3d_last_error(NULL)
+ * and on hs[0].  No counterpart in the reference. */
+MT3D_API int mt3d_fwdsolve_multi(int nh, mt3d_handle *hs, const int *nrhs, const double *const *omegas,
+                                 const int *const *trans, const double *const *bc, const double *const *src,
+                                 double *const *e, int *const *status, const int *zchunks);
+/* As mt3d_fwdsolve_multi with bc, src and e in device memory. */
+MT3D_API int mt3d_fwdsolve_multi_device(int nh, mt3d_handle *hs, const int *nrhs, const double *const *omegas,
+                                        const int *const *trans, const double *const *bc_dev,
+                                        const double *const *src_dev, double *const *e_dev, int *const *status,
+                                        const int *zchunks);
+
 /* Run the handle's work on a caller-owned CUDA stream (a cudaStream_t passed
  * as void*); NULL restores the handle's own stream. */
 MT3D_API int mt3d_set_stream(mt3d_handle h, void *stream);

@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libmt3d.so")
-SOURCES = ["kernels.cu", "colkernels.cu", "stagekernels.cu", "tmakernels.cu", "hatkernels.cu", "setupkernels.cu", "bc2d.cu", "datafunc.cu", "solnio.cu", "solver.cu", "sens.cu",
+SOURCES = ["kernels.cu", "colkernels.cu", "stagekernels.cu", "tmakernels.cu", "hatkernels.cu", "setupkernels.cu", "bc2d.cu", "datafunc.cu", "solnio.cu", "solver.cu", "sens.cu", "multi.cu",
            "noalloc.cu", "capi.cu"]
 # the operator set-up reproduces the host's operation order bit for bit: no contraction to FMA
 FILE_FLAGS = {"setupkernels.cu": ["-fmad=false"]}

@@ -281,6 +281,55 @@ int mt3d_jmult_t_device(mt3d_handle h, double omega, int nsite, const double *xy
     });
 }
 
+static int fwdsolve_multi_entry(int nh, mt3d_handle *hs, const int *nrhs, const double *const *omegas,
+                                const int *const *trans, const double *const *bc, const double *const *src,
+                                double *const *e, int *const *status, const int *zchunks, bool device)
+{
+    if (nh < 1 || nh > 8 || !hs) {
+        g_create_error = "mt3d_fwdsolve_multi: 1 to 8 handles";
+        return MT3D_INVALID_ARGUMENT;
+    }
+    mt3d::Solver *ss[8];
+    for (int i = 0; i < nh; i++) {
+        if (!hs[i]) {
+            g_create_error = "mt3d_fwdsolve_multi: null handle";
+            return MT3D_INVALID_ARGUMENT;
+        }
+        ss[i] = &hs[i]->s;
+    }
+    const int rc0 = guard_device(hs[0]);
+    if (rc0) return rc0;
+    try {
+        std::string err;
+        const int rc = mt3d::fwdsolve_multi(nh, ss, nrhs, omegas, trans, bc, src, e, status, zchunks, device, err);
+        if (rc) {
+            g_create_error = err;
+            hs[0]->s.last_error = err;
+        }
+        return rc;
+    } catch (const std::bad_alloc &) {
+        g_create_error = "host out of memory";
+        return MT3D_OUT_OF_MEMORY;
+    } catch (...) {
+        g_create_error = "unexpected exception";
+        return MT3D_CUDA_ERROR;
+    }
+}
+
+int mt3d_fwdsolve_multi(int nh, mt3d_handle *hs, const int *nrhs, const double *const *omegas,
+                        const int *const *trans, const double *const *bc, const double *const *src, double *const *e,
+                        int *const *status, const int *zchunks)
+{
+    return fwdsolve_multi_entry(nh, hs, nrhs, omegas, trans, bc, src, e, status, zchunks, false);
+}
+
+int mt3d_fwdsolve_multi_device(int nh, mt3d_handle *hs, const int *nrhs, const double *const *omegas,
+                               const int *const *trans, const double *const *bc_dev, const double *const *src_dev,
+                               double *const *e_dev, int *const *status, const int *zchunks)
+{
+    return fwdsolve_multi_entry(nh, hs, nrhs, omegas, trans, bc_dev, src_dev, e_dev, status, zchunks, true);
+}
+
 int mt3d_set_fused(mt3d_handle h, int on)
 {
     return wrap(h, [&] { return h->s.set_fused(on); });

@@ -36,6 +36,7 @@
 // k are kept in registers from the previous plane, so the node ring keeps
 // two slots).  kh_cast computes the same D from the global tables.
 #include <atomic>
+#include <cstring>
 
 #include "finalize.cuh"
 #include "tma.cuh"
@@ -149,16 +150,16 @@ __device__ __forceinline__ float4 c2mul2(float2 c, float4 v)
 __device__ __forceinline__ float4 add4(float4 a, float4 b) { return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w); }
 __device__ __forceinline__ float4 sub4(float4 a, float4 b) { return make_float4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w); }
 
-#define HAT_PAIRS(a)                                                                 \
+// pairs of entries of block bx of a right-hand side (a.chunk entries per block)
+#define HAT_PAIRS(a, bx)                                                             \
     const int n2 = (a).len / 2, c2 = (a).chunk / 2;                                  \
-    const int q1 = min((int)(blockIdx.x + 1) * c2, n2);                              \
-    for (int q = blockIdx.x * c2 + threadIdx.x; q < q1; q += kThreads)
+    const int q1 = min(((bx) + 1) * c2, n2);                                          \
+    for (int q = (bx) * c2 + threadIdx.x; q < q1; q += kThreads)
 
 // u = rh + beta (u - omega vh); u = rh on the first iteration of a cycle or
-// after a restart
-__global__ void __launch_bounds__(kThreads) kh_u(KArgs<float> a)
+// after a restart (block bx of right-hand side r)
+__device__ __forceinline__ void hat_u(const KArgs<float> &a, int r, int bx)
 {
-    const int r = blockIdx.y;
     const BicgState &st = a.st[r];
     if (st.status != KS_RUNNING || !a.ost[r].active) return;
     const size_t off = (size_t)r * a.stride / 2;
@@ -166,18 +167,17 @@ __global__ void __launch_bounds__(kThreads) kh_u(KArgs<float> a)
     const float4 *VH = reinterpret_cast<const float4 *>(a.v) + off;
     float4 *U = reinterpret_cast<float4 *>(a.ph) + off;
     if (st.first) {
-        HAT_PAIRS(a) U[q] = RH[q];
+        HAT_PAIRS(a, bx) U[q] = RH[q];
         return;
     }
     const float2 be = make_float2((float)st.beta.re, (float)st.beta.im);
     const float2 om = make_float2((float)st.omega.re, (float)st.omega.im);
-    HAT_PAIRS(a) U[q] = add4(RH[q], c2mul2(be, sub4(U[q], c2mul2(om, VH[q]))));
+    HAT_PAIRS(a, bx) U[q] = add4(RH[q], c2mul2(be, sub4(U[q], c2mul2(om, VH[q]))));
 }
 
 // sh = rh - alpha vh
-__global__ void __launch_bounds__(kThreads) kh_s(KArgs<float> a)
+__device__ __forceinline__ void hat_s(const KArgs<float> &a, int r, int bx)
 {
-    const int r = blockIdx.y;
     const BicgState &st = a.st[r];
     if (st.status != KS_RUNNING || !a.ost[r].active) return;
     const size_t off = (size_t)r * a.stride / 2;
@@ -185,15 +185,14 @@ __global__ void __launch_bounds__(kThreads) kh_s(KArgs<float> a)
     const float4 *VH = reinterpret_cast<const float4 *>(a.v) + off;
     float4 *SH = reinterpret_cast<float4 *>(a.sh) + off;
     const float2 al = make_float2((float)st.alpha.re, (float)st.alpha.im);
-    HAT_PAIRS(a) SH[q] = sub4(RH[q], c2mul2(al, VH[q]));
+    HAT_PAIRS(a, bx) SH[q] = sub4(RH[q], c2mul2(al, VH[q]));
 }
 
 // x += alpha u + omega sh (into the buffer that does not hold the best
 // iterate); rh = sh - omega th; rho = (z, rh).  The true residual norm of the
 // new iterate comes from the inner products of kh_vt 1 (BicgState::rn2).
-__global__ void __launch_bounds__(kThreads) kh_xr(KArgs<float> a)
+__device__ __forceinline__ void hat_xr(const KArgs<float> &a, int r, int bx)
 {
-    const int r = blockIdx.y;
     BicgState &st = a.st[r];
     if (st.status != KS_RUNNING || !a.ost[r].active) return;
     const size_t off = (size_t)r * a.stride / 2;
@@ -207,7 +206,7 @@ __global__ void __launch_bounds__(kThreads) kh_xr(KArgs<float> a)
     const float4 *TH = reinterpret_cast<const float4 *>(a.t) + off;
     float4 *RH = reinterpret_cast<float4 *>(a.r) + off;
     double u[2] = {0.0, 0.0};
-    HAT_PAIRS(a)
+    HAT_PAIRS(a, bx)
     {
         const float4 sh = SH[q];
         XD[q] = add4(add4(XS[q], c2mul2(al, U[q])), c2mul2(om, sh));
@@ -218,7 +217,7 @@ __global__ void __launch_bounds__(kThreads) kh_xr(KArgs<float> a)
         u[1] += (double)(z0.x * rn.y - z0.y * rn.x) + (double)(z1.x * rn.w - z1.y * rn.z);
     }
     double tot[2];
-    if (block_reduce_last<2>(u, a.parts, a.cnt, r, blockIdx.x, gridDim.x, tot) && threadIdx.x == 0) {
+    if (block_reduce_last<2>(u, a.parts, a.cnt, r, bx, a.nblk, tot) && threadIdx.x == 0) {
         double *rerr = a.rerr + (size_t)r * a.rerr_stride;
         const double rnorm = sqrt(st.rn2);
         st.iter += 1;
@@ -474,15 +473,16 @@ __device__ __forceinline__ bool hat_march(TmaSmem &sm, const TmaParams &tp, cons
 
 // vh = D^-1 A u, (z, vh) -> alpha   (which = 0)
 // th = D^-1 A sh, (t, s)_W, (t, t)_W, (s, s)_W -> omega, ||r_new||   (which = 1)
-__global__ void __launch_bounds__(kThreads, 4) kh_vt(const __grid_constant__ TmaParams tp, KArgs<float> a, int which)
+// for column tile bx and plane chunk bz of gz of right-hand side r
+__device__ __forceinline__ void hat_vt(const TmaParams &tp, const KArgs<float> &a, int which, int r, int bx, int bz,
+                                       int gz)
 {
-    const int r = blockIdx.y;
     BicgState &st = a.st[r];
     if (st.status != KS_RUNNING || !a.ost[r].active) return;
-    if (a.sweeps && threadIdx.x == 0 && blockIdx.x == 0 && blockIdx.z == 0) atomicAdd(a.sweeps, 1ULL);
+    if (a.sweeps && threadIdx.x == 0 && bx == 0 && bz == 0) atomicAdd(a.sweeps, 1ULL);
     int i0, j0, k0, k1;
-    tma_tile(a.cmap, i0, j0);
-    tma_range(a.g.nz, k0, k1);
+    tma_tile_at(a.cmap, bx, i0, j0);
+    tma_range_at(a.g.nz, bz, gz, k0, k1);
     const size_t off = (size_t)r * a.stride;
     float2 *out = (which ? a.t : a.v) + off;
     double u[4] = {0.0, 0.0, 0.0, 0.0};
@@ -504,7 +504,7 @@ __global__ void __launch_bounds__(kThreads, 4) kh_vt(const __grid_constant__ Tma
                               });
     if (!ok) return;
     double tot[4];
-    if (block_reduce_last<4>(u, a.parts, a.cnt, r, blockIdx.x + gridDim.x * blockIdx.z, gridDim.x * gridDim.z, tot) &&
+    if (block_reduce_last<4>(u, a.parts, a.cnt, r, bx + a.cmap.tiles * bz, a.cmap.tiles * gz, tot) &&
         threadIdx.x == 0) {
         if (which == 0) {
             fin_v(st, tot);
@@ -517,6 +517,57 @@ __global__ void __launch_bounds__(kThreads, 4) kh_vt(const __grid_constant__ Tma
             }
         }
     }
+}
+
+// ---------------------------------------------------------------------------
+// kernels of one grid (blockIdx.y = right-hand side) and of a multi-grid
+// batch (one flat block index over the right-hand sides of every grid)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads) kh_u(KArgs<float> a) { hat_u(a, blockIdx.y, blockIdx.x); }
+__global__ void __launch_bounds__(kThreads) kh_s(KArgs<float> a) { hat_s(a, blockIdx.y, blockIdx.x); }
+__global__ void __launch_bounds__(kThreads) kh_xr(KArgs<float> a) { hat_xr(a, blockIdx.y, blockIdx.x); }
+__global__ void __launch_bounds__(kThreads, 4) kh_vt(const __grid_constant__ TmaParams tp, KArgs<float> a, int which)
+{
+    hat_vt(tp, a, which, blockIdx.y, blockIdx.x, blockIdx.z, gridDim.z);
+}
+
+// the grids of a multi-grid batch, passed by value: each grid's arguments,
+// its tensor maps (u and sh inputs) and where its blocks start in the flat
+// launches
+struct alignas(64) HatMulti {
+    TmaParams tp[kMaxMultiGrids][2];
+    KArgs<float> a[kMaxMultiGrids];
+    int ng;
+    int nr[kMaxMultiGrids];            // right-hand sides of each grid
+    int zch[kMaxMultiGrids];           // node-plane chunks of its stencil launches
+    int eb0[kMaxMultiGrids + 1];       // first flat block of each grid: elementwise launches
+    int sb0[kMaxMultiGrids + 1];       // first flat block of each grid: stencil launches
+};
+__device__ __forceinline__ int multi_grid_of(const int *b0, int ng, int b)
+{
+    int g = 0;
+    while (g + 1 < ng && b >= b0[g + 1]) g++;
+    return g;
+}
+template <int K> __global__ void __launch_bounds__(kThreads) kh_elem_multi(const __grid_constant__ HatMulti p)
+{
+    const int g = multi_grid_of(p.eb0, p.ng, blockIdx.x);
+    const KArgs<float> &a = p.a[g];
+    const int local = blockIdx.x - p.eb0[g];
+    const int r = local / a.nblk, bx = local - r * a.nblk;
+    if (K == 0) hat_u(a, r, bx);
+    else if (K == 1) hat_s(a, r, bx);
+    else hat_xr(a, r, bx);
+}
+__global__ void __launch_bounds__(kThreads, 4) kh_vt_multi(const __grid_constant__ HatMulti p, int which)
+{
+    const int g = multi_grid_of(p.sb0, p.ng, blockIdx.x);
+    const KArgs<float> &a = p.a[g];
+    const int per = a.cmap.tiles * p.zch[g];
+    const int local = blockIdx.x - p.sb0[g];
+    const int r = local / per, rem = local - r * per;
+    const int bz = rem / a.cmap.tiles, bx = rem - bz * a.cmap.tiles;
+    hat_vt(p.tp[g][which], a, which, r, bx, bz, p.zch[g]);
 }
 
 // ---------------------------------------------------------------------------
@@ -558,5 +609,41 @@ void launch_hat_iter(const KArgs<float> &a, int nrhs, cudaStream_t s, cudaEvent_
 }
 
 void launch_hat_apply(const KArgs<float> &a, int nrhs, cudaStream_t s) { launch_hat_vt(a, a.tma, 0, nrhs, s); }
+
+// one iteration of the fused FP32 BiCGStab over the grids of a multi-grid
+// batch: five launches in all, each over the right-hand sides of every grid
+// (zch[g]: node-plane chunks of grid g's stencil blocks, 0 for the
+// occupancy-based choice)
+int launch_hat_iter_multi(const KArgs<float> *args, const int *nrhs, const int *zch, int ng, cudaStream_t s)
+{
+    if (ng < 1 || ng > kMaxMultiGrids) return 1;
+    static_assert(sizeof(HatMulti) <= 32000, "multi-grid parameters exceed the kernel parameter space");
+    HatMulti p;
+    std::memset(&p, 0, sizeof p);
+    p.ng = ng;
+    const int res = tma_resident(kh_vt_multi, sizeof(TmaSmem), 3);
+    p.eb0[0] = p.sb0[0] = 0;
+    for (int g = 0; g < ng; g++) {
+        p.a[g] = args[g];
+        p.nr[g] = nrhs[g];
+        p.tp[g][0].in = args[g].tma->ph;
+        p.tp[g][1].in = args[g].tma->sh;
+        for (int w = 0; w < 2; w++) {
+            p.tp[g][w].sig = args[g].tma->sig;
+            p.tp[g][w].node = args[g].tma->node;
+        }
+        p.zch[g] = zch && zch[g] > 0 ? zch[g] : stage_chunks(args[g].g.nz, args[g].cmap.tiles, res);
+        p.eb0[g + 1] = p.eb0[g] + nrhs[g] * args[g].nblk;
+        p.sb0[g + 1] = p.sb0[g] + nrhs[g] * args[g].cmap.tiles * p.zch[g];
+    }
+    counted(5);
+    const size_t sm = sizeof(TmaSmem);
+    kh_elem_multi<0><<<p.eb0[ng], kThreads, 0, s>>>(p);
+    kh_vt_multi<<<p.sb0[ng], kThreads, sm, s>>>(p, 0);
+    kh_elem_multi<1><<<p.eb0[ng], kThreads, 0, s>>>(p);
+    kh_vt_multi<<<p.sb0[ng], kThreads, sm, s>>>(p, 1);
+    kh_elem_multi<2><<<p.eb0[ng], kThreads, 0, s>>>(p);
+    return 0;
+}
 
 }  // namespace mt3d

@@ -668,6 +668,25 @@ int Solver::run_hat(int nrhs, int maxit)
     return check(cudaGetLastError(), "fused BiCGStab launch");
 }
 
+KArgs<float> Solver::hat_args(int nrhs)
+{
+    KArgs<float> a = kargs<float>(nrhs, 1);
+    a.maxit = ctl.IterPerDivCor;
+    a.sweeps = nullptr;
+    return a;
+}
+int Solver::hat_cycle_begin(int nrhs, KArgs<float> &a)
+{
+    a = hat_args(nrhs);
+    launch_hat_cast(a, ws_.tmp.as<double2>(), nE, nrhs, stream_);
+    return check(cudaGetLastError(), "fused BiCGStab start");
+}
+int Solver::hat_cycle_end(int nrhs, const KArgs<float> &a)
+{
+    launch_bicg_finish(a, nrhs, stream_);
+    return check(cudaGetLastError(), "fused BiCGStab end");
+}
+
 int Solver::run_divcorr(int nrhs)
 {
     DArgs a = dargs(nrhs);
@@ -810,8 +829,61 @@ int Solver::bicg(const double *b, double *x, int maxit, double tol, int *niter, 
 // ---------------------------------------------------------------------------
 // FWDsolve3D over a batch of right-hand sides
 // ---------------------------------------------------------------------------
+void Solver::push_state(SolveRun &run)
+{
+    cudaMemcpyAsync(ws_.ost.as<void>(), run.os.data(), run.nrhs * sizeof(OuterState), cudaMemcpyHostToDevice,
+                    stream_);
+}
+
+// take over the device-written fields of the outer states
+int Solver::pull_state(SolveRun &run)
+{
+    std::vector<OuterState> dv(run.nrhs);
+    cudaMemcpyAsync(dv.data(), ws_.ost.as<void>(), run.nrhs * sizeof(OuterState), cudaMemcpyDeviceToHost, stream_);
+    int rc = sync("fwdsolve");
+    if (rc) return rc;
+    for (int r = 0; r < run.nrhs; r++) {
+        run.os[r].bnorm64 = dv[r].bnorm64;
+        run.os[r].relres = dv[r].relres;
+        run.os[r].scale = dv[r].scale;
+        run.os[r].divJ[0] = dv[r].divJ[0];
+        run.os[r].divJ[1] = dv[r].divJ[1];
+    }
+    return 0;
+}
+
+bool SolveRun::any_active() const
+{
+    for (auto &o : os)
+        if (o.active) return true;
+    return false;
+}
+
 int Solver::solve(int nrhs, const double *omegas, const int *trans, const double *bc, const double *src, double *e,
                   int *status, bool device)
+{
+    SolveRun run;
+    int rc = solve_begin(run, nrhs, omegas, trans, bc, src, e, status, device);
+    if (rc) return rc;
+    while (!run.done) {
+        if ((rc = solve_pre(run))) return rc;
+        if (run.done) break;
+        if ((rc = solve_fp32(run))) return rc;
+        if ((rc = solve_post(run))) return rc;
+    }
+    return solve_end(run);
+}
+
+// ---------------------------------------------------------------------------
+// FWDsolve3D over a batch of right-hand sides, in phases: set-up (RHS
+// assembly, initial divergence correction), then per outer cycle the true
+// residual and the decisions (solve_pre), the FP32 Krylov cycle (solve_fp32),
+// the FP64 cycles and bookkeeping (solve_post), and the post-processing
+// (solve_end).  A multi-grid batch runs the phases of several handles in
+// lockstep, with the FP32 cycles of all grids in shared launches.
+// ---------------------------------------------------------------------------
+int Solver::solve_begin(SolveRun &run, int nrhs, const double *omegas, const int *trans, const double *bc,
+                        const double *src, double *e, int *status, bool device)
 {
     if (!cond_set) return fail(5, "fwdsolve: conductivity not set (call mt3d_update_cond)");
     if (nrhs < 1 || !omegas || !e) return fail(5, "fwdsolve: invalid arguments");
@@ -821,20 +893,26 @@ int Solver::solve(int nrhs, const double *omegas, const int *trans, const double
     int rc;
     if ((rc = ensure_workspace(nrhs, prec))) return rc;
     Workspace &w = ws_;
+    run = SolveRun{};
+    run.nrhs = nrhs;
+    run.prec = prec;
+    run.device = device;
+    run.e = e;
+    run.status = status;
+    run.refine = prec == 1 || ctl.formulation == 1;  // loop driven by the true FP64 residual
     const size_t ebytes = nE * sizeof(double2);
     const cudaMemcpyKind in_kind = device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-    const cudaMemcpyKind out_kind = device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
     if (prof_) collect_events();
     double2 *B = w.b.as<double2>(), *X = w.X.as<double2>(), *BC = w.bc.as<double2>(), *TMP = w.tmp.as<double2>();
     // boundary data (kept for the post-processing) and initial guess
-    std::vector<OuterState> os(nrhs);
+    std::vector<OuterState> &os = run.os;
+    os.assign(nrhs, OuterState{});
     for (int r = 0; r < nrhs; r++) {
-        os[r] = OuterState{};
         os[r].omega = omegas[r];
         os[r].trans = trans ? (trans[r] != 0) : 0;
         os[r].active = 1;
     }
-    cudaMemcpyAsync(w.ost.as<void>(), os.data(), nrhs * sizeof(OuterState), cudaMemcpyHostToDevice, stream_);
+    push_state(run);
     cudaMemsetAsync(BC, 0, nrhs * ebytes, stream_);
     if (bc) cudaMemcpyAsync(BC, bc, nrhs * ebytes, in_kind, stream_);
     cudaMemcpyAsync(X, e, nrhs * ebytes, in_kind, stream_);
@@ -869,7 +947,7 @@ int Solver::solve(int nrhs, const double *omegas, const int *trans, const double
         o.tol = o.trans ? ctl.tolEMadj : (o.has_bc ? ctl.tolEMfwd : ctl.tolEMadj);
         any_src = any_src || o.has_src;
     }
-    cudaMemcpyAsync(w.ost.as<void>(), os.data(), nrhs * sizeof(OuterState), cudaMemcpyHostToDevice, stream_);
+    push_state(run);
     // sources: b += V_E src (forward) or b = src (transposed); phi0 for the
     // divergence correction, or the grad-div source correction of the SP2
     // right-hand side (f90/3D_MT/FWD_SP2/EMsolve3D.f90:215-228, 271-289)
@@ -894,26 +972,8 @@ int Solver::solve(int nrhs, const double *omegas, const int *trans, const double
             os[r].converged = 1;
         }
     diag = Diag{};
-    std::vector<Diag> dg(nrhs);
-    auto push_state = [&]() {
-        cudaMemcpyAsync(w.ost.as<void>(), os.data(), nrhs * sizeof(OuterState), cudaMemcpyHostToDevice, stream_);
-    };
-    auto pull_state = [&]() -> int {
-        // only the device-written fields are taken over
-        std::vector<OuterState> dv(nrhs);
-        cudaMemcpyAsync(dv.data(), w.ost.as<void>(), nrhs * sizeof(OuterState), cudaMemcpyDeviceToHost, stream_);
-        int rc2 = sync("fwdsolve");
-        if (rc2) return rc2;
-        for (int r = 0; r < nrhs; r++) {
-            os[r].bnorm64 = dv[r].bnorm64;
-            os[r].relres = dv[r].relres;
-            os[r].scale = dv[r].scale;
-            os[r].divJ[0] = dv[r].divJ[0];
-            os[r].divJ[1] = dv[r].divJ[1];
-        }
-        return 0;
-    };
-    if ((rc = pull_state())) return rc;
+    run.dg.assign(nrhs, Diag{});
+    if ((rc = pull_state(run))) return rc;
     for (int r = 0; r < nrhs; r++)
         if (!std::isfinite(os[r].bnorm64)) {
             os[r].active = 0;
@@ -925,182 +985,235 @@ int Solver::solve(int nrhs, const double *omegas, const int *trans, const double
         os[r].dc_run = ctl.formulation == 0 && os[r].active && os[r].has_src;
         if (os[r].dc_run) { os[r].nDivCor = 1; any_dc = true; }
     }
-    push_state();
+    push_state(run);
     if (any_dc) {
         if ((rc = run_divcorr(nrhs))) return rc;
-        if ((rc = pull_state())) return rc;
+        if ((rc = pull_state(run))) return rc;
         for (int r = 0; r < nrhs; r++)
-            if (os[r].dc_run) { dg[r].divJ.push_back(os[r].divJ[0]); dg[r].divJ.push_back(os[r].divJ[1]); }
+            if (os[r].dc_run) { run.dg[r].divJ.push_back(os[r].divJ[0]); run.dg[r].divJ.push_back(os[r].divJ[1]); }
     }
-    std::vector<BicgState> bs(nrhs);
-    std::vector<double> rerr((size_t)nrhs * (ctl.IterPerDivCor + 1));
-    auto any_active = [&]() {
-        for (auto &o : os) if (o.active) return true;
-        return false;
-    };
-    const bool refine = prec == 1 || ctl.formulation == 1;  // loop driven by the true FP64 residual
+    run.bs.assign(nrhs, BicgState{});
+    run.rerr.assign((size_t)nrhs * (ctl.IterPerDivCor + 1), 0.0);
     // mixed precision: a right-hand side whose last FP32 cycle did not halve
     // its true FP64 residual continues with FP64 Krylov cycles (the FP32
     // operator's rounding can stop an FP32 solve from reducing a residual
     // that is already small relative to the field)
-    std::vector<double> prev_relres(nrhs, std::numeric_limits<double>::infinity());
-    std::vector<char> hi(nrhs, 0);
+    run.prev_relres.assign(nrhs, std::numeric_limits<double>::infinity());
+    run.hi.assign(nrhs, 0);
     // smallest relative residual of the last FP32 cycle's own iteration and
     // the number of FP32 cycles in a row that did not halve the true residual
-    std::vector<double> inner_best(nrhs, 0.0);
-    std::vector<int> stalls(nrhs, 0);
-    while (any_active()) {
-        if (refine) {
-            // true FP64 residual r64 = b - A X (into tmp); converged right-hand
-            // sides leave the loop, the others get an FP32 correction solve
-            for (auto &o : os) o.dc_run = 0;
-            push_state();
-            {
-                KArgs<double> a = kargs<double>(nrhs, 0);
-                a.r = w.tmp.as<double2>();
-                launch_res64(a, nrhs, stream_);
-            }
-            if ((rc = pull_state())) return rc;
-            bool work = false;
-            for (int r = 0; r < nrhs; r++) {
-                OuterState &o = os[r];
-                if (!o.active) continue;
-                if (!std::isfinite(o.relres)) { o.active = 0; o.failed = 3; continue; }
-                if (o.relres <= o.tol) { o.active = 0; o.converged = 1; continue; }
-                if (o.nDivCor >= ctl.MaxDivCor) { o.active = 0; o.failed = 1; continue; }
-                o.tol_inner = o.tol * o.bnorm64 * o.scale;  // tol*||b|| relative to ||r64||
-                // an FP32 cycle that did not halve the true residual: when its
-                // own iteration converged well, the FP32 operator's rounding is
-                // the limit and the right-hand side moves to FP64; when the
-                // iteration itself stagnated, one more FP32 cycle restarts it
-                // from the new residual first
-                if (prec == 1 && !hi[r]) {
-                    if (o.relres > 0.5 * prev_relres[r]) {
-                        if (inner_best[r] < 0.1 || ++stalls[r] >= 2) hi[r] = 1;
-                    } else {
-                        stalls[r] = 0;
-                    }
-                }
-                prev_relres[r] = o.relres;
-                work = true;
-            }
-            if (!work) break;
-            push_state();
-        }
-        if (prec == 1) {
-            // FP32 cycles on the normalised residual, FP64 cycles on (b, X) for
-            // the right-hand sides that left FP32; each group runs with the
-            // other group's right-hand sides marked inactive on the device
-            bool n32 = false, n64 = false;
-            for (int r = 0; r < nrhs; r++) {
-                if (!os[r].active) continue;
-                (hi[r] ? n64 : n32) = true;
-            }
-            std::vector<OuterState> grp(os);
-            if (n32) {
-                for (int r = 0; r < nrhs; r++) grp[r].active = os[r].active && !hi[r];
-                cudaMemcpyAsync(w.ost.as<void>(), grp.data(), nrhs * sizeof(OuterState), cudaMemcpyHostToDevice,
-                                stream_);
-                if (w.padded && ctl.fused) {
-                    // FP32 cycle in preconditioned variables from a zero first guess
-                    if ((rc = tma_ready())) return rc;
-                    if ((rc = run_hat(nrhs, ctl.IterPerDivCor))) return rc;
-                } else if (w.padded) {
-                    if ((rc = tma_ready())) return rc;
-                    launch_cast_padded(g64_, w.ost.as<OuterState>(), nE, w.tmp.as<double2>(), pl_, w.f_b.as<float2>(),
-                                       w.f_x0.as<float2>(), nrhs, stream_);
-                    if ((rc = run_bicg(nrhs, 1, ctl.IterPerDivCor))) return rc;
-                } else {
-                    launch_cast(w.ost.as<OuterState>(), (int)nE, nE, w.tmp.as<double2>(), w.f_b.as<float2>(),
-                                w.f_x0.as<float2>(), nrhs, stream_);
-                    if ((rc = run_bicg(nrhs, 1, ctl.IterPerDivCor))) return rc;
-                }
-                if (w.padded)
-                    launch_update_padded(g64_, w.ost.as<OuterState>(), nE, pl_, w.f_x0.as<float2>(), X, nrhs, stream_);
-                else
-                    launch_update(w.ost.as<OuterState>(), (int)nE, nE, w.f_x0.as<float2>(), X, nrhs, stream_);
-            }
-            if (n64) {
-                if ((rc = ensure_fp64_krylov(nrhs))) return rc;
-                for (int r = 0; r < nrhs; r++) grp[r].active = os[r].active && hi[r];
-                cudaMemcpyAsync(w.ost.as<void>(), grp.data(), nrhs * sizeof(OuterState), cudaMemcpyHostToDevice,
-                                stream_);
-                if ((rc = run_bicg(nrhs, 0, ctl.IterPerDivCor))) return rc;
-            }
-            push_state();
-        } else {
-            // Krylov call: FP64 on (b, X)
-            if ((rc = run_bicg(nrhs, prec, ctl.IterPerDivCor))) return rc;
-        }
-        cudaMemcpyAsync(bs.data(), w.bst.as<void>(), nrhs * sizeof(BicgState), cudaMemcpyDeviceToHost, stream_);
-        cudaMemcpyAsync(rerr.data(), w.rerr.as<void>(), rerr.size() * sizeof(double), cudaMemcpyDeviceToHost, stream_);
-        if ((rc = sync("fwdsolve Krylov cycle"))) return rc;
-        if ((rc = check_device_error("fwdsolve Krylov cycle"))) return rc;
-        if (prof_) collect_events();
-        for (int r = 0; r < nrhs; r++) {
-            OuterState &o = os[r];
-            o.dc_run = 0;
-            if (!o.active) continue;
-            const BicgState &st = bs[r];
-            const int maxit = ctl.IterPerDivCor;
-            const bool conv = st.status == KS_CONVERGED;
-            const int niter = conv ? st.iter : maxit;
-            double *h = &rerr[(size_t)r * (maxit + 1)];
-            if (!conv) h[maxit - 1] = st.imin > 0 ? h[st.imin - 1] : h[0];
-            for (int k = 0; k < niter; k++) dg[r].EMrelErr.push_back(h[k]);
-            if (prec == 1 && !hi[r]) {
-                double best = 1.0;
-                for (int k = 0; k < niter; k++) best = std::min(best, h[k]);
-                inner_best[r] = best;
-            }
-            o.nIterTotal += niter;
-            if (!refine) {
-                if (conv) o.converged = 1;
-                if (st.status == KS_BREAKDOWN || st.status == KS_NAN) o.failed = (st.status == KS_NAN) ? 3 : 2;
-            } else if (st.status == KS_NAN) {
-                o.failed = 3;
-            }
-            o.nDivCor += 1;
-            if (o.nDivCor < ctl.MaxDivCor) {
-                o.dc_run = ctl.formulation == 0;
-            } else if (!refine) {
-                if (!o.failed) o.failed = 1;
-            }
-        }
-        push_state();
-        bool dc = false;
-        for (auto &o : os) dc = dc || o.dc_run;
-        if (dc) {
-            if ((rc = run_divcorr(nrhs))) return rc;
-            if ((rc = pull_state())) return rc;
-            for (int r = 0; r < nrhs; r++)
-                if (os[r].dc_run) { dg[r].divJ.push_back(os[r].divJ[0]); dg[r].divJ.push_back(os[r].divJ[1]); }
-        }
-        for (int r = 0; r < nrhs; r++) {
-            OuterState &o = os[r];
-            o.dc_run = 0;
-            if (!o.active) continue;
-            if (!refine) {
-                if (o.converged || o.failed) o.active = 0;
-            } else if (o.failed == 3) {
-                o.active = 0;
-            }
-        }
-        // right-hand sides that finished in this cycle sit out the next one
-        push_state();
+    run.inner_best.assign(nrhs, 0.0);
+    run.stalls.assign(nrhs, 0);
+    run.done = !run.any_active();
+    return 0;
+}
+
+// start of an outer cycle: the true FP64 residual r64 = b - A X (into tmp);
+// converged right-hand sides leave the loop; the FP32 and FP64 groups of the
+// mixed-precision cycle; the FP32 group marked active on the device
+int Solver::solve_pre(SolveRun &run)
+{
+    Workspace &w = ws_;
+    std::vector<OuterState> &os = run.os;
+    const int nrhs = run.nrhs;
+    int rc;
+    run.n32 = run.n64 = false;
+    if (!run.any_active()) {
+        run.done = true;
+        return 0;
     }
-    // true relative residual of the returned interior field (all right-hand sides)
+    if (run.refine) {
+        for (auto &o : os) o.dc_run = 0;
+        push_state(run);
+        {
+            KArgs<double> a = kargs<double>(nrhs, 0);
+            a.r = w.tmp.as<double2>();
+            launch_res64(a, nrhs, stream_);
+        }
+        if ((rc = pull_state(run))) return rc;
+        bool work = false;
+        for (int r = 0; r < nrhs; r++) {
+            OuterState &o = os[r];
+            if (!o.active) continue;
+            if (!std::isfinite(o.relres)) { o.active = 0; o.failed = 3; continue; }
+            if (o.relres <= o.tol) { o.active = 0; o.converged = 1; continue; }
+            if (o.nDivCor >= ctl.MaxDivCor) { o.active = 0; o.failed = 1; continue; }
+            o.tol_inner = o.tol * o.bnorm64 * o.scale;  // tol*||b|| relative to ||r64||
+            // an FP32 cycle that did not halve the true residual: when its
+            // own iteration converged well, the FP32 operator's rounding is
+            // the limit and the right-hand side moves to FP64; when the
+            // iteration itself stagnated, one more FP32 cycle restarts it
+            // from the new residual first
+            if (run.prec == 1 && !run.hi[r]) {
+                if (o.relres > 0.5 * run.prev_relres[r]) {
+                    if (run.inner_best[r] < 0.1 || ++run.stalls[r] >= 2) run.hi[r] = 1;
+                } else {
+                    run.stalls[r] = 0;
+                }
+            }
+            run.prev_relres[r] = o.relres;
+            work = true;
+        }
+        if (!work) {
+            run.done = true;
+            return 0;
+        }
+        push_state(run);
+    }
+    if (run.prec == 1) {
+        // FP32 cycles on the normalised residual, FP64 cycles on (b, X) for
+        // the right-hand sides that left FP32; each group runs with the
+        // other group's right-hand sides marked inactive on the device
+        for (int r = 0; r < nrhs; r++) {
+            if (!os[r].active) continue;
+            (run.hi[r] ? run.n64 : run.n32) = true;
+        }
+        run.grp = os;
+        if (run.n32) {
+            for (int r = 0; r < nrhs; r++) run.grp[r].active = os[r].active && !run.hi[r];
+            cudaMemcpyAsync(w.ost.as<void>(), run.grp.data(), nrhs * sizeof(OuterState), cudaMemcpyHostToDevice,
+                            stream_);
+            if (w.padded && (rc = tma_ready())) return rc;
+        }
+    }
+    return 0;
+}
+
+// whether this cycle's FP32 group runs the fused iteration (and so may share
+// launches with other grids)
+bool Solver::fp32_fused(const SolveRun &run) const
+{
+    return run.prec == 1 && run.n32 && ws_.padded && ctl.fused;
+}
+
+// the FP32 cycle of the FP32 group on this handle alone
+int Solver::solve_fp32(SolveRun &run)
+{
+    Workspace &w = ws_;
+    const int nrhs = run.nrhs;
+    if (!(run.prec == 1 && run.n32)) return 0;
+    if (fp32_fused(run)) return run_hat(nrhs, ctl.IterPerDivCor);
+    if (w.padded) {
+        launch_cast_padded(g64_, w.ost.as<OuterState>(), nE, w.tmp.as<double2>(), pl_, w.f_b.as<float2>(),
+                           w.f_x0.as<float2>(), nrhs, stream_);
+    } else {
+        launch_cast(w.ost.as<OuterState>(), (int)nE, nE, w.tmp.as<double2>(), w.f_b.as<float2>(), w.f_x0.as<float2>(),
+                    nrhs, stream_);
+    }
+    return run_bicg(nrhs, 1, ctl.IterPerDivCor);
+}
+
+// end of an outer cycle: the FP32 correction into X, the FP64 group (or the
+// FP64 Krylov call), the Krylov states and histories, the divergence
+// correction and the right-hand sides that finished
+int Solver::solve_post(SolveRun &run)
+{
+    Workspace &w = ws_;
+    std::vector<OuterState> &os = run.os;
+    const int nrhs = run.nrhs, prec = run.prec;
+    double2 *X = w.X.as<double2>();
+    int rc;
+    if (prec == 1) {
+        if (run.n32) {
+            if (w.padded)
+                launch_update_padded(g64_, w.ost.as<OuterState>(), nE, pl_, w.f_x0.as<float2>(), X, nrhs, stream_);
+            else
+                launch_update(w.ost.as<OuterState>(), (int)nE, nE, w.f_x0.as<float2>(), X, nrhs, stream_);
+        }
+        if (run.n64) {
+            if ((rc = ensure_fp64_krylov(nrhs))) return rc;
+            for (int r = 0; r < nrhs; r++) run.grp[r].active = os[r].active && run.hi[r];
+            cudaMemcpyAsync(w.ost.as<void>(), run.grp.data(), nrhs * sizeof(OuterState), cudaMemcpyHostToDevice,
+                            stream_);
+            if ((rc = run_bicg(nrhs, 0, ctl.IterPerDivCor))) return rc;
+        }
+        push_state(run);
+    } else {
+        // Krylov call: FP64 on (b, X)
+        if ((rc = run_bicg(nrhs, prec, ctl.IterPerDivCor))) return rc;
+    }
+    std::vector<BicgState> &bs = run.bs;
+    std::vector<double> &rerr = run.rerr;
+    cudaMemcpyAsync(bs.data(), w.bst.as<void>(), nrhs * sizeof(BicgState), cudaMemcpyDeviceToHost, stream_);
+    cudaMemcpyAsync(rerr.data(), w.rerr.as<void>(), rerr.size() * sizeof(double), cudaMemcpyDeviceToHost, stream_);
+    if ((rc = sync("fwdsolve Krylov cycle"))) return rc;
+    if ((rc = check_device_error("fwdsolve Krylov cycle"))) return rc;
+    if (prof_) collect_events();
+    for (int r = 0; r < nrhs; r++) {
+        OuterState &o = os[r];
+        o.dc_run = 0;
+        if (!o.active) continue;
+        const BicgState &st = bs[r];
+        const int maxit = ctl.IterPerDivCor;
+        const bool conv = st.status == KS_CONVERGED;
+        const int niter = conv ? st.iter : maxit;
+        double *h = &rerr[(size_t)r * (maxit + 1)];
+        if (!conv) h[maxit - 1] = st.imin > 0 ? h[st.imin - 1] : h[0];
+        for (int k = 0; k < niter; k++) run.dg[r].EMrelErr.push_back(h[k]);
+        if (prec == 1 && !run.hi[r]) {
+            double best = 1.0;
+            for (int k = 0; k < niter; k++) best = std::min(best, h[k]);
+            run.inner_best[r] = best;
+        }
+        o.nIterTotal += niter;
+        if (!run.refine) {
+            if (conv) o.converged = 1;
+            if (st.status == KS_BREAKDOWN || st.status == KS_NAN) o.failed = (st.status == KS_NAN) ? 3 : 2;
+        } else if (st.status == KS_NAN) {
+            o.failed = 3;
+        }
+        o.nDivCor += 1;
+        if (o.nDivCor < ctl.MaxDivCor) {
+            o.dc_run = ctl.formulation == 0;
+        } else if (!run.refine) {
+            if (!o.failed) o.failed = 1;
+        }
+    }
+    push_state(run);
+    bool dc = false;
+    for (auto &o : os) dc = dc || o.dc_run;
+    if (dc) {
+        if ((rc = run_divcorr(nrhs))) return rc;
+        if ((rc = pull_state(run))) return rc;
+        for (int r = 0; r < nrhs; r++)
+            if (os[r].dc_run) { run.dg[r].divJ.push_back(os[r].divJ[0]); run.dg[r].divJ.push_back(os[r].divJ[1]); }
+    }
+    for (int r = 0; r < nrhs; r++) {
+        OuterState &o = os[r];
+        o.dc_run = 0;
+        if (!o.active) continue;
+        if (!run.refine) {
+            if (o.converged || o.failed) o.active = 0;
+        } else if (o.failed == 3) {
+            o.active = 0;
+        }
+    }
+    // right-hand sides that finished in this cycle sit out the next one
+    push_state(run);
+    run.done = !run.any_active();
+    return 0;
+}
+
+// true relative residual of the returned interior fields, post-processing,
+// copy back and the statuses
+int Solver::solve_end(SolveRun &run)
+{
+    Workspace &w = ws_;
+    std::vector<OuterState> &os = run.os;
+    const int nrhs = run.nrhs;
+    double2 *X = w.X.as<double2>(), *BC = w.bc.as<double2>();
+    int rc;
     for (auto &o : os) { o.active = 1; o.dc_run = 0; }
-    push_state();
+    push_state(run);
     {
         KArgs<double> a = kargs<double>(nrhs, 0);
-        if (prec == 1) a.r = w.tmp.as<double2>();
+        if (run.prec == 1) a.r = w.tmp.as<double2>();
         launch_res64(a, nrhs, stream_);
     }
-    if ((rc = pull_state())) return rc;
-    // post-processing and copy back
+    if ((rc = pull_state(run))) return rc;
     launch_post(g64_, X, BC, nE, w.ost.as<OuterState>(), nrhs, stream_);
-    cudaMemcpyAsync(e, X, nrhs * ebytes, out_kind, stream_);
+    cudaMemcpyAsync(run.e, X, nrhs * nE * sizeof(double2),
+                    run.device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, stream_);
     if ((rc = sync("fwdsolve copy back"))) return rc;
     if (prof_) collect_events();
     int worst = 0;
@@ -1110,14 +1223,14 @@ int Solver::solve(int nrhs, const double *omegas, const int *trans, const double
         if (o.failed == 3) s = 3;
         else if (o.failed == 2) s = 2;
         else if (!o.converged) s = 1;
-        if (status) status[r] = s;
+        if (run.status) run.status[r] = s;
         worst = std::max(worst, s);
-        dg[r].nIterTotal = o.nIterTotal;
-        dg[r].nDivCor = o.nDivCor;
-        dg[r].failed = s != 0;
-        dg[r].final_relres = o.relres;
+        run.dg[r].nIterTotal = o.nIterTotal;
+        run.dg[r].nDivCor = o.nDivCor;
+        run.dg[r].failed = s != 0;
+        run.dg[r].final_relres = o.relres;
     }
-    diag = dg[0];
+    diag = run.dg[0];
     batch_niter.assign(nrhs, 0);
     batch_relres.assign(nrhs, 0.0);
     for (int r = 0; r < nrhs; r++) {

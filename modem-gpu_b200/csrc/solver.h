@@ -64,9 +64,35 @@ struct Workspace {
     DevBuf bst, pst, ost, parts, cnt, rerr, dcrerr;
 };
 
+// state of one FWDsolve3D call over a batch between its phases (solve_begin,
+// solve_pre, solve_fp32, solve_post, solve_end); a multi-grid batch drives
+// several of these in lockstep
+struct SolveRun {
+    int nrhs = 0, prec = 0;
+    bool device = false, refine = false, done = false;
+    bool n32 = false, n64 = false;  // groups of the current mixed-precision cycle
+    double *e = nullptr;
+    int *status = nullptr;
+    std::vector<OuterState> os, grp;
+    std::vector<Diag> dg;
+    std::vector<BicgState> bs;
+    std::vector<double> rerr, prev_relres, inner_best;
+    std::vector<char> hi;
+    std::vector<int> stalls;
+    bool any_active() const;
+};
+
 // fixed scratch of mt3d_mult_aii_device_noalloc (noalloc.cu): resolved and
 // committed once per device at handle creation
 int noalloc_prepare(int dev, std::string &err);
+
+class Solver;
+// FWDsolve3D over the right-hand sides of several handles, the FP32 cycles
+// of all grids in shared launches (multi.cu); zch: node-plane chunks of each
+// grid's stencil blocks (NULL or 0 entries: the occupancy-based choice)
+int fwdsolve_multi(int nh, Solver *const *hs, const int *nrhs, const double *const *omegas, const int *const *trans,
+                   const double *const *bc, const double *const *src, double *const *e, int *const *status,
+                   const int *zch, bool device, std::string &err);
 
 // header of a solution file (solnio.cu); any output may be NULL
 int read_soln_header(const char *path, int *nTx, int *nMode, int *nx, int *ny, int *nz, int *nzAir, double *origin,
@@ -84,6 +110,20 @@ class Solver {
     int bicg(const double *b, double *x, int maxit, double tol, int *niter, double *rerr, int *failed);
     int solve(int nrhs, const double *omegas, const int *trans, const double *bc, const double *src, double *e,
               int *status, bool device = false);
+    int solve_begin(SolveRun &run, int nrhs, const double *omegas, const int *trans, const double *bc,
+                    const double *src, double *e, int *status, bool device);
+    int solve_pre(SolveRun &run);
+    int solve_fp32(SolveRun &run);
+    int solve_post(SolveRun &run);
+    int solve_end(SolveRun &run);
+    bool fp32_fused(const SolveRun &run) const;
+    // multi-grid batches (multi.cu): the arguments of this handle's fused
+    // FP32 cycle, its cast and end kernels, and its stream and device
+    KArgs<float> hat_args(int nrhs);
+    int hat_cycle_begin(int nrhs, KArgs<float> &a);
+    int hat_cycle_end(int nrhs, const KArgs<float> &a);
+    cudaStream_t stream() const { return stream_; }
+    int device() const { return dev_; }
     int set_stream(void *s);
     int set_wait_limit(int polls);
     int set_fused(int on);
@@ -122,6 +162,8 @@ class Solver {
     int run_bicg(int nrhs, int precision, int maxit);
     int run_divcorr(int nrhs);
     int run_hat(int nrhs, int maxit);
+    void push_state(SolveRun &run);
+    int pull_state(SolveRun &run);
     template <typename T> KArgs<T> kargs(int nrhs, int precision_ws);
     template <typename T> ColArgs<T> cargs();
     DArgs dargs(int nrhs);

@@ -48,6 +48,7 @@ constexpr unsigned kNBytes = kNR * kNW * 4;      // 1296
 // (k+1, k+2), so that four blocks fit on an SM
 constexpr unsigned kFSlot = 8704, kSSlot = 4864, kNSlot = 1408;
 constexpr int kWaitLimit = 1 << 22;
+constexpr int kMaxMultiGrids = 8;  // grids of one multi-grid batch
 static_assert(kTX * kTY == kThreads, "one thread per node column");
 static_assert(kFSlot % 128 == 0 && kSSlot % 128 == 0 && kNSlot % 128 == 0, "tensor-copy destinations 128-byte aligned");
 static_assert(kFSlot >= kFBytes && kSSlot >= kSBytes && kNSlot >= kNBytes, "slot sizes");
@@ -138,17 +139,20 @@ __device__ __forceinline__ float2 tma_phi_node(const TmaSmem &sm, const Geo<floa
     return cscale(acc, wn);
 }
 
-__device__ __forceinline__ void tma_tile(const ColMap &m, int &i0, int &j0)
+// tile (i0, j0) of column-tile bx, and node planes [k0, k1) of chunk bz of gz
+__device__ __forceinline__ void tma_tile_at(const ColMap &m, int bx, int &i0, int &j0)
 {
-    i0 = (blockIdx.x % m.tiles_x) * kTX;
-    j0 = (blockIdx.x / m.tiles_x) * kTY;
+    i0 = (bx % m.tiles_x) * kTX;
+    j0 = (bx / m.tiles_x) * kTY;
 }
-__device__ __forceinline__ void tma_range(int nz, int &k0, int &k1)
+__device__ __forceinline__ void tma_range_at(int nz, int bz, int gz, int &k0, int &k1)
 {
-    const int kc = (nz + 1 + gridDim.z - 1) / gridDim.z;
-    k0 = blockIdx.z * kc;
+    const int kc = (nz + 1 + gz - 1) / gz;
+    k0 = bz * kc;
     k1 = min(k0 + kc, nz + 1);
 }
+__device__ __forceinline__ void tma_tile(const ColMap &m, int &i0, int &j0) { tma_tile_at(m, blockIdx.x, i0, j0); }
+__device__ __forceinline__ void tma_range(int nz, int &k0, int &k1) { tma_range_at(nz, blockIdx.z, gridDim.z, k0, k1); }
 __device__ __forceinline__ TmaSmem &tma_smem()
 {
     extern __shared__ __align__(128) unsigned char tma_raw[];

@@ -26,7 +26,8 @@ FORM_CCDC, FORM_CCGD = 0, 1
 EXPORTS = ["mt3d_version", "mt3d_device_count", "mt3d_create", "mt3d_destroy", "mt3d_set_control", "mt3d_update_cond",
            "mt3d_get_cond", "mt3d_compute_bc", "mt3d_compute_bc_device", "mt3d_update_freq", "mt3d_set_formulation", "mt3d_set_restart", "mt3d_sizes", "mt3d_interior_index", "mt3d_mult_aii",
            "mt3d_mult_aii_device_noalloc", "mt3d_bicg", "mt3d_fwdsolve",
-           "mt3d_fwdsolve_batch", "mt3d_fwdsolve_batch_device", "mt3d_set_stream", "mt3d_set_wait_limit", "mt3d_set_fused",
+           "mt3d_fwdsolve_batch", "mt3d_fwdsolve_batch_device", "mt3d_fwdsolve_multi",
+           "mt3d_fwdsolve_multi_device", "mt3d_set_stream", "mt3d_set_wait_limit", "mt3d_set_fused",
            "mt3d_apply_kernel", "mt3d_profile",
            "mt3d_kernel_time", "mt3d_get_diag", "mt3d_get_batch_diag", "mt3d_pmult_t", "mt3d_impedance", "mt3d_impedance_device", "mt3d_lmult_t", "mt3d_lmult_t_device", "mt3d_jmult_t", "mt3d_jmult_t_device", "mt3d_write_soln", "mt3d_read_soln", "mt3d_read_soln_header", "mt3d_launch_counter", "mt3d_alloc_counter",
            "mt3d_last_error"]
@@ -78,6 +79,9 @@ def load(path: str = LIB_PATH):
     L.mt3d_fwdsolve_batch_device.argtypes = [P, I, D, IP, C.c_void_p, C.c_void_p, C.c_void_p, IP]
     L.mt3d_set_stream.argtypes = [P, C.c_void_p]
     L.mt3d_set_wait_limit.argtypes = [P, I]
+    PP = C.POINTER(C.c_void_p)
+    for name in ("mt3d_fwdsolve_multi", "mt3d_fwdsolve_multi_device"):
+        getattr(L, name).argtypes = [I, C.POINTER(P), IP, PP, PP, PP, PP, PP, PP, IP]
     L.mt3d_set_fused.argtypes = [P, I]
     L.mt3d_jmult_t.argtypes = [P, C.c_double, I, D, D, D, D, D, D, D]
     L.mt3d_jmult_t_device.argtypes = [P, C.c_double, I, D, D, C.c_void_p, D, D, C.c_void_p, C.c_void_p]
@@ -122,6 +126,8 @@ class Solver:
                                 C.byref(self.h))
         if rc:
             raise MT3DError(rc, self._err(None))
+        self.control = dict(IterPerDivCor=40, MaxDivCor=20, MaxIterDivCor=100, tolEMfwd=1e-7, tolEMadj=1e-7,
+                            tolDivCor=1e-5, solver=SOLVER_BICG, precision=PREC_FP64)
         nE, nEi, nN = C.c_int64(), C.c_int64(), C.c_int64()
         self.L.mt3d_sizes(self.h, C.byref(nE), C.byref(nEi), C.byref(nN))
         self.nE, self.nEi, self.nN = nE.value, nEi.value, nN.value
@@ -151,6 +157,9 @@ class Solver:
                     tolDivCor=1e-5, solver=SOLVER_BICG, precision=PREC_FP64):
         self._check(self.L.mt3d_set_control(self.h, IterPerDivCor, MaxDivCor, MaxIterDivCor, tolEMfwd, tolEMadj,
                                             tolDivCor, solver, precision))
+        self.control = dict(IterPerDivCor=IterPerDivCor, MaxDivCor=MaxDivCor, MaxIterDivCor=MaxIterDivCor,
+                            tolEMfwd=tolEMfwd, tolEMadj=tolEMadj, tolDivCor=tolDivCor, solver=solver,
+                            precision=precision)
 
     def set_formulation(self, formulation):
         self._check(self.L.mt3d_set_formulation(self.h, int(formulation)))
@@ -385,6 +394,52 @@ class Solver:
         out = np.zeros(g.nx * g.ny * g.nzEarth)
         self._check(self.L.mt3d_pmult_t(self.h, npol, _d(e0), _d(ea), _d(m0), _d(out)))
         return out
+
+
+def fwdsolve_multi(solvers, omegas, e, trans=None, bc=None, src=None, zchunks=None, device=False):
+    """mt3d_fwdsolve_multi over several handles (one grid each).
+
+    omegas, trans: per handle, arrays of its right-hand sides' angular
+    frequencies and transposition flags.  e, bc, src: per handle, either host
+    arrays [nrhs, nE] (complex128, e is updated in place) or, with
+    device=True, device addresses (ints); bc / src (or entries) may be None.
+    zchunks: per-handle node-plane chunk counts of the stencil blocks (None
+    or 0: the default).  Returns (statuses per handle, worst status)."""
+    L = load()
+    nh = len(solvers)
+    hs = (C.c_void_p * nh)(*[s.h for s in solvers])
+    om = [np.ascontiguousarray(o, np.float64) for o in omegas]
+    nr = (C.c_int * nh)(*[o.size for o in om])
+    tr = [np.zeros(o.size, np.int32) if trans is None or trans[i] is None else np.ascontiguousarray(trans[i], np.int32)
+          for i, o in enumerate(om)]
+    st = [np.zeros(o.size, np.int32) for o in om]
+
+    def ptrs(xs, kind):
+        out = (C.c_void_p * nh)()
+        for i in range(nh):
+            x = None if xs is None else xs[i]
+            if x is None:
+                out[i] = None
+            elif device:
+                out[i] = int(x)
+            else:
+                assert x.dtype == kind and x.flags.c_contiguous
+                out[i] = x.ctypes.data
+        return out
+
+    if not device:
+        for i, x in enumerate(e):
+            assert x.shape == (om[i].size, solvers[i].nE)
+    ap = lambda arrs: (C.c_void_p * nh)(*[a.ctypes.data for a in arrs])
+    zc = None if zchunks is None else (C.c_int * nh)(*[int(z) for z in zchunks])
+    fn = L.mt3d_fwdsolve_multi_device if device else L.mt3d_fwdsolve_multi
+    rc = fn(nh, hs, nr, ap(om), ap(tr), ptrs(bc, np.complex128), ptrs(src, np.complex128), ptrs(e, np.complex128),
+            ap(st), zc)
+    if rc not in (0, 1):
+        buf = C.create_string_buffer(512)
+        L.mt3d_last_error(None, buf, 512)
+        raise MT3DError(rc, buf.value.decode())
+    return st, rc
 
 
 def device_count() -> int:

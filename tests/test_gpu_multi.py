@@ -1,0 +1,100 @@
+"""Multi-grid batches (mt3d_fwdsolve_multi): three models of uneven size solved
+in one call, the FP32 iterations of all grids sharing their launches, against
+the same right-hand sides solved per grid (mt3d_fwdsolve_batch).
+
+Both reach the FP64 tolerance 1e-7; their fields agree to 1e-5 (relative
+2-norm on the edges where the field is unique), the bound of the other
+mixed-precision parity tests.  Also: the device-memory entry gives the host
+entry's fields bit for bit, and the chunk tuner returns a valid choice and
+caches it.
+"""
+import numpy as np
+import pytest
+
+from helpers import earth_mask, random_model, relerr
+from mt3d import bc as mbc
+from mt3d import capi, models
+
+pytestmark = pytest.mark.gpu
+
+
+def _problems():
+    shapes = [(14, 14, 4, 10), (20, 24, 5, 13), (28, 18, 6, 16)]
+    out = []
+    for k, (nx, ny, na, ne) in enumerate(shapes):
+        g = models.make_grid(nx, ny, na, ne, core=400.0, n_pad=3, pad_growth=1.5, air_first=60.0, air_growth=2.0,
+                             earth_first=60.0, earth_growth=1.25)
+        m = random_model(g, seed=20 + k)
+        om = 2 * np.pi * np.array([0.05, 0.05, 2.0, 2.0, 2.0])
+        bcs = [mbc.boundary_1d(m, om[0], 1), mbc.boundary_1d(m, om[1], 2), mbc.boundary_1d(m, om[2], 1),
+               mbc.boundary_1d(m, om[3], 2), np.zeros(g.n_edges, complex)]
+        rng = np.random.default_rng(k)
+        src = np.zeros((5, g.n_edges), complex)
+        em = earth_mask(g, m)
+        src[4] = np.where(em, rng.standard_normal(g.n_edges) + 1j * rng.standard_normal(g.n_edges), 0) * 1e-3
+        tr = np.array([0, 0, 0, 0, 1], np.int32)
+        out.append((g, m, om, np.stack(bcs), src, tr))
+    return out
+
+
+def _solver(g, m):
+    s = capi.Solver(g)
+    s.set_formulation(capi.FORM_CCGD)
+    s.set_restart(0)
+    s.update_cond(m.m_earth, m.air_cond)
+    s.set_control(IterPerDivCor=150, MaxDivCor=40, precision=capi.PREC_MIXED)
+    return s
+
+
+@pytest.fixture(scope="module")
+def mprob(cuda):
+    probs = _problems()
+    return probs, [_solver(g, m) for g, m, *_ in probs]
+
+
+def test_multi_grid_batch_matches_per_grid_solves(mprob):
+    probs, ss = mprob
+    es = [np.zeros((5, g.n_edges), complex) for g, *_ in probs]
+    st, rc = capi.fwdsolve_multi(ss, [p[2] for p in probs], es, trans=[p[5] for p in probs],
+                                 bc=[p[3] for p in probs], src=[p[4] for p in probs])
+    assert rc == 0 and all(np.all(x == 0) for x in st)
+    for (g, m, om, bc, src, tr), s, e in zip(probs, ss, es):
+        it, rr = s.batch_diagnostics(5)
+        assert np.all(rr <= 1e-7)
+        ref, st1, rc1 = s.fwdsolve_batch(om, trans=tr, bc=bc, src=src)
+        assert rc1 == 0
+        em = earth_mask(g, m)
+        for r in range(5):
+            assert relerr(e[r][em], ref[r][em]) < 1e-5, (g.nx, r)
+
+
+def test_multi_device_entry_matches_host_entry(mprob):
+    import torch
+    probs, ss = mprob
+    es = [np.zeros((5, g.n_edges), complex) for g, *_ in probs]
+    capi.fwdsolve_multi(ss, [p[2] for p in probs], es, trans=[p[5] for p in probs], bc=[p[3] for p in probs],
+                        src=[p[4] for p in probs])
+    dbc = [torch.from_numpy(p[3]).cuda() for p in probs]
+    dsrc = [torch.from_numpy(p[4]).cuda() for p in probs]
+    de = [torch.zeros((5, g.n_edges), dtype=torch.complex128, device="cuda") for g, *_ in probs]
+    torch.cuda.synchronize()
+    st, rc = capi.fwdsolve_multi(ss, [p[2] for p in probs], [x.data_ptr() for x in de], trans=[p[5] for p in probs],
+                                 bc=[x.data_ptr() for x in dbc], src=[x.data_ptr() for x in dsrc], device=True)
+    torch.cuda.synchronize()
+    assert rc == 0
+    for e, d in zip(es, de):
+        assert np.array_equal(d.cpu().numpy(), e)
+
+
+def test_chunk_tuner_returns_and_caches_a_choice(mprob, tmp_path):
+    import torch
+    from mt3d import tune
+    probs, ss = mprob
+    dbc = [torch.from_numpy(p[3]).cuda() for p in probs]
+    de = [torch.zeros((5, g.n_edges), dtype=torch.complex128, device="cuda") for g, *_ in probs]
+    path = str(tmp_path / "tune.json")
+    zch = tune.tune(ss, [p[2] for p in probs], [x.data_ptr() for x in de], [x.data_ptr() for x in dbc],
+                    None, [np.zeros(5, np.int32)] * 3, torch.cuda.synchronize, cache_path=path, iters=20, reps=1)
+    assert len(zch) == 3 and all(z in tune.candidates(s.grid.nz) for z, s in zip(zch, ss))
+    assert tune.tune(ss, [p[2] for p in probs], None, None, None, None, None, cache_path=path) == zch
+    assert all(s.control["IterPerDivCor"] == 150 for s in ss)
