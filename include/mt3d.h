@@ -59,8 +59,12 @@ typedef enum {
  * preconditioner.  MT3D_SOLVER_COCG: Bi-CG specialised to the complex-
  * symmetric operator (conjugate-orthogonal CG, one operator application per
  * iteration) with the vertical-line (z-line) tridiagonal preconditioner.
- * MT3D_SOLVER_BICG_ZLINE: BiCGStab with the z-line preconditioner. */
-enum { MT3D_SOLVER_BICG = 1, MT3D_SOLVER_COCG = 2, MT3D_SOLVER_BICG_ZLINE = 3 };
+ * MT3D_SOLVER_BICG_ZLINE: BiCGStab with the z-line preconditioner.
+ * MT3D_SOLVER_QMR: QMR without look-ahead, the reference's default solver
+ * (QMR, f90/3D_MT/FWD/solver.f90:122-343; solver_name "QMR",
+ * f90/3D_MT/FWD/EMsolve3D.f90:70), with the diagonal preconditioner as M1
+ * and M2 = I; FP64 only. */
+enum { MT3D_SOLVER_BICG = 1, MT3D_SOLVER_COCG = 2, MT3D_SOLVER_BICG_ZLINE = 3, MT3D_SOLVER_QMR = 4 };
 enum { MT3D_PREC_FP64 = 0, MT3D_PREC_MIXED = 1 };
 
 /* Library version string. */

@@ -107,8 +107,13 @@ int mt3d_set_control(mt3d_handle h, int IterPerDivCor, int MaxDivCor, int MaxIte
         h->s.last_error = "mt3d_set_control: iteration counts must be >= 1 and tolerances > 0";
         return MT3D_INVALID_ARGUMENT;
     }
-    if (solver != MT3D_SOLVER_BICG && solver != MT3D_SOLVER_COCG && solver != MT3D_SOLVER_BICG_ZLINE) {
+    if (solver != MT3D_SOLVER_BICG && solver != MT3D_SOLVER_COCG && solver != MT3D_SOLVER_BICG_ZLINE &&
+        solver != MT3D_SOLVER_QMR) {
         h->s.last_error = "mt3d_set_control: unknown solver";
+        return MT3D_INVALID_ARGUMENT;
+    }
+    if (solver == MT3D_SOLVER_QMR && precision != MT3D_PREC_FP64) {
+        h->s.last_error = "mt3d_set_control: QMR runs in FP64 (MT3D_PREC_FP64)";
         return MT3D_INVALID_ARGUMENT;
     }
     if (precision != MT3D_PREC_FP64 && precision != MT3D_PREC_MIXED) {

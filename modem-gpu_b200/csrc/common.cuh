@@ -222,6 +222,17 @@ struct BicgState {
     int pad;
 };
 
+// QMR without look-ahead (f90/3D_MT/FWD/solver.f90:122-343), one per
+// right-hand side; the names are the reference's
+struct QmrState {
+    cd rho, rho1, psi, delta, epsil, beta, eta, thet, thet1, gamm, gamm1, tm2, pde, rde;
+    double bnorm, tol;
+    int iter;    // the reference's counter (1 before the first iteration)
+    int maxit;
+    int status;  // KStatus
+    int zero;    // zero right-hand side: zero solution
+};
+
 struct PcgState {
     cd delta, deltaOld, alpha, beta;
     double bnorm, rnorm, tol;

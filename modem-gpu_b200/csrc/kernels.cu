@@ -430,6 +430,296 @@ template <typename T> __global__ void __launch_bounds__(kThreads) kb_finish(KArg
 }
 
 // ---------------------------------------------------------------------------
+// QMR without look-ahead (f90/3D_MT/FWD/solver.f90:122-343, Barrett et al.'s
+// template with the complex changes of the reference), FP64, with the
+// diagonal preconditioner as M1 and M2 = I, so Z = WT, YT = Y and
+// ZT = D^-H Z.  The vectors: R = r, VT = rt, Y = ph, V = v, WT = s, W = w,
+// P = p, Q = q, PT = t, D = d, S = sh, x = x0.  Each right-hand side's scalars
+// live in QmrState; the kernels run the reference's statements in order:
+//   kq_vw   V = VT / RHO, W = WT / PSI, Y = Y / RHO, DELTA = (Z, Y)
+//   kq_pq   P = Y + PDE P, Q = D^-H W + RDE Q
+//   kq_pt   PT = A P, EPSIL = (Q, PT), BETA
+//   kq_vt   VT = PT - BETA V, Y = D^-1 VT, RHO
+//   kq_wt   WT = A^H Q - conj(BETA) W, PSI, THET, GAMM, ETA
+//   kq_xr   D, S, x += D, R -= S, ||R||, iteration bookkeeping
+// (A^H: the conjugate-transposed operator; in the grad-div formulation its
+// grad-div part is GD^T, as Mult_Aii(adjt) forms it.)
+// ---------------------------------------------------------------------------
+__device__ inline cd cd_sqrt(cd z)
+{
+    // principal square root from |z|: sqrt((|z| + x)/2) + i sign(y) sqrt((|z| - x)/2)
+    const double m = hypot(z.re, z.im);
+    const double re = sqrt(0.5 * (m + z.re)), im = sqrt(fmax(0.0, 0.5 * (m - z.re)));
+    return {re, z.im < 0.0 ? -im : im};
+}
+__device__ inline cd cd_add(cd a, cd b) { return {a.re + b.re, a.im + b.im}; }
+__device__ inline cd cd_neg(cd a) { return {-a.re, -a.im}; }
+__device__ inline cd cd_conj(cd a) { return {a.re, -a.im}; }
+__device__ inline cd cd_real(double x) { return {x, 0.0}; }
+__device__ __forceinline__ double2 cdm(cd c, double2 v) { return make_double2(c.re * v.x - c.im * v.y, c.re * v.y + c.im * v.x); }
+
+// conj(a) b accumulated
+template <int N> __device__ __forceinline__ void dotc_acc(double (&u)[N], int o, double2 a, double2 b)
+{
+    u[o] += a.x * b.x + a.y * b.y;
+    u[o + 1] += a.x * b.y - a.y * b.x;
+}
+
+// D^-1 v (adj = 0) or D^-H v (adj = 1) at an interior edge
+__device__ __forceinline__ double2 qmr_jac(const KArgs<double> &a, const EdgeIdx &q, int r, int e, double2 v, int adj)
+{
+    const double wmu = rhs_wmu(a, r), sg = a.sigma[e];
+    const double dt = dterm_of(a.g, q, wmu, sg);
+    return jacobi(a.g, q, adj ? -dt : dt, v, a.gd ? gd_diag(a, q, sg) : 0.0);
+}
+
+// R = b - A x, VT = R, Y = D^-1 R, WT = R; ||b||, ||R||, RHO = ||Y||, PSI = ||R||
+__global__ void __launch_bounds__(kThreads) kq_init(KArgs<double> a)
+{
+    const int r = blockIdx.y;
+    if (!a.ost[r].active) return;
+    const size_t off = (size_t)r * a.stride;
+    const Geo<double> &g = a.g;
+    const double wmu = rhs_wmu(a, r);
+    double u[4] = {0.0, 0.0, 0.0, 0.0};
+    const int end = min((blockIdx.x + 1) * a.chunk, g.nE);
+    for (int e = chunk_begin(a.chunk); e < end; e += kThreads) {
+        EdgeIdx q = edge_decode(g, e);
+        double2 res = make_double2(0.0, 0.0), y = res;
+        if (edge_interior(g, q)) {
+            double2 ax = stencil(g, a.x0 + off, q, dterm_of(g, q, wmu, a.sigma[e]));
+            if (a.gd) ax = cadd(ax, gd_edge(g, q, a.phi + (size_t)r * g.nN));
+            const double2 bb = a.b[off + e];
+            res = csub(bb, ax);
+            y = qmr_jac(a, q, r, e, res, 0);
+            u[0] += bb.x * bb.x + bb.y * bb.y;
+            u[1] += res.x * res.x + res.y * res.y;
+            u[2] += y.x * y.x + y.y * y.y;
+        }
+        a.r[off + e] = res;
+        a.rt[off + e] = res;
+        a.s[off + e] = res;
+        a.ph[off + e] = y;
+    }
+    double tot[4];
+    if (block_reduce_last<4>(u, a.parts, a.cnt, r, blockIdx.x, gridDim.x, tot) && threadIdx.x == 0) {
+        QmrState &st = a.qst[r];
+        st = QmrState{};
+        st.maxit = a.maxit;
+        st.tol = a.ost[r].tol;
+        st.bnorm = sqrt(tot[0]);
+        const double rnorm = sqrt(tot[1]);
+        st.iter = 1;
+        st.rho = cd_real(sqrt(tot[2]));
+        st.psi = cd_real(rnorm);
+        st.gamm = cd_real(1.0);
+        st.eta = cd_real(-1.0);
+        double *rerr = a.rerr + (size_t)r * a.rerr_stride;
+        if (!isfinite(st.bnorm)) {
+            st.status = KS_NAN;
+        } else if (st.bnorm == 0.0) {
+            st.status = KS_CONVERGED;
+            st.zero = 1;
+            rerr[0] = 0.0;
+        } else {
+            rerr[0] = rnorm / st.bnorm;
+            st.status = (rerr[0] > st.tol && st.iter < st.maxit) ? KS_RUNNING : KS_CONVERGED;
+            if (st.status == KS_RUNNING && (cd_zero(st.rho) || cd_zero(st.psi))) st.status = KS_BREAKDOWN;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) kq_vw(KArgs<double> a)
+{
+    const int r = blockIdx.y;
+    QmrState &st = a.qst[r];
+    if (st.status != KS_RUNNING || !a.ost[r].active) return;
+    const size_t off = (size_t)r * a.stride;
+    const cd ri = cd_div(cd_real(1.0), st.rho), pi = cd_div(cd_real(1.0), st.psi);
+    double u[2] = {0.0, 0.0};
+    const int end = min((blockIdx.x + 1) * a.chunk, a.g.nE);
+    for (int e = chunk_begin(a.chunk); e < end; e += kThreads) {
+        const double2 v = cdm(ri, a.rt[off + e]), w = cdm(pi, a.s[off + e]), y = cdm(ri, a.ph[off + e]);
+        a.v[off + e] = v;
+        a.w[off + e] = w;
+        a.ph[off + e] = y;
+        dotc_acc(u, 0, w, y);  // DELTA = (Z, Y), Z = W
+    }
+    double tot[2];
+    if (block_reduce_last<2>(u, a.parts, a.cnt, r, blockIdx.x, gridDim.x, tot) && threadIdx.x == 0) {
+        st.delta = {tot[0], tot[1]};
+        if (!cd_finite(st.delta)) { st.status = KS_NAN; return; }
+        if (cd_zero(st.delta)) { st.status = KS_BREAKDOWN; return; }
+        if (st.iter > 1) {
+            const cd de = cd_div(st.delta, st.epsil);
+            st.pde = cd_neg(cd_mul(st.psi, de));
+            st.rde = cd_neg(cd_mul(st.rho, cd_conj(de)));
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) kq_pq(KArgs<double> a)
+{
+    const int r = blockIdx.y;
+    const QmrState &st = a.qst[r];
+    if (st.status != KS_RUNNING || !a.ost[r].active) return;
+    const size_t off = (size_t)r * a.stride;
+    const bool first = st.iter == 1;
+    const int end = min((blockIdx.x + 1) * a.chunk, a.g.nE);
+    for (int e = chunk_begin(a.chunk); e < end; e += kThreads) {
+        const EdgeIdx q = edge_decode(a.g, e);
+        double2 zt = make_double2(0.0, 0.0);
+        if (edge_interior(a.g, q)) zt = qmr_jac(a, q, r, e, a.w[off + e], 1);
+        const double2 y = a.ph[off + e];
+        if (first) {
+            a.p[off + e] = y;
+            a.q[off + e] = zt;
+        } else {
+            a.p[off + e] = cadd(y, cdm(st.pde, a.p[off + e]));
+            a.q[off + e] = cadd(zt, cdm(st.rde, a.q[off + e]));
+        }
+    }
+}
+
+// PT = A P (which = 0): EPSIL = (Q, PT), BETA; WT = A^H Q - conj(BETA) W
+// (which = 1): PSI and the rotation scalars
+__global__ void __launch_bounds__(kThreads) kq_apply(KArgs<double> a, int which)
+{
+    const int r = blockIdx.y;
+    QmrState &st = a.qst[r];
+    if (st.status != KS_RUNNING || !a.ost[r].active) return;
+    const size_t off = (size_t)r * a.stride;
+    const Geo<double> &g = a.g;
+    const double wmu = (which ? 1.0 : -1.0) * a.ost[r].omega * kMu0;
+    const double2 *x = (which ? a.q : a.p) + off;
+    const double2 *phi = a.phi + (size_t)r * g.nN;
+    const cd cb = cd_conj(st.beta);
+    double u[2] = {0.0, 0.0};
+    const int end = min((blockIdx.x + 1) * a.chunk, g.nE);
+    for (int e = chunk_begin(a.chunk); e < end; e += kThreads) {
+        EdgeIdx q = edge_decode(g, e);
+        double2 out = make_double2(0.0, 0.0);
+        if (edge_interior(g, q)) {
+            const double sg = a.sigma[e];
+            out = stencil(g, x, q, dterm_of(g, q, wmu, sg));
+            if (a.gd) out = cadd(out, which ? gd_edge_t(a, q, sg, phi) : gd_edge(g, q, phi));
+            if (which == 0) {
+                dotc_acc(u, 0, a.q[off + e], out);
+            } else {
+                out = csub(out, cdm(cb, a.w[off + e]));
+                u[0] += out.x * out.x + out.y * out.y;
+            }
+        }
+        (which ? a.s : a.t)[off + e] = out;
+    }
+    double tot[2];
+    if (block_reduce_last<2>(u, a.parts, a.cnt, r, blockIdx.x, gridDim.x, tot) && threadIdx.x == 0) {
+        if (which == 0) {
+            st.epsil = {tot[0], tot[1]};
+            if (!cd_finite(st.epsil)) { st.status = KS_NAN; return; }
+            if (cd_zero(st.epsil)) { st.status = KS_BREAKDOWN; return; }
+            st.beta = cd_div(st.epsil, st.delta);
+            if (cd_zero(st.beta)) st.status = KS_BREAKDOWN;
+        } else {
+            st.psi = cd_real(sqrt(tot[0]));
+            if (st.iter > 1) st.thet1 = st.thet;
+            st.thet = cd_div(st.rho, cd_mul(st.gamm, cd_real(hypot(st.beta.re, st.beta.im))));
+            st.gamm1 = st.gamm;
+            st.gamm = cd_div(cd_real(1.0), cd_sqrt(cd_add(cd_real(1.0), cd_mul(st.thet, st.thet))));
+            if (cd_zero(st.gamm) || !cd_finite(st.gamm)) { st.status = cd_zero(st.gamm) ? KS_MAXIT : KS_NAN; return; }
+            // ETA = -ETA RHO1 GAMM^2 / (BETA GAMM1^2)
+            const cd num = cd_mul(cd_neg(st.eta), cd_mul(st.rho1, cd_mul(st.gamm, st.gamm)));
+            st.eta = cd_div(num, cd_mul(st.beta, cd_mul(st.gamm1, st.gamm1)));
+            st.tm2 = cd_mul(cd_mul(st.thet1, st.thet1), cd_mul(st.gamm, st.gamm));
+        }
+    }
+}
+
+// VT = PT - BETA V, Y = D^-1 VT, RHO = ||Y||
+__global__ void __launch_bounds__(kThreads) kq_vt(KArgs<double> a)
+{
+    const int r = blockIdx.y;
+    QmrState &st = a.qst[r];
+    if (st.status != KS_RUNNING || !a.ost[r].active) return;
+    const size_t off = (size_t)r * a.stride;
+    double u[1] = {0.0};
+    const int end = min((blockIdx.x + 1) * a.chunk, a.g.nE);
+    for (int e = chunk_begin(a.chunk); e < end; e += kThreads) {
+        const EdgeIdx q = edge_decode(a.g, e);
+        const double2 vt = csub(a.t[off + e], cdm(st.beta, a.v[off + e]));
+        double2 y = make_double2(0.0, 0.0);
+        if (edge_interior(a.g, q)) y = qmr_jac(a, q, r, e, vt, 0);
+        a.rt[off + e] = vt;
+        a.ph[off + e] = y;
+        u[0] += y.x * y.x + y.y * y.y;
+    }
+    double tot[1];
+    if (block_reduce_last<1>(u, a.parts, a.cnt, r, blockIdx.x, gridDim.x, tot) && threadIdx.x == 0) {
+        st.rho1 = st.rho;
+        st.rho = cd_real(sqrt(tot[0]));
+    }
+}
+
+// D = ETA P (+ TM2 D), S = ETA PT (+ TM2 S), x += D, R -= S; ||R||
+__global__ void __launch_bounds__(kThreads) kq_xr(KArgs<double> a)
+{
+    const int r = blockIdx.y;
+    QmrState &st = a.qst[r];
+    if (st.status != KS_RUNNING || !a.ost[r].active) return;
+    const size_t off = (size_t)r * a.stride;
+    const bool first = st.iter == 1;
+    double u[1] = {0.0};
+    const int end = min((blockIdx.x + 1) * a.chunk, a.g.nE);
+    for (int e = chunk_begin(a.chunk); e < end; e += kThreads) {
+        double2 d = cdm(st.eta, a.p[off + e]), sv = cdm(st.eta, a.t[off + e]);
+        if (!first) {
+            d = cadd(d, cdm(st.tm2, a.d[off + e]));
+            sv = cadd(sv, cdm(st.tm2, a.sh[off + e]));
+        }
+        a.d[off + e] = d;
+        a.sh[off + e] = sv;
+        a.x0[off + e] = cadd(a.x0[off + e], d);
+        const double2 rn = csub(a.r[off + e], sv);
+        a.r[off + e] = rn;
+        u[0] += rn.x * rn.x + rn.y * rn.y;
+    }
+    double tot[1];
+    if (block_reduce_last<1>(u, a.parts, a.cnt, r, blockIdx.x, gridDim.x, tot) && threadIdx.x == 0) {
+        const double rnorm = sqrt(tot[0]);
+        st.iter += 1;
+        double *rerr = a.rerr + (size_t)r * a.rerr_stride;
+        rerr[st.iter - 1] = rnorm / st.bnorm;
+        if (!isfinite(rnorm)) { st.status = KS_NAN; return; }
+        if (!(rerr[st.iter - 1] > st.tol)) { st.status = KS_CONVERGED; return; }
+        if (st.iter >= st.maxit) { st.status = KS_MAXIT; return; }
+        if (cd_zero(st.rho) || cd_zero(st.psi)) st.status = KS_BREAKDOWN;
+    }
+}
+
+// end of a QMR call: x = 0 for a zero right-hand side; the statuses in the
+// BicgState the outer loop reads (iter = the reference's niter; the last
+// iterate is the returned one)
+__global__ void __launch_bounds__(kThreads) kq_finish(KArgs<double> a)
+{
+    const int r = blockIdx.y;
+    if (!a.ost[r].active) return;
+    const QmrState &st = a.qst[r];
+    const size_t off = (size_t)r * a.stride;
+    if (st.zero) {
+        const int end = min((blockIdx.x + 1) * a.chunk, a.g.nE);
+        for (int e = chunk_begin(a.chunk); e < end; e += kThreads) a.x0[off + e] = make_double2(0.0, 0.0);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        BicgState &b = a.st[r];
+        b.status = st.status == KS_CONVERGED ? KS_CONVERGED : st.status == KS_RUNNING ? KS_MAXIT : st.status;
+        b.iter = st.iter;
+        b.imin = st.iter;
+        b.xbest = 0;
+        b.xcur = 0;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // divergence correction (SdivCorr, f90/3D_MT/FWD/EMsolve3D.f90:403-492) with
 // PCG (f90/3D_MT/FWD/solver.f90:40-118) on DivCgrad and a diagonal
 // preconditioner, FP64 throughout.
@@ -1182,6 +1472,31 @@ template <typename T> void launch_bicg_finish(const KArgs<T> &a, int nrhs, cudaS
     counted(1);
     kb_finish<T><<<dim3(a.nblk, nrhs), kThreads, 0, s>>>(a);
 }
+void launch_qmr_init(const KArgs<double> &a, int nrhs, cudaStream_t s)
+{
+    if (a.gd) launch_gd_phi(a, a.x0, a.phi, 0, nrhs, s);
+    counted(1);
+    kq_init<<<dim3(a.nblk, nrhs), kThreads, 0, s>>>(a);
+}
+void launch_qmr_iter(const KArgs<double> &a, int nrhs, cudaStream_t s)
+{
+    const dim3 grid(a.nblk, nrhs);
+    counted(6);
+    kq_vw<<<grid, kThreads, 0, s>>>(a);
+    kq_pq<<<grid, kThreads, 0, s>>>(a);
+    if (a.gd) launch_gd_phi(a, a.p, a.phi, 0, nrhs, s);
+    kq_apply<<<grid, kThreads, 0, s>>>(a, 0);
+    kq_vt<<<grid, kThreads, 0, s>>>(a);
+    if (a.gd) launch_gd_phi(a, a.q, a.phi, 2, nrhs, s);
+    kq_apply<<<grid, kThreads, 0, s>>>(a, 1);
+    kq_xr<<<grid, kThreads, 0, s>>>(a);
+}
+void launch_qmr_finish(const KArgs<double> &a, int nrhs, cudaStream_t s)
+{
+    counted(1);
+    kq_finish<<<dim3(a.nblk, nrhs), kThreads, 0, s>>>(a);
+}
+
 template void launch_apply<double>(const KArgs<double> &, const double2 *, double2 *, int, int, cudaStream_t, int);
 template void launch_apply<float>(const KArgs<float> &, const float2 *, float2 *, int, int, cudaStream_t, int);
 template void launch_bicg_init<double>(const KArgs<double> &, int, cudaStream_t);

@@ -66,6 +66,10 @@ template <typename T> struct KArgs {
     // profiling: the staged stencil kernels count one sweep per active
     // right-hand side and launch here (nullptr when not profiling)
     unsigned long long *sweeps;
+    // QMR: scalar state and the vectors of the reference's routine that
+    // BiCGStab has no place for
+    QmrState *qst;
+    C2<T> *q, *w, *d;
 };
 
 // arguments of the divergence-correction kernels (FP64)
@@ -176,6 +180,11 @@ template <typename T> void launch_bicg_init(const KArgs<T> &a, int nrhs, cudaStr
 template <typename T> void launch_bicg_iter(const KArgs<T> &a, int nrhs, cudaStream_t s, cudaEvent_t *ev = nullptr,
                                             const ColArgs<T> *pc = nullptr);
 template <typename T> void launch_bicg_finish(const KArgs<T> &a, int nrhs, cudaStream_t s);
+// QMR (FP64, diagonal preconditioner M1 = D, M2 = I) in the BiCGStab call's
+// place: start, one iteration (six launches), end (statuses into BicgState)
+void launch_qmr_init(const KArgs<double> &a, int nrhs, cudaStream_t s);
+void launch_qmr_iter(const KArgs<double> &a, int nrhs, cudaStream_t s);
+void launch_qmr_finish(const KArgs<double> &a, int nrhs, cudaStream_t s);
 template <typename T> void launch_gd_phi(const KArgs<T> &a, const C2<T> *x, C2<T> *phi, int mode, int nrhs, cudaStream_t s);
 template <typename T> void launch_gd_add(const KArgs<T> &a, C2<T> *b, const C2<T> *phi, int nrhs, cudaStream_t s);
 void launch_norm_b(const KArgs<double> &a, int nrhs, cudaStream_t s);

@@ -394,7 +394,7 @@ int Solver::ensure_workspace(int nrhs, int precision)
                  e32 = (size_t)nrhs * (padded ? (size_t)pl_.len() : (size_t)nE) * sizeof(float2);
     const size_t n64 = (size_t)nrhs * nN * sizeof(double2);
     // release everything first so a precision change does not hold both sets
-    DevBuf *all[] = {&w.b, &w.X, &w.x1, &w.r, &w.rt, &w.p, &w.v, &w.ph, &w.s, &w.sh, &w.t, &w.bc, &w.tmp,
+    DevBuf *all[] = {&w.qst, &w.b, &w.X, &w.x1, &w.r, &w.rt, &w.p, &w.v, &w.ph, &w.s, &w.sh, &w.t, &w.bc, &w.tmp,
                      &w.f_b, &w.f_x0, &w.f_x1, &w.f_r, &w.f_rt, &w.f_p, &w.f_v, &w.f_ph, &w.f_s, &w.f_sh, &w.f_t,
                      &w.px, &w.pr, &w.pp, &w.pq, &w.phi0, &w.zm, &w.zc, &w.f_zm, &w.f_zc, &w.phi64, &w.phi32, &w.jinv64, &w.jinv32};
     for (DevBuf *d : all) d->release();
@@ -403,7 +403,7 @@ int Solver::ensure_workspace(int nrhs, int precision)
     if (precision == 0) {
         DevBuf *v64[] = {&w.x1, &w.r, &w.rt, &w.p, &w.v, &w.ph, &w.s, &w.sh, &w.t};
         for (DevBuf *d : v64) err |= d->alloc(e64);
-        if (ctl.solver == 3) err |= w.zm.alloc(e64) | w.zc.alloc(e64);
+        if (ctl.solver == 3 || ctl.solver == 4) err |= w.zm.alloc(e64) | w.zc.alloc(e64);
         if (ctl.solver == 1) err |= w.jinv64.alloc(e64);
     } else {
         DevBuf *v32[] = {&w.f_b, &w.f_x0, &w.f_x1, &w.f_r, &w.f_rt, &w.f_p, &w.f_v, &w.f_ph, &w.f_s, &w.f_sh, &w.f_t};
@@ -427,7 +427,7 @@ int Solver::ensure_workspace(int nrhs, int precision)
     const int nb = std::max({blocks_for(nE, c), blocks_for(nN, c), cm.tiles * std::max(1, (nz + 1) / 8),
                              1184});
     err |= w.bst.alloc(nrhs * sizeof(BicgState)) | w.pst.alloc(nrhs * sizeof(PcgState)) |
-           w.ost.alloc(nrhs * sizeof(OuterState));
+           w.ost.alloc(nrhs * sizeof(OuterState)) | w.qst.alloc(nrhs * sizeof(QmrState));
     err |= w.parts.alloc((size_t)nrhs * nb * kMaxParts * sizeof(double)) | w.cnt.alloc(3 * nrhs * sizeof(unsigned));
     err |= w.rerr.alloc((size_t)nrhs * rlen * sizeof(double));
     err |= w.dcrerr.alloc((size_t)nrhs * dlen * sizeof(double));
@@ -476,6 +476,10 @@ template <> KArgs<double> Solver::kargs<double>(int nrhs, int)
     a.colstencil = 2;
     a.cmap = col_map(nx, ny);
     a.jinv = ctl.solver == 1 ? w.jinv64.as<double2>() : nullptr;
+    a.qst = w.qst.as<QmrState>();
+    a.q = w.zm.as<double2>();
+    a.w = w.zc.as<double2>();
+    a.d = w.x1.as<double2>();
     if (ctl.formulation == 1) {
         a.sigma = sigs64_.as<double>();
         a.gd = 1;
@@ -605,6 +609,14 @@ DArgs Solver::dargs(int nrhs)
 int Solver::run_bicg(int nrhs, int precision, int maxit)
 {
     prof_cur_ = precision;
+    if (ctl.solver == 4) {  // QMR (FP64)
+        KArgs<double> a = kargs<double>(nrhs, 0);
+        a.maxit = maxit;
+        launch_qmr_init(a, nrhs, stream_);
+        for (int it = 1; it < maxit; it++) launch_qmr_iter(a, nrhs, stream_);
+        launch_qmr_finish(a, nrhs, stream_);
+        return check(cudaGetLastError(), "QMR launch");
+    }
     if (ctl.solver == 2) {  // Bi-CG for the complex-symmetric system (COCG) with z-line preconditioner
         if (precision == 0) {
             KArgs<double> a = kargs<double>(nrhs, 0);

@@ -61,7 +61,7 @@ struct Workspace {
     DevBuf zm, zc, f_zm, f_zc;  // z-line pivots for BiCGStab + z-line
     DevBuf phi64, phi32;        // grad-div node potentials
     DevBuf jinv64, jinv32;      // inverse diagonal (diagonal preconditioner)
-    DevBuf bst, pst, ost, parts, cnt, rerr, dcrerr;
+    DevBuf bst, pst, ost, qst, parts, cnt, rerr, dcrerr;
 };
 
 // state of one FWDsolve3D call over a batch between its phases (solve_begin,

@@ -18,7 +18,7 @@ LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libmt3d.so")
 
 STATUS = {0: "MT3D_OK", 1: "MT3D_NOT_CONVERGED", 2: "MT3D_BREAKDOWN", 3: "MT3D_NAN_INPUT", 4: "MT3D_CUDA_ERROR",
           5: "MT3D_INVALID_ARGUMENT", 6: "MT3D_DEVICE_TIMEOUT", 7: "MT3D_NO_DEVICE", 8: "MT3D_OUT_OF_MEMORY"}
-SOLVER_BICG, SOLVER_COCG, SOLVER_BICG_ZLINE = 1, 2, 3
+SOLVER_BICG, SOLVER_COCG, SOLVER_BICG_ZLINE, SOLVER_QMR = 1, 2, 3, 4
 PREC_FP64, PREC_MIXED = 0, 1
 FORM_CCDC, FORM_CCGD = 0, 1
 

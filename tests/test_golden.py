@@ -112,6 +112,34 @@ def test_gpu_reproduces_cylinder_fixture(cuda, formulation, solver, cycle, preci
     assert np.median(err) < 1e-5
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [0, 1])
+def test_gpu_reaches_cylinder_fixture_at_tight_tolerance(cuda, precision):
+    """The GPU chain's distance from the fixture at tolerance 1e-7 (up to 5e-4
+    of |Zxy|, above) is iteration error: solved to a relative residual of
+    1e-9 in the grad-div formulation, every site lies within 1e-5 of |Zxy|,
+    as the oracle (the reference's QMR + D-ILU) does at 1e-7."""
+    from mt3d import capi
+    g, m, omega, sites, origin, G = cylinder()
+    s = capi.Solver(g)
+    s.set_formulation(capi.FORM_CCGD)
+    s.set_restart(0)
+    s.update_cond(m.m_earth, m.air_cond)
+    s.update_freq(omega)
+    s.set_control(IterPerDivCor=1000, MaxDivCor=30, tolEMfwd=1e-9, tolEMadj=1e-9, precision=precision)
+    E = []
+    for imode in (1, 2):
+        e0 = s.compute_bc(imode)
+        e, rc = s.fwdsolve(bc=e0, e0=e0)
+        d = s.diagnostics()
+        print("imode", imode, "iterations", d["nIterTotal"], "relres", d["final_relres"])
+        assert rc == 0 and d["final_relres"] <= 1e-9
+        E.append(e)
+    err = site_errors(to_file_units(s.impedance(omega, sites, E[0], E[1], origin=origin)), G)
+    print("max", err.max(), "median", np.median(err))
+    assert err.max() < 1e-5, err.max()
+
+
 def test_air_layers_match_the_reference_log():
     """setup_airlayers 'fixed height 12 1000' on this model: the reference's
     log of the cylinder test prints 'The top of the air layers is at
