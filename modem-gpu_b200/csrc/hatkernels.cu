@@ -266,12 +266,12 @@ __device__ __forceinline__ void hat_xr(const KArgs<float> &a, int r, int bx)
 // March planes [k0, k1) of tile (i0, j0), right-hand side r, calling
 // f(e, interior, yhat, x_e, W) for every existing edge of the thread's node
 // column: yhat = D^-1 (A x)_e and W = |D_e|^2 at interior edges (zero
-// otherwise), e the padded index.  Returns false (all threads of the block
-// alike) when a wait gave up.
-template <typename F>
+// otherwise), e the padded index; plane_done() after each plane.  Returns
+// false (all threads of the block alike) when a wait gave up.
+template <typename F, typename G>
 __device__ __forceinline__ bool hat_march(TmaSmem &sm, const TmaParams &tp, const Geo<float> &g, PadLayout pl, int r,
                                           bool gd, float wmu, int i0, int j0, int k0, int k1, int *err, int limit,
-                                          F &&f)
+                                          F &&f, G &&plane_done)
 {
     const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
     const int i = i0 + tx, j = j0 + ty;
@@ -463,6 +463,7 @@ __device__ __forceinline__ bool hat_march(TmaSmem &sm, const TmaParams &tp, cons
                 f(2 * pc + eb, in, out, Z1, W);
             }
         }
+        plane_done();
         wS = nS;
         wX = nX;
         wY = nY;
@@ -485,23 +486,36 @@ __device__ __forceinline__ void hat_vt(const TmaParams &tp, const KArgs<float> &
     tma_range_at(a.g.nz, bz, gz, k0, k1);
     const size_t off = (size_t)r * a.stride;
     float2 *out = (which ? a.t : a.v) + off;
+    // inner products: the (at most three) terms of a plane summed in FP32,
+    // the planes in FP64
     double u[4] = {0.0, 0.0, 0.0, 0.0};
-    const bool ok = hat_march(tma_smem(), tp, a.g, a.pl, r, a.gd != 0, (float)(a.dsgn * a.ost[r].omega * kMu0), i0,
-                              j0, k0, k1, a.err, a.wait_limit, [&](int e, bool inn, float2 y, float2 x, float W) {
-                                  if (inn) {
-                                      if (which == 0) {
-                                          const float2 z = shadow_z((unsigned)e);
-                                          u[0] += (double)(z.x * y.x + z.y * y.y);  // conj(z) vh
-                                          u[1] += (double)(z.x * y.y - z.y * y.x);
-                                      } else {
-                                          u[0] += (double)(W * (y.x * x.x + y.y * x.y));  // conj(t) s
-                                          u[1] += (double)(W * (y.x * x.y - y.y * x.x));
-                                          u[2] += (double)(W * (y.x * y.x + y.y * y.y));
-                                          u[3] += (double)(W * (x.x * x.x + x.y * x.y));
-                                      }
-                                  }
-                                  out[e] = y;
-                              });
+    float p[4] = {0.f, 0.f, 0.f, 0.f};
+    const bool ok = hat_march(
+        tma_smem(), tp, a.g, a.pl, r, a.gd != 0, (float)(a.dsgn * a.ost[r].omega * kMu0), i0, j0, k0, k1, a.err,
+        a.wait_limit,
+        [&](int e, bool inn, float2 y, float2 x, float W) {
+            if (inn) {
+                if (which == 0) {
+                    const float2 z = shadow_z((unsigned)e);
+                    p[0] += z.x * y.x + z.y * y.y;  // conj(z) vh
+                    p[1] += z.x * y.y - z.y * y.x;
+                } else {
+                    p[0] += W * (y.x * x.x + y.y * x.y);  // conj(t) s
+                    p[1] += W * (y.x * x.y - y.y * x.x);
+                    p[2] += W * (y.x * y.x + y.y * y.y);
+                    p[3] += W * (x.x * x.x + x.y * x.y);
+                }
+            }
+            out[e] = y;
+        },
+        [&]() {
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                if (which == 0 && q >= 2) break;
+                u[q] += (double)p[q];
+                p[q] = 0.f;
+            }
+        });
     if (!ok) return;
     double tot[4];
     if (block_reduce_last<4>(u, a.parts, a.cnt, r, bx + a.cmap.tiles * bz, a.cmap.tiles * gz, tot) &&

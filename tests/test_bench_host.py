@@ -57,3 +57,34 @@ def test_steps_cover_all_frequencies_once():
         seen += bench.step_rows("combined", 16, s)
     assert sorted(seen) == list(range(16))
     assert bench.step_rows("precision", 1, 5) == [0]
+
+
+def test_impedance_error_is_site_relative():
+    import numpy as np
+    Zref = np.array([[[0.0, 2.0], [-2.0, 0.0]], [[0.0, 10.0], [-10.0, 0.0]]], complex)
+    Z = Zref.copy()
+    Z[0, 0, 1] += 2e-6  # 1e-6 of the first site's largest component
+    Z[1, 1, 0] += 5e-6  # 5e-7 of the second site's
+    assert abs(bench.z_error(Z, Zref) - 1e-6) < 1e-12
+
+
+def test_surface_sites_lie_on_core_cells():
+    import numpy as np
+    from mt3d import models
+    m, _ = models.config_small_forward()
+    s = bench.surface_sites(m, 4)
+    assert s.shape == (16, 3) and np.all(s[:, 2] == 0.0)
+    assert np.all((s[:, 0] > 0) & (s[:, 0] < m.grid.dx.sum()) & (s[:, 1] > 0) & (s[:, 1] < m.grid.dy.sum()))
+
+
+def test_both_arms_report_the_same_config():
+    cfg = bench.bench_config("combined", "desc", [8, 8], 1)
+    assert cfg == bench.bench_config("combined", "desc", [8, 8], 1)
+    assert cfg["workload"] == "combined: desc" and cfg["solves_per_step"] == 8
+
+
+def test_cpu_iterations_source_is_named():
+    it, src = bench.cpu_iterations("combined")
+    assert it > 0 and src
+    it2, src2 = bench.cpu_iterations("precision")
+    assert it2 == bench.CPU_ITERS_PRECISION and "100x100x60" in src2
