@@ -302,12 +302,13 @@ def stencil_bytes(kprec: int, nE: int, nN: int, fused: bool = False) -> float:
     """Algorithmic bytes per edge and right-hand side of one staged stencil
     launch.  Unfused (v = A ph with rt . v, or t = A sh with t . s, t . t):
     read the input vector, the auxiliary vector and sigma, the signed node
-    weight (nN / nE per edge), write the output.  Fused FP32 iteration
-    (vh = D^-1 A u, or th = D^-1 A sh): the same without the auxiliary
-    vector (the shadow vector is generated, s is the staged input)."""
+    weight (nN / nE per edge), write the output.  Fused FP32 iteration:
+    vh = D^-1 A u with the shadow's (rt, v) reads the same, th = D^-1 A sh
+    with its dots needs no auxiliary vector (s is the staged input); the
+    two launches alternate, so a launch averages 2.5 vectors."""
     sc = 8 if kprec else 16
     sr = 4 if kprec else 8
-    return (2 if (fused and kprec) else 3) * sc + sr + sr * nN / nE
+    return (2.5 if (fused and kprec) else 3) * sc + sr + sr * nN / nE
 
 
 # DRAM bytes (read + write) per edge and right-hand side of one kct_vt launch,

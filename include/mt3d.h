@@ -116,13 +116,12 @@ MT3D_API int mt3d_set_restart(mt3d_handle h, int restart);
 /* The FP32 iteration of the mixed-precision BiCGStab (MT3D_PREC_MIXED with
  * MT3D_SOLVER_BICG).  on != 0 (default): the iteration runs in
  * preconditioned variables (u = D^-1 p, D^-1 r, D^-1 v, ...) with the
- * diagonal preconditioner fused into the operator kernels and a fixed
- * pseudo-random shadow vector, 147 bytes of memory traffic per edge and
- * iteration; 0: the kernels that keep the reference's variables (rt = r0,
- * the preconditioned vectors formed in separate passes), 211 bytes.  Both
- * are BiCGStab with the diagonal preconditioner of BICG
- * (f90/3D_MT/FWD/solver.f90:346-555); they differ in the shadow vector and
- * rounding.  No counterpart in the reference. */
+ * diagonal preconditioner fused into the operator kernels, 163 bytes of
+ * memory traffic per edge and iteration; 0: the kernels that keep the
+ * reference's variables (the preconditioned vectors formed in separate
+ * passes), 211 bytes.  Both are BiCGStab with the diagonal preconditioner of
+ * BICG (f90/3D_MT/FWD/solver.f90:346-555) and the shadow rt = r0; they
+ * differ in rounding.  No counterpart in the reference. */
 MT3D_API int mt3d_set_fused(mt3d_handle h, int on);
 
 /* Set the conductivity model (UpdateCond, f90/3D_MT/FWD/modelOperator3D.f90:

@@ -9,25 +9,27 @@
 // (vh = D^-1 A u, th = D^-1 A sh), and no vector of D^-1 exists:
 //
 //   kh_u     u  = rh + beta (u - omega vh)   (u = rh on the first iteration)
-//   kh_vt 0  vh = D^-1 A u,       (z, vh)                  -> alpha
+//   kh_vt 0  vh = D^-1 A u,       (rt, v)                  -> alpha
 //   kh_s     sh = rh - alpha vh
 //   kh_vt 1  th = D^-1 A sh,      (t, s), (t, t), (s, s)   -> omega, ||r||
-//   kh_xr    x += alpha u + omega sh,  rh = sh - omega th,  (z, rh) -> beta
+//   kh_xr    x += alpha u + omega sh,  rh = sh - omega th,  (rt, r) -> beta
 //
-// 147 bytes per edge and iteration instead of the 211 of the unfused
+// 163 bytes per edge and iteration instead of the 211 of the unfused
 // kernels (kb_p, kct_vt, kb_s, kct_vt, kb_xr).  The inner products of the
 // method in the original variables follow from the hat ones:
-//   - the shadow residual is rt = D^-H z, so (rt, r) = (z, rh) and
-//     (rt, v) = (z, vh); z is a fixed pseudo-random vector of entries
-//     +-1 +- i generated from the edge index, so it costs no memory traffic
-//     (any shadow with (rt, r0) != 0 is a valid BiCGStab shadow; a random one
-//     converges like rt = r0);
+//   - the shadow residual is the reference's rt = r0 = b; with y =
+//     conj(D) b stored once per cycle (written by kh_cast), (rt, r) =
+//     sum conj(y) rh and (rt, v) = sum conj(y) vh;
 //   - with W = |D|^2 per edge, computed in the operator kernel where D is,
 //     (t, s) = sum W conj(th) sh, (t, t) = sum W |th|^2, and the true
 //     residual norm of the new iterate follows without another pass:
 //     ||s - omega t||^2 = ||s||^2 - 2 Re(conj(omega) (t, s)) + |omega|^2 ||t||^2.
 // The iterates, step lengths and residual norms are those of the unfused
-// kernels up to the shadow vector and rounding.
+// kernels up to rounding.  (A shadow generated from the edge index instead
+// of a stored one, rt = D^-H z with z = +-1 +- i, saves 16 bytes an
+// iteration, but its entries scale as 1/|D|, which on the benchmark model
+// cost 40 % more iterations and on the reference's cylinder model stalled
+// the solve.)
 //
 // The operator kernels stage u or sh with the tensor copies of tma.cuh.  D =
 // V_E xXO-diagonal of the curl-curl term (col_ccdiag) + the grad-div diagonal
@@ -45,19 +47,6 @@ namespace mt3d {
 
 extern std::atomic<long long> g_launch_count;
 static inline void counted(int n) { g_launch_count.fetch_add(n, std::memory_order_relaxed); }
-
-// shadow vector entry of padded index e: +-1 +- i from a 32-bit integer hash
-// (the "lowbias32" mixer of C. Wellons' hash-prospector)
-__device__ __forceinline__ float2 shadow_z(unsigned e)
-{
-    unsigned h = e;
-    h ^= h >> 16;
-    h *= 0x7feb352du;
-    h ^= h >> 15;
-    h *= 0x846ca68bu;
-    h ^= h >> 16;
-    return make_float2((h & 1u) ? 1.f : -1.f, (h & 2u) ? 1.f : -1.f);
-}
 
 // diagonal of A at an interior edge: dr + i di
 __device__ __forceinline__ void hat_diag(int comp, const ColGeo<float> &cg, const PlaneGeo<float> &pg, float wmu,
@@ -92,8 +81,8 @@ __device__ __forceinline__ float2 hat_div(float2 y, float dr, float di, float &W
 
 // ---------------------------------------------------------------------------
 // start of an FP32 cycle: rh = D^-1 b with b = r64 scale on the padded
-// layout, x = 0; ||b||^2 and rho = (z, rh).  The first guess is zero, so
-// r = b and no operator pass is needed.
+// layout, the shadow y = conj(D) b (rt = b), x = 0; ||b||^2 = rho = (rt, r).
+// The first guess is zero, so r = b and no operator pass is needed.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kThreads) kh_cast(KArgs<float> a, const double2 *r64, size_t stride64)
 {
@@ -103,13 +92,13 @@ __global__ void __launch_bounds__(kThreads) kh_cast(KArgs<float> a, const double
     const size_t off = (size_t)r * stride64, offp = (size_t)r * a.stride;
     const double sc = a.ost[r].scale;
     const float wmu = (float)(a.dsgn * a.ost[r].omega * kMu0);
-    double u[3] = {0.0, 0.0, 0.0};
+    double u[1] = {0.0};
     for (int e = blockIdx.x * kThreads + threadIdx.x; e < g.nE; e += gridDim.x * kThreads) {
         const EdgeIdx q = edge_decode(g, e);
         const int pe = a.pl.idx(q.c, q.i, q.j, q.k);
         const double2 v = r64[off + e];
         const float2 b = make_float2((float)(v.x * sc), (float)(v.y * sc));
-        float2 rh = make_float2(0.f, 0.f);
+        float2 rh = make_float2(0.f, 0.f), y = rh;
         if (edge_interior(g, q)) {
             const ColGeo<float> cg = col_geo(g, q.i, q.j);
             const PlaneGeo<float> pg = plane_geo(g, q.k);
@@ -122,21 +111,17 @@ __global__ void __launch_bounds__(kThreads) kh_cast(KArgs<float> a, const double
             float dr, di, W;
             hat_diag(q.c, cg, pg, wmu, a.sigma[e], a.gd != 0, wns, wne, dr, di);
             rh = hat_div(b, dr, di, W);
-            const float2 z = shadow_z((unsigned)pe);
+            y = make_float2(dr * b.x + di * b.y, dr * b.y - di * b.x);  // conj(D) b
             u[0] += (double)b.x * b.x + (double)b.y * b.y;
-            u[1] += (double)z.x * rh.x + (double)z.y * rh.y;  // conj(z) rh
-            u[2] += (double)z.x * rh.y - (double)z.y * rh.x;
         }
         a.r[offp + pe] = rh;
+        a.rt[offp + pe] = y;
         a.x0[offp + pe] = make_float2(0.f, 0.f);
     }
-    double tot[3];
-    if (block_reduce_last<3>(u, a.parts, a.cnt, r, blockIdx.x, gridDim.x, tot) && threadIdx.x == 0) {
+    double tot[1];
+    if (block_reduce_last<1>(u, a.parts, a.cnt, r, blockIdx.x, gridDim.x, tot) && threadIdx.x == 0) {
         const double t2[2] = {tot[0], tot[0]};
-        BicgState &st = a.st[r];
-        fin_init(st, t2, a.rerr + (size_t)r * a.rerr_stride, a.maxit, a.ost[r].tol_inner);
-        st.rho = {tot[1], tot[2]};
-        if (st.status == KS_RUNNING && cd_zero(st.rho)) st.status = KS_BREAKDOWN;
+        fin_init(a.st[r], t2, a.rerr + (size_t)r * a.rerr_stride, a.maxit, a.ost[r].tol_inner);
     }
 }
 
@@ -205,6 +190,7 @@ __device__ __forceinline__ void hat_xr(const KArgs<float> &a, int r, int bx)
     const float4 *SH = reinterpret_cast<const float4 *>(a.sh) + off;
     const float4 *TH = reinterpret_cast<const float4 *>(a.t) + off;
     float4 *RH = reinterpret_cast<float4 *>(a.r) + off;
+    const float4 *Y = reinterpret_cast<const float4 *>(a.rt) + off;
     double u[2] = {0.0, 0.0};
     HAT_PAIRS(a, bx)
     {
@@ -212,9 +198,9 @@ __device__ __forceinline__ void hat_xr(const KArgs<float> &a, int r, int bx)
         XD[q] = add4(add4(XS[q], c2mul2(al, U[q])), c2mul2(om, sh));
         const float4 rn = sub4(sh, c2mul2(om, TH[q]));
         RH[q] = rn;
-        const float2 z0 = shadow_z(2u * q), z1 = shadow_z(2u * q + 1u);
-        u[0] += (double)(z0.x * rn.x + z0.y * rn.y) + (double)(z1.x * rn.z + z1.y * rn.w);
-        u[1] += (double)(z0.x * rn.y - z0.y * rn.x) + (double)(z1.x * rn.w - z1.y * rn.z);
+        const float4 y = Y[q];  // conj(y) rh
+        u[0] += (double)y.x * rn.x + (double)y.y * rn.y + (double)y.z * rn.z + (double)y.w * rn.w;
+        u[1] += (double)y.x * rn.y - (double)y.y * rn.x + (double)y.z * rn.w - (double)y.w * rn.z;
     }
     double tot[2];
     if (block_reduce_last<2>(u, a.parts, a.cnt, r, bx, a.nblk, tot) && threadIdx.x == 0) {
@@ -243,7 +229,7 @@ __device__ __forceinline__ void hat_xr(const KArgs<float> &a, int r, int bx)
         const cd rho_new = {tot[0], tot[1]};
         if (a.restart > 0 && st.iter % a.restart == 0) {
             // restart towards steepest descent: p = r, omega = 1 (the shadow
-            // vector is kept)
+            // vector of the cycle is kept)
             st.first = 1;
             st.rho = rho_new;
             st.omega = {1.0, 0.0};
@@ -486,36 +472,31 @@ __device__ __forceinline__ void hat_vt(const TmaParams &tp, const KArgs<float> &
     tma_range_at(a.g.nz, bz, gz, k0, k1);
     const size_t off = (size_t)r * a.stride;
     float2 *out = (which ? a.t : a.v) + off;
-    // inner products: the (at most three) terms of a plane summed in FP32,
-    // the planes in FP64
+    // inner products summed per edge in FP64 (per-plane FP32 partial sums
+    // changed the Krylov rounding enough to send more right-hand sides to
+    // the FP64 fallback)
+    const float2 *Yr = a.rt + off;
     double u[4] = {0.0, 0.0, 0.0, 0.0};
-    float p[4] = {0.f, 0.f, 0.f, 0.f};
     const bool ok = hat_march(
         tma_smem(), tp, a.g, a.pl, r, a.gd != 0, (float)(a.dsgn * a.ost[r].omega * kMu0), i0, j0, k0, k1, a.err,
         a.wait_limit,
         [&](int e, bool inn, float2 y, float2 x, float W) {
             if (inn) {
                 if (which == 0) {
-                    const float2 z = shadow_z((unsigned)e);
-                    p[0] += z.x * y.x + z.y * y.y;  // conj(z) vh
-                    p[1] += z.x * y.y - z.y * y.x;
+                    const float2 z = Yr[e];
+                    u[0] += (double)z.x * y.x + (double)z.y * y.y;  // conj(y) vh
+                    u[1] += (double)z.x * y.y - (double)z.y * y.x;
                 } else {
-                    p[0] += W * (y.x * x.x + y.y * x.y);  // conj(t) s
-                    p[1] += W * (y.x * x.y - y.y * x.x);
-                    p[2] += W * (y.x * y.x + y.y * y.y);
-                    p[3] += W * (x.x * x.x + x.y * x.y);
+                    const double w = W;
+                    u[0] += w * ((double)y.x * x.x + (double)y.y * x.y);  // conj(t) s
+                    u[1] += w * ((double)y.x * x.y - (double)y.y * x.x);
+                    u[2] += w * ((double)y.x * y.x + (double)y.y * y.y);
+                    u[3] += w * ((double)x.x * x.x + (double)x.y * x.y);
                 }
             }
             out[e] = y;
         },
-        [&]() {
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-                if (which == 0 && q >= 2) break;
-                u[q] += (double)p[q];
-                p[q] = 0.f;
-            }
-        });
+        [&]() {});
     if (!ok) return;
     double tot[4];
     if (block_reduce_last<4>(u, a.parts, a.cnt, r, bx + a.cmap.tiles * bz, a.cmap.tiles * gz, tot) &&

@@ -113,7 +113,7 @@ __global__ void __launch_bounds__(kThreads) k_gd_phi(KArgs<T> a, const C2<T> *x,
         const int i = n % (g.nx + 1), t = n / (g.nx + 1), j = t % (g.ny + 1), k = t / (g.ny + 1);
         C2<T> out = mk<T>(0, 0);
         const bool earth = a.gde[n];
-        if (i >= 1 && i <= g.nx - 1 && j >= 1 && j <= g.ny - 1 && k >= 1 && k <= g.nz - 1 && (mode == 0 || earth)) {
+        if (i >= 1 && i <= g.nx - 1 && j >= 1 && j <= g.ny - 1 && k >= 1 && k <= g.nz - 1 && (mode != 1 || earth)) {
             const int e[6] = {iX(g, i - 1, j, k), iX(g, i, j, k), iY(g, i, j - 1, k),
                               iY(g, i, j, k), iZ(g, i, j, k - 1), iZ(g, i, j, k)};
             const T dfa[3] = {g.delY[j] * g.delZ[k], g.delX[i] * g.delZ[k], g.delX[i] * g.delY[j]};

@@ -986,11 +986,18 @@ int Solver::solve_begin(SolveRun &run, int nrhs, const double *omegas, const int
     diag = Diag{};
     run.dg.assign(nrhs, Diag{});
     if ((rc = pull_state(run))) return rc;
-    for (int r = 0; r < nrhs; r++)
+    for (int r = 0; r < nrhs; r++) {
         if (!std::isfinite(os[r].bnorm64)) {
             os[r].active = 0;
             os[r].failed = 3;
+        } else if (os[r].active && os[r].bnorm64 == 0.0) {
+            // zero right-hand side (no boundary data, no source): zero
+            // interior solution, as BICG returns for b = 0
+            cudaMemsetAsync(X + (size_t)r * nE, 0, ebytes, stream_);
+            os[r].active = 0;
+            os[r].converged = 1;
         }
+    }
     // initial divergence correction for a source term (EMsolve3D.f90:298-303)
     bool any_dc = false;
     for (int r = 0; r < nrhs; r++) {

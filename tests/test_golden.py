@@ -117,16 +117,21 @@ def test_gpu_reproduces_cylinder_fixture(cuda, formulation, solver, cycle, preci
 def test_gpu_reaches_cylinder_fixture_at_tight_tolerance(cuda, precision):
     """The GPU chain's distance from the fixture at tolerance 1e-7 (up to 5e-4
     of |Zxy|, above) is iteration error: solved to a relative residual of
-    1e-9 in the grad-div formulation, every site lies within 1e-5 of |Zxy|,
-    as the oracle (the reference's QMR + D-ILU) does at 1e-7."""
+    1e-9 in the reference's formulation (curl-curl with the divergence
+    correction, here with the z-line preconditioner), every site lies within
+    1e-5 of |Zxy|, as the oracle (the reference's QMR + D-ILU) does at 1e-7.
+    (In the grad-div formulation the same residual leaves up to 3e-5: its
+    residual norm is dominated by the grad-div rows, whose weights
+    1/(sigma_N V_N) are large in resistive cells, so it bounds the field
+    error less tightly.)"""
     from mt3d import capi
     g, m, omega, sites, origin, G = cylinder()
     s = capi.Solver(g)
-    s.set_formulation(capi.FORM_CCGD)
-    s.set_restart(0)
+    s.set_formulation(capi.FORM_CCDC)
     s.update_cond(m.m_earth, m.air_cond)
     s.update_freq(omega)
-    s.set_control(IterPerDivCor=1000, MaxDivCor=30, tolEMfwd=1e-9, tolEMadj=1e-9, precision=precision)
+    s.set_control(IterPerDivCor=100, MaxDivCor=150, tolEMfwd=1e-9, tolEMadj=1e-9, solver=capi.SOLVER_BICG_ZLINE,
+                  precision=precision)
     E = []
     for imode in (1, 2):
         e0 = s.compute_bc(imode)
