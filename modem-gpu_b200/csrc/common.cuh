@@ -279,6 +279,62 @@ template <int N> __device__ __forceinline__ void warp_sum(double (&v)[N])
 // Reduce v over the block, write this block's partial, and return true in
 // the (single) last block of this right-hand side, whose thread 0 then holds
 // the total in `tot`.  `parts` is [nrhs][nblk][N]; `cnt` one counter per rhs.
+// As block_reduce_last below, with its shared scratch (N * kThreads / 32
+// doubles and one flag) supplied by the caller, e.g. part of a ring buffer
+// the block no longer reads.
+template <int N>
+__device__ __forceinline__ bool block_reduce_last_in(double (&v)[N], double *__restrict__ parts, unsigned *cnt,
+                                                     int rhs, int blk, int nblk, double (&tot)[N], double *scratch,
+                                                     int *flag)
+{
+    double(*sm)[kThreads / 32] = reinterpret_cast<double(*)[kThreads / 32]>(scratch);
+    int &s_last = *flag;
+    warp_sum<N>(v);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0)
+#pragma unroll
+        for (int n = 0; n < N; n++) sm[n][w] = v[n];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double *p = parts + ((size_t)rhs * nblk + blk) * N;
+#pragma unroll
+        for (int n = 0; n < N; n++) {
+            double s = 0.0;
+            for (int q = 0; q < kThreads / 32; q++) s += sm[n][q];
+            p[n] = s;
+        }
+        __threadfence();
+        unsigned t = atomicAdd(&cnt[rhs], 1u);
+        s_last = (t == (unsigned)nblk - 1);
+    }
+    __syncthreads();
+    if (!s_last) return false;
+    __threadfence();
+    double acc[N];
+#pragma unroll
+    for (int n = 0; n < N; n++) acc[n] = 0.0;
+    const volatile double *pp = parts + (size_t)rhs * nblk * N;
+    for (int b = threadIdx.x; b < nblk; b += kThreads)
+#pragma unroll
+        for (int n = 0; n < N; n++) acc[n] += pp[(size_t)b * N + n];
+    warp_sum<N>(acc);
+    __syncthreads();
+    if (lane == 0)
+#pragma unroll
+        for (int n = 0; n < N; n++) sm[n][w] = acc[n];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int n = 0; n < N; n++) {
+            double s = 0.0;
+            for (int q = 0; q < kThreads / 32; q++) s += sm[n][q];
+            tot[n] = s;
+        }
+        cnt[rhs] = 0u;
+    }
+    return true;
+}
+
 template <int N>
 __device__ __forceinline__ bool block_reduce_last(double (&v)[N], double *__restrict__ parts, unsigned *cnt, int rhs,
                                                   int blk, int nblk, double (&tot)[N])

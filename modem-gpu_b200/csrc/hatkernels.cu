@@ -228,10 +228,12 @@ __device__ __forceinline__ void hat_xr(const KArgs<float> &a, int r, int bx)
         }
         const cd rho_new = {tot[0], tot[1]};
         if (a.restart > 0 && st.iter % a.restart == 0) {
-            // restart towards steepest descent: p = r, omega = 1 (the shadow
-            // vector of the cycle is kept)
+            // restart towards steepest descent (cuBiCG, f90/3D_MT/FWD_SP2/
+            // solver.f90:1545-1573): rt = r, rho = (rt, r) = ||r||^2, p = r,
+            // omega = 1; the next kh_vt 0 writes the new shadow y = W rh
             st.first = 1;
-            st.rho = rho_new;
+            st.pad = 1;
+            st.rho = {st.rn2, 0.0};
             st.omega = {1.0, 0.0};
             if (cd_zero(st.rho)) st.status = KS_BREAKDOWN;
             return;
@@ -250,14 +252,15 @@ __device__ __forceinline__ void hat_xr(const KArgs<float> &a, int r, int bx)
 // ---------------------------------------------------------------------------
 
 // March planes [k0, k1) of tile (i0, j0), right-hand side r, calling
-// f(e, interior, yhat, x_e, W) for every existing edge of the thread's node
-// column: yhat = D^-1 (A x)_e and W = |D_e|^2 at interior edges (zero
-// otherwise), e the padded index; plane_done() after each plane.  Returns
-// false (all threads of the block alike) when a wait gave up.
-template <typename F, typename G>
+// f(e, interior, yhat, x_e, W, aux_e) for every existing edge of the thread's
+// node column: yhat = D^-1 (A x)_e and W = |D_e|^2 at interior edges (zero
+// otherwise), e the padded index, aux_e the entry of the vector aux (read one
+// plane ahead, zero when aux is null).  Returns false (all threads of the
+// block alike) when a wait gave up.
+template <typename F>
 __device__ __forceinline__ bool hat_march(TmaSmem &sm, const TmaParams &tp, const Geo<float> &g, PadLayout pl, int r,
-                                          bool gd, float wmu, int i0, int j0, int k0, int k1, int *err, int limit,
-                                          F &&f, G &&plane_done)
+                                          const float2 *__restrict__ aux, bool gd, float wmu, int i0, int j0, int k0,
+                                          int k1, int *err, int limit, F &&f)
 {
     const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
     const int i = i0 + tx, j = j0 + ty;
@@ -330,6 +333,16 @@ __device__ __forceinline__ bool hat_march(TmaSmem &sm, const TmaParams &tp, cons
         y = N[hw + kNW];
     };
 
+    float2 ax = zero, ay = zero, az = zero;
+    auto load_aux = [&](int k) {
+        if (!aux || !live || k > g.nz) return;
+        const int b = col + pxy * k;
+        if (cg.hasX) ax = aux[b];
+        if (cg.hasY) ay = aux[pc + b];
+        if (k < g.nz) az = aux[2 * pc + b];
+    };
+
+    load_aux(k0);
     issue(k0 - 1);
     issue(k0);
     issue(k0 + 1);
@@ -394,7 +407,7 @@ __device__ __forceinline__ bool hat_march(TmaSmem &sm, const TmaParams &tp, cons
                     if (gd) out = cadd(out, cscale(csub(P0[hn + 1], P0[hn]), cg.delYj * pg.delZk));
                     out = hat_div(out, dr, di, W);
                 }
-                f(eb, in, out, X1, W);
+                f(eb, in, out, X1, W, ax);
             }
             // ---- Ey(i, j, k)
             if (cg.hasY) {
@@ -420,7 +433,7 @@ __device__ __forceinline__ bool hat_march(TmaSmem &sm, const TmaParams &tp, cons
                     if (gd) out = cadd(out, cscale(csub(P0[hn + kPhX], P0[hn]), cg.delXi * pg.delZk));
                     out = hat_div(out, dr, di, W);
                 }
-                f(pc + eb, in, out, Y1, W);
+                f(pc + eb, in, out, Y1, W, ay);
             }
             // ---- Ez(i, j, k)
             if (k < g.nz) {
@@ -446,10 +459,10 @@ __device__ __forceinline__ bool hat_march(TmaSmem &sm, const TmaParams &tp, cons
                     if (gd) out = cadd(out, cscale(csub(P1[hn], P0[hn]), cg.delXi * cg.delYj));
                     out = hat_div(out, dr, di, W);
                 }
-                f(2 * pc + eb, in, out, Z1, W);
+                f(2 * pc + eb, in, out, Z1, W, az);
             }
+            if (k + 1 < k1) load_aux(k + 1);
         }
-        plane_done();
         wS = nS;
         wX = nX;
         wY = nY;
@@ -475,15 +488,20 @@ __device__ __forceinline__ void hat_vt(const TmaParams &tp, const KArgs<float> &
     // inner products summed per edge in FP64 (per-plane FP32 partial sums
     // changed the Krylov rounding enough to send more right-hand sides to
     // the FP64 fallback)
-    const float2 *Yr = a.rt + off;
+    float2 *Yr = a.rt + off;
+    // after a restart (first iteration, pad set) the shadow becomes the
+    // current residual: y = W rh, rh being the staged u of this launch
+    const bool reset = which == 0 && st.first && st.pad;
     double u[4] = {0.0, 0.0, 0.0, 0.0};
+    TmaSmem &sm = tma_smem();
     const bool ok = hat_march(
-        tma_smem(), tp, a.g, a.pl, r, a.gd != 0, (float)(a.dsgn * a.ost[r].omega * kMu0), i0, j0, k0, k1, a.err,
-        a.wait_limit,
-        [&](int e, bool inn, float2 y, float2 x, float W) {
+        sm, tp, a.g, a.pl, r, (which == 0 && !reset) ? Yr : nullptr, a.gd != 0,
+        (float)(a.dsgn * a.ost[r].omega * kMu0), i0, j0, k0, k1, a.err, a.wait_limit,
+        [&](int e, bool inn, float2 y, float2 x, float W, float2 ya) {
+            if (reset) Yr[e] = inn ? make_float2(W * x.x, W * x.y) : make_float2(0.f, 0.f);
             if (inn) {
                 if (which == 0) {
-                    const float2 z = Yr[e];
+                    const float2 z = reset ? make_float2(W * x.x, W * x.y) : ya;
                     u[0] += (double)z.x * y.x + (double)z.y * y.y;  // conj(y) vh
                     u[1] += (double)z.x * y.y - (double)z.y * y.x;
                 } else {
@@ -495,14 +513,16 @@ __device__ __forceinline__ void hat_vt(const TmaParams &tp, const KArgs<float> &
                 }
             }
             out[e] = y;
-        },
-        [&]() {});
+        });
     if (!ok) return;
+    // the march has read its last staged plane: the field ring is free
     double tot[4];
-    if (block_reduce_last<4>(u, a.parts, a.cnt, r, bx + a.cmap.tiles * bz, a.cmap.tiles * gz, tot) &&
+    if (block_reduce_last_in<4>(u, a.parts, a.cnt, r, bx + a.cmap.tiles * bz, a.cmap.tiles * gz, tot,
+                                reinterpret_cast<double *>(sm.fld[0]), reinterpret_cast<int *>(sm.fld[1])) &&
         threadIdx.x == 0) {
         if (which == 0) {
             fin_v(st, tot);
+            st.pad = 0;
         } else {
             fin_t(st, tot);
             if (st.status == KS_RUNNING) {
