@@ -71,11 +71,12 @@ __device__ __forceinline__ void hat_diag(int comp, const ColGeo<float> &cg, cons
     di = wmu * sig * ve;
 }
 
-// y / D and |D|^2
+// y / D and |D|^2 (the fast reciprocal intrinsic: D^-1 only has to be the
+// same in every kernel that applies it, which one function guarantees)
 __device__ __forceinline__ float2 hat_div(float2 y, float dr, float di, float &W)
 {
     W = dr * dr + di * di;
-    const float inv = 1.f / W;
+    const float inv = __fdividef(1.f, W);
     return make_float2((y.x * dr + y.y * di) * inv, (y.y * dr - y.x * di) * inv);
 }
 
@@ -257,10 +258,10 @@ __device__ __forceinline__ void hat_xr(const KArgs<float> &a, int r, int bx)
 // otherwise), e the padded index, aux_e the entry of the vector aux (read one
 // plane ahead, zero when aux is null).  Returns false (all threads of the
 // block alike) when a wait gave up.
-template <typename F>
+template <bool gd, typename F>
 __device__ __forceinline__ bool hat_march(TmaSmem &sm, const TmaParams &tp, const Geo<float> &g, PadLayout pl, int r,
-                                          const float2 *__restrict__ aux, bool gd, float wmu, int i0, int j0, int k0,
-                                          int k1, int *err, int limit, F &&f)
+                                          const float2 *__restrict__ aux, float wmu, int i0, int j0, int k0, int k1,
+                                          int *err, int limit, F &&f)
 {
     const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
     const int i = i0 + tx, j = j0 + ty;
@@ -471,11 +472,12 @@ __device__ __forceinline__ bool hat_march(TmaSmem &sm, const TmaParams &tp, cons
     return true;
 }
 
-// vh = D^-1 A u, (z, vh) -> alpha   (which = 0)
+// vh = D^-1 A u, (rt, v) -> alpha   (which = 0)
 // th = D^-1 A sh, (t, s)_W, (t, t)_W, (s, s)_W -> omega, ||r_new||   (which = 1)
-// for column tile bx and plane chunk bz of gz of right-hand side r
-__device__ __forceinline__ void hat_vt(const TmaParams &tp, const KArgs<float> &a, int which, int r, int bx, int bz,
-                                       int gz)
+// for column tile bx and plane chunk bz of gz of right-hand side r; which and
+// the grad-div term are compile-time, so the march carries no branch on them
+template <int which, bool gd>
+__device__ __forceinline__ void hat_vt(const TmaParams &tp, const KArgs<float> &a, int r, int bx, int bz, int gz)
 {
     BicgState &st = a.st[r];
     if (st.status != KS_RUNNING || !a.ost[r].active) return;
@@ -494,9 +496,9 @@ __device__ __forceinline__ void hat_vt(const TmaParams &tp, const KArgs<float> &
     const bool reset = which == 0 && st.first && st.pad;
     double u[4] = {0.0, 0.0, 0.0, 0.0};
     TmaSmem &sm = tma_smem();
-    const bool ok = hat_march(
-        sm, tp, a.g, a.pl, r, (which == 0 && !reset) ? Yr : nullptr, a.gd != 0,
-        (float)(a.dsgn * a.ost[r].omega * kMu0), i0, j0, k0, k1, a.err, a.wait_limit,
+    const bool ok = hat_march<gd>(
+        sm, tp, a.g, a.pl, r, (which == 0 && !reset) ? Yr : nullptr, (float)(a.dsgn * a.ost[r].omega * kMu0), i0,
+        j0, k0, k1, a.err, a.wait_limit,
         [&](int e, bool inn, float2 y, float2 x, float W, float2 ya) {
             if (reset) Yr[e] = inn ? make_float2(W * x.x, W * x.y) : make_float2(0.f, 0.f);
             if (inn) {
@@ -541,9 +543,10 @@ __device__ __forceinline__ void hat_vt(const TmaParams &tp, const KArgs<float> &
 __global__ void __launch_bounds__(kThreads) kh_u(KArgs<float> a) { hat_u(a, blockIdx.y, blockIdx.x); }
 __global__ void __launch_bounds__(kThreads) kh_s(KArgs<float> a) { hat_s(a, blockIdx.y, blockIdx.x); }
 __global__ void __launch_bounds__(kThreads) kh_xr(KArgs<float> a) { hat_xr(a, blockIdx.y, blockIdx.x); }
-__global__ void __launch_bounds__(kThreads, 4) kh_vt(const __grid_constant__ TmaParams tp, KArgs<float> a, int which)
+template <int which, bool gd>
+__global__ void __launch_bounds__(kThreads, 4) kh_vt(const __grid_constant__ TmaParams tp, KArgs<float> a)
 {
-    hat_vt(tp, a, which, blockIdx.y, blockIdx.x, blockIdx.z, gridDim.z);
+    hat_vt<which, gd>(tp, a, blockIdx.y, blockIdx.x, blockIdx.z, gridDim.z);
 }
 
 // the grids of a multi-grid batch, passed by value: each grid's arguments,
@@ -574,7 +577,7 @@ template <int K> __global__ void __launch_bounds__(kThreads) kh_elem_multi(const
     else if (K == 1) hat_s(a, r, bx);
     else hat_xr(a, r, bx);
 }
-__global__ void __launch_bounds__(kThreads, 4) kh_vt_multi(const __grid_constant__ HatMulti p, int which)
+template <int which> __global__ void __launch_bounds__(kThreads, 4) kh_vt_multi(const __grid_constant__ HatMulti p)
 {
     const int g = multi_grid_of(p.sb0, p.ng, blockIdx.x);
     const KArgs<float> &a = p.a[g];
@@ -582,7 +585,8 @@ __global__ void __launch_bounds__(kThreads, 4) kh_vt_multi(const __grid_constant
     const int local = blockIdx.x - p.sb0[g];
     const int r = local / per, rem = local - r * per;
     const int bz = rem / a.cmap.tiles, bx = rem - bz * a.cmap.tiles;
-    hat_vt(p.tp[g][which], a, which, r, bx, bz, p.zch[g]);
+    if (a.gd) hat_vt<which, true>(p.tp[g][which], a, r, bx, bz, p.zch[g]);
+    else hat_vt<which, false>(p.tp[g][which], a, r, bx, bz, p.zch[g]);
 }
 
 // ---------------------------------------------------------------------------
@@ -596,6 +600,13 @@ void launch_hat_cast(const KArgs<float> &a, const double2 *r64, size_t stride64,
     kh_cast<<<dim3(hat_grid(a.g.nE), nrhs), kThreads, 0, s>>>(a, r64, stride64);
 }
 
+template <int which, bool gd> static void launch_hat_vt_t(const KArgs<float> &a, const TmaParams &tp, int nrhs,
+                                                           cudaStream_t s)
+{
+    const size_t sm = sizeof(TmaSmem);
+    const int res = tma_resident(kh_vt<which, gd>, sm, 2);
+    kh_vt<which, gd><<<dim3(a.cmap.tiles, nrhs, stage_chunks(a.g.nz, a.cmap.tiles, res)), kThreads, sm, s>>>(tp, a);
+}
 static void launch_hat_vt(const KArgs<float> &a, const TmaMaps *m, int which, int nrhs, cudaStream_t s)
 {
     counted(1);
@@ -603,9 +614,13 @@ static void launch_hat_vt(const KArgs<float> &a, const TmaMaps *m, int which, in
     tp.in = which ? m->sh : m->ph;
     tp.sig = m->sig;
     tp.node = m->node;
-    const size_t sm = sizeof(TmaSmem);
-    const int res = tma_resident(kh_vt, sm, 2);
-    kh_vt<<<dim3(a.cmap.tiles, nrhs, stage_chunks(a.g.nz, a.cmap.tiles, res)), kThreads, sm, s>>>(tp, a, which);
+    if (which == 0) {
+        if (a.gd) launch_hat_vt_t<0, true>(a, tp, nrhs, s);
+        else launch_hat_vt_t<0, false>(a, tp, nrhs, s);
+    } else {
+        if (a.gd) launch_hat_vt_t<1, true>(a, tp, nrhs, s);
+        else launch_hat_vt_t<1, false>(a, tp, nrhs, s);
+    }
 }
 
 void launch_hat_iter(const KArgs<float> &a, int nrhs, cudaStream_t s, cudaEvent_t *ev)
@@ -636,7 +651,8 @@ int launch_hat_iter_multi(const KArgs<float> *args, const int *nrhs, const int *
     HatMulti p;
     std::memset(&p, 0, sizeof p);
     p.ng = ng;
-    const int res = tma_resident(kh_vt_multi, sizeof(TmaSmem), 3);
+    const int res = tma_resident(kh_vt_multi<0>, sizeof(TmaSmem), 3);
+    tma_resident(kh_vt_multi<1>, sizeof(TmaSmem), 3);
     p.eb0[0] = p.sb0[0] = 0;
     for (int g = 0; g < ng; g++) {
         p.a[g] = args[g];
@@ -654,9 +670,9 @@ int launch_hat_iter_multi(const KArgs<float> *args, const int *nrhs, const int *
     counted(5);
     const size_t sm = sizeof(TmaSmem);
     kh_elem_multi<0><<<p.eb0[ng], kThreads, 0, s>>>(p);
-    kh_vt_multi<<<p.sb0[ng], kThreads, sm, s>>>(p, 0);
+    kh_vt_multi<0><<<p.sb0[ng], kThreads, sm, s>>>(p);
     kh_elem_multi<1><<<p.eb0[ng], kThreads, 0, s>>>(p);
-    kh_vt_multi<<<p.sb0[ng], kThreads, sm, s>>>(p, 1);
+    kh_vt_multi<1><<<p.sb0[ng], kThreads, sm, s>>>(p);
     kh_elem_multi<2><<<p.eb0[ng], kThreads, 0, s>>>(p);
     return 0;
 }
