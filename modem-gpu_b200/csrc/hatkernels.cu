@@ -604,7 +604,7 @@ template <int which, bool gd> static void launch_hat_vt_t(const KArgs<float> &a,
                                                            cudaStream_t s)
 {
     const size_t sm = sizeof(TmaSmem);
-    const int res = tma_resident(kh_vt<which, gd>, sm, 2);
+    const int res = tma_resident(kh_vt<which, gd>, sm, 2 + 2 * which + (gd ? 1 : 0));
     kh_vt<which, gd><<<dim3(a.cmap.tiles, nrhs, stage_chunks(a.g.nz, a.cmap.tiles, res)), kThreads, sm, s>>>(tp, a);
 }
 static void launch_hat_vt(const KArgs<float> &a, const TmaMaps *m, int which, int nrhs, cudaStream_t s)
@@ -651,8 +651,8 @@ int launch_hat_iter_multi(const KArgs<float> *args, const int *nrhs, const int *
     HatMulti p;
     std::memset(&p, 0, sizeof p);
     p.ng = ng;
-    const int res = tma_resident(kh_vt_multi<0>, sizeof(TmaSmem), 3);
-    tma_resident(kh_vt_multi<1>, sizeof(TmaSmem), 3);
+    const int res = tma_resident(kh_vt_multi<0>, sizeof(TmaSmem), 6);
+    tma_resident(kh_vt_multi<1>, sizeof(TmaSmem), 7);
     p.eb0[0] = p.sb0[0] = 0;
     for (int g = 0; g < ng; g++) {
         p.a[g] = args[g];

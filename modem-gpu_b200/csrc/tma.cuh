@@ -159,11 +159,14 @@ __device__ __forceinline__ TmaSmem &tma_smem()
     return *reinterpret_cast<TmaSmem *>(tma_raw);
 }
 
-// the chunk count of stagekernels.cu, for the resident blocks of these kernels
+// the chunk count of stagekernels.cu, for the resident blocks of these
+// kernels; `slot` identifies the kernel (its shared-memory attribute is set
+// the first time its slot is seen), so every kernel needs its own slot
+constexpr int kTmaSlots = 16;
 template <typename K> inline int tma_resident(K kern, size_t smem, int slot)
 {
     static std::mutex mu;
-    static int occ[64][4] = {};
+    static int occ[64][kTmaSlots] = {};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) dev = 0;
