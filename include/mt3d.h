@@ -124,6 +124,18 @@ MT3D_API int mt3d_set_restart(mt3d_handle h, int restart);
  * differ in rounding.  No counterpart in the reference. */
 MT3D_API int mt3d_set_fused(mt3d_handle h, int on);
 
+/* Polynomial preconditioner of the fused FP32 iteration: c > 0 replaces the
+ * diagonal preconditioner D^-1 by the first-degree Neumann polynomial
+ * M^-1 = c D^-1 (2 I - c A D^-1), two operator applications per
+ * preconditioned product (4 stencil launches an iteration instead of 2).
+ * c = 0 (default) keeps D^-1 alone.  c must lie in [0, 1.5]; an eigenvalue
+ * z of A D^-1 becomes 1 - (1 - c z)^2, so c below 2 / max|z| keeps the
+ * spectrum off zero, and c = 1 is the truncated Neumann series.  Applies
+ * to MT3D_PREC_MIXED with
+ * the fused iteration (mt3d_set_fused on); the FP64 refinement and the FP64
+ * fall-back keep D^-1.  No counterpart in the reference. */
+MT3D_API int mt3d_set_poly(mt3d_handle h, double c);
+
 /* Set the conductivity model (UpdateCond, f90/3D_MT/FWD/modelOperator3D.f90:
  * 211-232): ModelParamToEdge (LOGE, ModelMap.inc:88-188) and DivCorrSetUp. */
 MT3D_API int mt3d_update_cond(mt3d_handle h, const double *m_earth, double airCond);
@@ -249,9 +261,10 @@ MT3D_API int mt3d_fwdsolve_batch_device(mt3d_handle h, int nrhs, const double *o
  * (f90/MPI/Main_MPI.f90:1444-1649) for models of uneven size on one GPU:
  * the handles' FWDsolve3D phases run in lockstep on the first handle's
  * stream and the FP32 iterations of all grids share their launches (five per
- * iteration for the whole batch).  Every handle must be on one device, in
- * mixed precision with MT3D_SOLVER_BICG and the fused FP32 iteration
- * (mt3d_set_fused), with the same IterPerDivCor; 1 to 8 handles.  zchunks
+ * iteration for the whole batch, seven with the polynomial preconditioner).
+ * Every handle must be on one device, in mixed precision with
+ * MT3D_SOLVER_BICG and the fused FP32 iteration (mt3d_set_fused), with the
+ * same IterPerDivCor and mt3d_set_poly coefficient; 1 to 8 handles.  zchunks
  * (nh entries, may be NULL; 0 = the occupancy-based default) sets how many
  * chunks of node planes each grid's stencil blocks split the column into --
  * the knob mt3d/tune.py tunes.  Errors are reported by mt3d_last_error(NULL)

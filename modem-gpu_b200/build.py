@@ -55,11 +55,20 @@ def built_hash(path: str = LIB):
     return data[k + 9:k + 25].decode() if k >= 0 else None
 
 
+def compile_flags() -> list:
+    return ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
+                   "--expt-relaxed-constexpr", "-I", os.path.join(HERE, "..", "include")]
+
+
+def expected_hash() -> str:
+    """The source hash a library built from the current sources reports."""
+    return source_hash(compile_flags() + [f"{k}={v}" for k, v in sorted(FILE_FLAGS.items())])
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(LIBDIR, exist_ok=True)
-    flags = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
-                    "--expt-relaxed-constexpr", "-I", os.path.join(HERE, "..", "include")]
-    digest = source_hash(flags + [f"{k}={v}" for k, v in sorted(FILE_FLAGS.items())])
+    flags = compile_flags()
+    digest = expected_hash()
     if not force and built_hash() == digest:
         return LIB
     objdir = os.path.join(HERE, "_build")

@@ -340,6 +340,11 @@ int mt3d_set_fused(mt3d_handle h, int on)
     return wrap(h, [&] { return h->s.set_fused(on); });
 }
 
+int mt3d_set_poly(mt3d_handle h, double c)
+{
+    return wrap(h, [&] { return h->s.set_poly(c); });
+}
+
 int mt3d_set_wait_limit(mt3d_handle h, int polls)
 {
     return wrap(h, [&] { return h->s.set_wait_limit(polls); });

@@ -138,9 +138,9 @@ __device__ __forceinline__ float4 sub4(float4 a, float4 b) { return make_float4(
 
 // pairs of entries of block bx of a right-hand side (a.chunk entries per block)
 #define HAT_PAIRS(a, bx)                                                             \
-    const int n2 = (a).len / 2, c2 = (a).chunk / 2;                                  \
-    const int q1 = min(((bx) + 1) * c2, n2);                                          \
-    for (int q = (bx) * c2 + threadIdx.x; q < q1; q += kThreads)
+    const int hp_n2 = (a).len / 2, hp_c2 = (a).chunk / 2;                            \
+    const int q1 = min(((bx) + 1) * hp_c2, hp_n2);                                    \
+    for (int q = (bx) * hp_c2 + threadIdx.x; q < q1; q += kThreads)
 
 // u = rh + beta (u - omega vh); u = rh on the first iteration of a cycle or
 // after a restart (block bx of right-hand side r)
@@ -177,7 +177,7 @@ __device__ __forceinline__ void hat_s(const KArgs<float> &a, int r, int bx)
 // x += alpha u + omega sh (into the buffer that does not hold the best
 // iterate); rh = sh - omega th; rho = (z, rh).  The true residual norm of the
 // new iterate comes from the inner products of kh_vt 1 (BicgState::rn2).
-__device__ __forceinline__ void hat_xr(const KArgs<float> &a, int r, int bx)
+template <bool poly> __device__ __forceinline__ void hat_xr_t(const KArgs<float> &a, int r, int bx)
 {
     BicgState &st = a.st[r];
     if (st.status != KS_RUNNING || !a.ost[r].active) return;
@@ -190,13 +190,27 @@ __device__ __forceinline__ void hat_xr(const KArgs<float> &a, int r, int bx)
     const float4 *U = reinterpret_cast<const float4 *>(a.ph) + off;
     const float4 *SH = reinterpret_cast<const float4 *>(a.sh) + off;
     const float4 *TH = reinterpret_cast<const float4 *>(a.t) + off;
+    const float4 *W1 = reinterpret_cast<const float4 *>(a.p) + off;
+    const float4 *W2 = reinterpret_cast<const float4 *>(a.s) + off;
     float4 *RH = reinterpret_cast<float4 *>(a.r) + off;
     const float4 *Y = reinterpret_cast<const float4 *>(a.rt) + off;
+    // with the polynomial preconditioner the directions are M^-1 p =
+    // c (2 u - c w1) and M^-1 s = c (2 sh - c w2)
+    const float c2 = 2.f * a.pc, cc = a.pc * a.pc;
     double u[2] = {0.0, 0.0};
     HAT_PAIRS(a, bx)
     {
         const float4 sh = SH[q];
-        XD[q] = add4(add4(XS[q], c2mul2(al, U[q])), c2mul2(om, sh));
+        if (poly) {
+            const float4 pu = U[q], w1 = W1[q], w2 = W2[q];
+            const float4 dp = make_float4(c2 * pu.x - cc * w1.x, c2 * pu.y - cc * w1.y, c2 * pu.z - cc * w1.z,
+                                          c2 * pu.w - cc * w1.w);
+            const float4 ds = make_float4(c2 * sh.x - cc * w2.x, c2 * sh.y - cc * w2.y, c2 * sh.z - cc * w2.z,
+                                          c2 * sh.w - cc * w2.w);
+            XD[q] = add4(add4(XS[q], c2mul2(al, dp)), c2mul2(om, ds));
+        } else {
+            XD[q] = add4(add4(XS[q], c2mul2(al, U[q])), c2mul2(om, sh));
+        }
         const float4 rn = sub4(sh, c2mul2(om, TH[q]));
         RH[q] = rn;
         const float4 y = Y[q];  // conj(y) rh
@@ -245,6 +259,12 @@ __device__ __forceinline__ void hat_xr(const KArgs<float> &a, int r, int bx)
         st.beta = cd_mul(cd_div(st.rho, st.rho1), cd_div(st.alpha, st.omega));
         if (cd_zero(st.beta)) st.status = KS_BREAKDOWN;
     }
+}
+
+__device__ __forceinline__ void hat_xr(const KArgs<float> &a, int r, int bx)
+{
+    if (a.pc > 0.f) hat_xr_t<true>(a, r, bx);
+    else hat_xr_t<false>(a, r, bx);
 }
 
 // ---------------------------------------------------------------------------
@@ -472,13 +492,26 @@ __device__ __forceinline__ bool hat_march(TmaSmem &sm, const TmaParams &tp, cons
     return true;
 }
 
-// vh = D^-1 A u, (rt, v) -> alpha   (which = 0)
-// th = D^-1 A sh, (t, s)_W, (t, t)_W, (s, s)_W -> omega, ||r_new||   (which = 1)
-// for column tile bx and plane chunk bz of gz of right-hand side r; which and
-// the grad-div term are compile-time, so the march carries no branch on them
-template <int which, bool gd>
+// The operator launches of one iteration, by stage:
+//   diagonal preconditioner
+//     0  vh = D^-1 A u,            (rt, v) = sum conj(y) vh  -> alpha
+//     1  th = D^-1 A sh,           (t, s)_W, (t, t)_W, (s, s)_W -> omega, ||r||
+//   polynomial preconditioner M^-1 = c D^-1 (2 I - c A D^-1)
+//     2  w1 = D^-1 A u
+//     3  vh = c (2 w1 - c D^-1 A w1),  (rt, v)              -> alpha
+//     4  w2 = D^-1 A sh
+//     5  th = c (2 w2 - c D^-1 A w2),  (t, s)_W ... with s = sh read from memory
+// (D^-1 A (M^-1 p) = c (2 D^-1 A u - c D^-1 A w1) since u = D^-1 p.)  Stages
+// 0 and 2 stage u and, after a restart, write the new shadow y = W rh
+// (u = rh on that iteration).  For column tile bx and plane chunk bz of gz of
+// right-hand side r; the stage and the grad-div term are compile-time.
+template <int stage, bool gd>
 __device__ __forceinline__ void hat_vt(const TmaParams &tp, const KArgs<float> &a, int r, int bx, int bz, int gz)
 {
+    constexpr bool kv = stage == 0 || stage == 3;  // (rt, v) and alpha
+    constexpr bool kt = stage == 1 || stage == 5;  // omega and ||r||
+    constexpr bool poly = stage == 3 || stage == 5;
+    constexpr bool dots = kv || kt;
     BicgState &st = a.st[r];
     if (st.status != KS_RUNNING || !a.ost[r].active) return;
     if (a.sweeps && threadIdx.x == 0 && bx == 0 && bz == 0) atomicAdd(a.sweeps, 1ULL);
@@ -486,43 +519,48 @@ __device__ __forceinline__ void hat_vt(const TmaParams &tp, const KArgs<float> &
     tma_tile_at(a.cmap, bx, i0, j0);
     tma_range_at(a.g.nz, bz, gz, k0, k1);
     const size_t off = (size_t)r * a.stride;
-    float2 *out = (which ? a.t : a.v) + off;
-    // inner products summed per edge in FP64 (per-plane FP32 partial sums
-    // changed the Krylov rounding enough to send more right-hand sides to
-    // the FP64 fallback)
+    float2 *out = (stage == 0 || stage == 3 ? a.v : stage == 2 ? a.p : stage == 4 ? a.s : a.t) + off;
     float2 *Yr = a.rt + off;
     // after a restart (first iteration, pad set) the shadow becomes the
     // current residual: y = W rh, rh being the staged u of this launch
-    const bool reset = which == 0 && st.first && st.pad;
+    const bool reset = (stage == 0 || stage == 2) && st.first && st.pad;
+    const float2 *aux = nullptr;
+    if (kv && !reset) aux = Yr;
+    if (stage == 5) aux = a.sh + off;
+    const float c2 = 2.f * a.pc, cc = a.pc * a.pc;
+    // inner products summed per edge in FP64 (per-plane FP32 partial sums
+    // changed the Krylov rounding enough to send more right-hand sides to
+    // the FP64 fallback)
     double u[4] = {0.0, 0.0, 0.0, 0.0};
     TmaSmem &sm = tma_smem();
     const bool ok = hat_march<gd>(
-        sm, tp, a.g, a.pl, r, (which == 0 && !reset) ? Yr : nullptr, (float)(a.dsgn * a.ost[r].omega * kMu0), i0,
-        j0, k0, k1, a.err, a.wait_limit,
-        [&](int e, bool inn, float2 y, float2 x, float W, float2 ya) {
+        sm, tp, a.g, a.pl, r, aux, (float)(a.dsgn * a.ost[r].omega * kMu0), i0, j0, k0, k1, a.err, a.wait_limit,
+        [&](int e, bool inn, float2 y, float2 x, float W, float2 xa) {
             if (reset) Yr[e] = inn ? make_float2(W * x.x, W * x.y) : make_float2(0.f, 0.f);
+            if (poly && inn) y = make_float2(c2 * x.x - cc * y.x, c2 * x.y - cc * y.y);  // c (2 x - c D^-1 A x)
             if (inn) {
-                if (which == 0) {
-                    const float2 z = reset ? make_float2(W * x.x, W * x.y) : ya;
+                if (kv) {
+                    const float2 z = reset ? make_float2(W * x.x, W * x.y) : xa;
                     u[0] += (double)z.x * y.x + (double)z.y * y.y;  // conj(y) vh
                     u[1] += (double)z.x * y.y - (double)z.y * y.x;
-                } else {
+                } else if (kt) {
+                    const float2 sv = stage == 5 ? xa : x;
                     const double w = W;
-                    u[0] += w * ((double)y.x * x.x + (double)y.y * x.y);  // conj(t) s
-                    u[1] += w * ((double)y.x * x.y - (double)y.y * x.x);
+                    u[0] += w * ((double)y.x * sv.x + (double)y.y * sv.y);  // conj(t) s
+                    u[1] += w * ((double)y.x * sv.y - (double)y.y * sv.x);
                     u[2] += w * ((double)y.x * y.x + (double)y.y * y.y);
-                    u[3] += w * ((double)x.x * x.x + (double)x.y * x.y);
+                    u[3] += w * ((double)sv.x * sv.x + (double)sv.y * sv.y);
                 }
             }
             out[e] = y;
         });
-    if (!ok) return;
+    if (!ok || !dots) return;
     // the march has read its last staged plane: the field ring is free
     double tot[4];
     if (block_reduce_last_in<4>(u, a.parts, a.cnt, r, bx + a.cmap.tiles * bz, a.cmap.tiles * gz, tot,
                                 reinterpret_cast<double *>(sm.fld[0]), reinterpret_cast<int *>(sm.fld[1])) &&
         threadIdx.x == 0) {
-        if (which == 0) {
+        if (kv) {
             fin_v(st, tot);
             st.pad = 0;
         } else {
@@ -543,17 +581,17 @@ __device__ __forceinline__ void hat_vt(const TmaParams &tp, const KArgs<float> &
 __global__ void __launch_bounds__(kThreads) kh_u(KArgs<float> a) { hat_u(a, blockIdx.y, blockIdx.x); }
 __global__ void __launch_bounds__(kThreads) kh_s(KArgs<float> a) { hat_s(a, blockIdx.y, blockIdx.x); }
 __global__ void __launch_bounds__(kThreads) kh_xr(KArgs<float> a) { hat_xr(a, blockIdx.y, blockIdx.x); }
-template <int which, bool gd>
+template <int stage, bool gd>
 __global__ void __launch_bounds__(kThreads, 4) kh_vt(const __grid_constant__ TmaParams tp, KArgs<float> a)
 {
-    hat_vt<which, gd>(tp, a, blockIdx.y, blockIdx.x, blockIdx.z, gridDim.z);
+    hat_vt<stage, gd>(tp, a, blockIdx.y, blockIdx.x, blockIdx.z, gridDim.z);
 }
 
 // the grids of a multi-grid batch, passed by value: each grid's arguments,
 // its tensor maps (u and sh inputs) and where its blocks start in the flat
 // launches
 struct alignas(64) HatMulti {
-    TmaParams tp[kMaxMultiGrids][2];
+    TmaParams tp[kMaxMultiGrids][4];  // inputs u, sh, w1, w2
     KArgs<float> a[kMaxMultiGrids];
     int ng;
     int nr[kMaxMultiGrids];            // right-hand sides of each grid
@@ -577,7 +615,12 @@ template <int K> __global__ void __launch_bounds__(kThreads) kh_elem_multi(const
     else if (K == 1) hat_s(a, r, bx);
     else hat_xr(a, r, bx);
 }
-template <int which> __global__ void __launch_bounds__(kThreads, 4) kh_vt_multi(const __grid_constant__ HatMulti p)
+// input map of each stage: u, sh, u, w1, sh, w2
+__host__ __device__ constexpr int stage_input(int stage)
+{
+    return stage == 0 || stage == 2 ? 0 : stage == 1 || stage == 4 ? 1 : stage == 3 ? 2 : 3;
+}
+template <int stage> __global__ void __launch_bounds__(kThreads, 4) kh_vt_multi(const __grid_constant__ HatMulti p)
 {
     const int g = multi_grid_of(p.sb0, p.ng, blockIdx.x);
     const KArgs<float> &a = p.a[g];
@@ -585,8 +628,9 @@ template <int which> __global__ void __launch_bounds__(kThreads, 4) kh_vt_multi(
     const int local = blockIdx.x - p.sb0[g];
     const int r = local / per, rem = local - r * per;
     const int bz = rem / a.cmap.tiles, bx = rem - bz * a.cmap.tiles;
-    if (a.gd) hat_vt<which, true>(p.tp[g][which], a, r, bx, bz, p.zch[g]);
-    else hat_vt<which, false>(p.tp[g][which], a, r, bx, bz, p.zch[g]);
+    const TmaParams &tp = p.tp[g][stage_input(stage)];
+    if (a.gd) hat_vt<stage, true>(tp, a, r, bx, bz, p.zch[g]);
+    else hat_vt<stage, false>(tp, a, r, bx, bz, p.zch[g]);
 }
 
 // ---------------------------------------------------------------------------
@@ -600,45 +644,55 @@ void launch_hat_cast(const KArgs<float> &a, const double2 *r64, size_t stride64,
     kh_cast<<<dim3(hat_grid(a.g.nE), nrhs), kThreads, 0, s>>>(a, r64, stride64);
 }
 
-template <int which, bool gd> static void launch_hat_vt_t(const KArgs<float> &a, const TmaParams &tp, int nrhs,
+template <int stage, bool gd> static void launch_hat_vt_t(const KArgs<float> &a, const TmaParams &tp, int nrhs,
                                                            cudaStream_t s)
 {
     const size_t sm = sizeof(TmaSmem);
-    const int res = tma_resident(kh_vt<which, gd>, sm, 2 + 2 * which + (gd ? 1 : 0));
-    kh_vt<which, gd><<<dim3(a.cmap.tiles, nrhs, stage_chunks(a.g.nz, a.cmap.tiles, res)), kThreads, sm, s>>>(tp, a);
+    const int res = tma_resident(kh_vt<stage, gd>, sm, 2 + 2 * stage + (gd ? 1 : 0));
+    kh_vt<stage, gd><<<dim3(a.cmap.tiles, nrhs, stage_chunks(a.g.nz, a.cmap.tiles, res)), kThreads, sm, s>>>(tp, a);
 }
-static void launch_hat_vt(const KArgs<float> &a, const TmaMaps *m, int which, int nrhs, cudaStream_t s)
+template <int stage> static void launch_hat_stage(const KArgs<float> &a, int nrhs, cudaStream_t s)
 {
     counted(1);
+    const TmaMaps *m = a.tma;
     TmaParams tp;
-    tp.in = which ? m->sh : m->ph;
+    constexpr int in = stage_input(stage);
+    tp.in = in == 0 ? m->ph : in == 1 ? m->sh : in == 2 ? m->pw : m->sw;
     tp.sig = m->sig;
     tp.node = m->node;
-    if (which == 0) {
-        if (a.gd) launch_hat_vt_t<0, true>(a, tp, nrhs, s);
-        else launch_hat_vt_t<0, false>(a, tp, nrhs, s);
-    } else {
-        if (a.gd) launch_hat_vt_t<1, true>(a, tp, nrhs, s);
-        else launch_hat_vt_t<1, false>(a, tp, nrhs, s);
-    }
+    if (a.gd) launch_hat_vt_t<stage, true>(a, tp, nrhs, s);
+    else launch_hat_vt_t<stage, false>(a, tp, nrhs, s);
 }
 
+// one iteration; the events bracket the operator launches (the two of the
+// polynomial preconditioner's first and second half together)
 void launch_hat_iter(const KArgs<float> &a, int nrhs, cudaStream_t s, cudaEvent_t *ev)
 {
     counted(3);
     const dim3 grid(a.nblk, nrhs);
+    const bool poly = a.pc > 0.f;
     kh_u<<<grid, kThreads, 0, s>>>(a);
     if (ev) cudaEventRecord(ev[0], s);
-    launch_hat_vt(a, a.tma, 0, nrhs, s);
+    if (poly) {
+        launch_hat_stage<2>(a, nrhs, s);
+        launch_hat_stage<3>(a, nrhs, s);
+    } else {
+        launch_hat_stage<0>(a, nrhs, s);
+    }
     if (ev) cudaEventRecord(ev[1], s);
     kh_s<<<grid, kThreads, 0, s>>>(a);
     if (ev) cudaEventRecord(ev[2], s);
-    launch_hat_vt(a, a.tma, 1, nrhs, s);
+    if (poly) {
+        launch_hat_stage<4>(a, nrhs, s);
+        launch_hat_stage<5>(a, nrhs, s);
+    } else {
+        launch_hat_stage<1>(a, nrhs, s);
+    }
     if (ev) cudaEventRecord(ev[3], s);
     kh_xr<<<grid, kThreads, 0, s>>>(a);
 }
 
-void launch_hat_apply(const KArgs<float> &a, int nrhs, cudaStream_t s) { launch_hat_vt(a, a.tma, 0, nrhs, s); }
+void launch_hat_apply(const KArgs<float> &a, int nrhs, cudaStream_t s) { launch_hat_stage<0>(a, nrhs, s); }
 
 // one iteration of the fused FP32 BiCGStab over the grids of a multi-grid
 // batch: five launches in all, each over the right-hand sides of every grid
@@ -651,15 +705,24 @@ int launch_hat_iter_multi(const KArgs<float> *args, const int *nrhs, const int *
     HatMulti p;
     std::memset(&p, 0, sizeof p);
     p.ng = ng;
-    const int res = tma_resident(kh_vt_multi<0>, sizeof(TmaSmem), 6);
-    tma_resident(kh_vt_multi<1>, sizeof(TmaSmem), 7);
+    const int res = tma_resident(kh_vt_multi<0>, sizeof(TmaSmem), 14);
+    for (int q = 1; q < 6; q++) {
+        const size_t smb = sizeof(TmaSmem);
+        if (q == 1) tma_resident(kh_vt_multi<1>, smb, 15);
+        if (q == 2) tma_resident(kh_vt_multi<2>, smb, 16);
+        if (q == 3) tma_resident(kh_vt_multi<3>, smb, 17);
+        if (q == 4) tma_resident(kh_vt_multi<4>, smb, 18);
+        if (q == 5) tma_resident(kh_vt_multi<5>, smb, 19);
+    }
     p.eb0[0] = p.sb0[0] = 0;
     for (int g = 0; g < ng; g++) {
         p.a[g] = args[g];
         p.nr[g] = nrhs[g];
         p.tp[g][0].in = args[g].tma->ph;
         p.tp[g][1].in = args[g].tma->sh;
-        for (int w = 0; w < 2; w++) {
+        p.tp[g][2].in = args[g].tma->pw;
+        p.tp[g][3].in = args[g].tma->sw;
+        for (int w = 0; w < 4; w++) {
             p.tp[g][w].sig = args[g].tma->sig;
             p.tp[g][w].node = args[g].tma->node;
         }
@@ -667,12 +730,25 @@ int launch_hat_iter_multi(const KArgs<float> *args, const int *nrhs, const int *
         p.eb0[g + 1] = p.eb0[g] + nrhs[g] * args[g].nblk;
         p.sb0[g + 1] = p.sb0[g] + nrhs[g] * args[g].cmap.tiles * p.zch[g];
     }
-    counted(5);
+    // the polynomial preconditioner is used when the first grid's handle
+    // has it (every handle of a batch shares the control)
+    const bool poly = args[0].pc > 0.f;
+    counted(poly ? 7 : 5);
     const size_t sm = sizeof(TmaSmem);
     kh_elem_multi<0><<<p.eb0[ng], kThreads, 0, s>>>(p);
-    kh_vt_multi<0><<<p.sb0[ng], kThreads, sm, s>>>(p);
+    if (poly) {
+        kh_vt_multi<2><<<p.sb0[ng], kThreads, sm, s>>>(p);
+        kh_vt_multi<3><<<p.sb0[ng], kThreads, sm, s>>>(p);
+    } else {
+        kh_vt_multi<0><<<p.sb0[ng], kThreads, sm, s>>>(p);
+    }
     kh_elem_multi<1><<<p.eb0[ng], kThreads, 0, s>>>(p);
-    kh_vt_multi<1><<<p.sb0[ng], kThreads, sm, s>>>(p);
+    if (poly) {
+        kh_vt_multi<4><<<p.sb0[ng], kThreads, sm, s>>>(p);
+        kh_vt_multi<5><<<p.sb0[ng], kThreads, sm, s>>>(p);
+    } else {
+        kh_vt_multi<1><<<p.sb0[ng], kThreads, sm, s>>>(p);
+    }
     kh_elem_multi<2><<<p.eb0[ng], kThreads, 0, s>>>(p);
     return 0;
 }

@@ -70,6 +70,9 @@ template <typename T> struct KArgs {
     // BiCGStab has no place for
     QmrState *qst;
     C2<T> *q, *w, *d;
+    // fused FP32 iteration: coefficient c of the polynomial preconditioner
+    // c D^-1 (2 I - c A D^-1) (0: the diagonal preconditioner alone)
+    float pc;
 };
 
 // arguments of the divergence-correction kernels (FP64)
@@ -126,8 +129,8 @@ void launch_stage_res64(const KArgs<double> &a, int nrhs, cudaStream_t s);
 // TMA-staged FP32 stencil kernels on the padded layout (colstencil == 3):
 // tensor maps of the input vectors, of sigma and of the signed node weights
 struct TmaMaps;
-int tma_maps_build(TmaMaps *m, const float2 *x0, const float2 *ph, const float2 *sh, const float *sig,
-                   const float *gdn, PadLayout pl, int nrhs);
+int tma_maps_build(TmaMaps *m, const float2 *x0, const float2 *ph, const float2 *sh, const float2 *pw,
+                   const float2 *sw, const float *sig, const float *gdn, PadLayout pl, int nrhs);
 TmaMaps *tma_maps_new();
 void tma_maps_free(TmaMaps *m);
 void launch_tma_init(const KArgs<float> &a, const TmaMaps *m, int nrhs, cudaStream_t s);

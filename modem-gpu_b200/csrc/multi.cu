@@ -13,8 +13,9 @@
 // leaving most of it idle.
 //
 // Conditions: all handles on one device, mixed precision with the fused FP32
-// iteration, BiCGStab + diagonal, the same IterPerDivCor (the FP32 cycles
-// run in step); at most kMaxMultiGrids handles.
+// iteration, BiCGStab + diagonal, the same IterPerDivCor and polynomial
+// preconditioner coefficient (the FP32 cycles run in step); at most
+// kMaxMultiGrids handles.
 #include <algorithm>
 #include <string>
 #include <vector>
@@ -49,9 +50,9 @@ int fwdsolve_multi(int nh, Solver *const *hs, const int *nrhs, const double *con
             return 5;
         }
         if (h->ctl.precision != 1 || h->ctl.solver != 1 || !h->ctl.fused ||
-            h->ctl.IterPerDivCor != h0->ctl.IterPerDivCor) {
+            h->ctl.IterPerDivCor != h0->ctl.IterPerDivCor || h->ctl.poly != h0->ctl.poly) {
             err = "mt3d_fwdsolve_multi: every handle needs mixed precision, BiCGStab + diagonal, the fused FP32 "
-                  "iteration and the same IterPerDivCor";
+                  "iteration, the same IterPerDivCor and the same polynomial coefficient";
             return 5;
         }
     }

@@ -316,7 +316,8 @@ int Solver::tma_ready()
     if (!tma_stale_) return 0;
     if (!tma_) tma_ = tma_maps_new();
     Workspace &w = ws_;
-    if (tma_maps_build(tma_, w.f_x0.as<float2>(), w.f_ph.as<float2>(), w.f_sh.as<float2>(),
+    if (tma_maps_build(tma_, w.f_x0.as<float2>(), w.f_ph.as<float2>(), w.f_sh.as<float2>(), w.f_p.as<float2>(),
+                       w.f_s.as<float2>(),
                        (ctl.formulation == 1 ? sigsP32_ : sigP32_).as<float>(), gdnP32_.as<float>(), pl_, w.nrhs))
         return fail(4, "cuTensorMapEncodeTiled failed for the padded FP32 vectors");
     tma_stale_ = false;
@@ -512,6 +513,7 @@ template <> KArgs<float> Solver::kargs<float>(int nrhs, int)
     a.len = (int)nE;
     a.err = errf_.as<int>();
     a.wait_limit = wait_limit_;
+    a.pc = (float)ctl.poly;
     if (w.padded) {
         // padded layout: the elementwise kernels sweep the padded length and
         // the stencil runs on the TMA-staged kernels
@@ -686,6 +688,13 @@ KArgs<float> Solver::hat_args(int nrhs)
     a.maxit = ctl.IterPerDivCor;
     a.sweeps = nullptr;
     return a;
+}
+
+int Solver::set_poly(double c)
+{
+    if (!(c >= 0.0 && c <= 1.5)) return fail(5, "mt3d_set_poly: the coefficient must lie in [0, 1.5]");
+    ctl.poly = c;
+    return 0;
 }
 int Solver::hat_cycle_begin(int nrhs, KArgs<float> &a)
 {

@@ -20,6 +20,7 @@ struct Control {
     int formulation = 0;  // 0 curl-curl + divergence correction (MF), 1 curl-curl + grad-div (SP2)
     int restart = 120;    // grad-div formulation: BiCGStab restart length (cuBiCG's 120; 0 never)
     int fused = 1;        // mixed precision: FP32 iteration in preconditioned variables (hatkernels.cu)
+    double poly = 0.0;    // fused iteration: polynomial preconditioner coefficient (0: diagonal alone)
 };
 
 struct Diag {
@@ -127,6 +128,7 @@ class Solver {
     int set_stream(void *s);
     int set_wait_limit(int polls);
     int set_fused(int on);
+    int set_poly(double c);
     int profile(int enable);
     int kernel_time(int precision, int *launches, double *ms, int64_t *sweeps);
     int get_cond(double *sigma_e, double *divcorr, double *node_w);

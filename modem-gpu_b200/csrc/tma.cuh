@@ -25,6 +25,7 @@ namespace mt3d {
 
 struct TmaMaps {
     CUtensorMap x0, ph, sh;  // input vectors [nrhs][3][Pz][Py][2 Px] (float)
+    CUtensorMap pw, sw;      // the polynomial preconditioner's intermediates (vectors p, s)
     CUtensorMap sig;         // sigma [3][Pz][Py][Px] (float)
     CUtensorMap node;        // signed node weights [Pz][Py][Px] (float)
     int ok;
@@ -162,7 +163,7 @@ __device__ __forceinline__ TmaSmem &tma_smem()
 // the chunk count of stagekernels.cu, for the resident blocks of these
 // kernels; `slot` identifies the kernel (its shared-memory attribute is set
 // the first time its slot is seen), so every kernel needs its own slot
-constexpr int kTmaSlots = 16;
+constexpr int kTmaSlots = 20;
 template <typename K> inline int tma_resident(K kern, size_t smem, int slot)
 {
     static std::mutex mu;

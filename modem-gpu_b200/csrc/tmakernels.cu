@@ -336,8 +336,8 @@ TmaMaps *tma_maps_new()
 }
 void tma_maps_free(TmaMaps *m) { delete m; }
 
-int tma_maps_build(TmaMaps *m, const float2 *x0, const float2 *ph, const float2 *sh, const float *sig,
-                   const float *gdn, PadLayout pl, int nrhs)
+int tma_maps_build(TmaMaps *m, const float2 *x0, const float2 *ph, const float2 *sh, const float2 *pw,
+                   const float2 *sw, const float *sig, const float *gdn, PadLayout pl, int nrhs)
 {
     m->ok = 0;
     const cuuint64_t Px = pl.Px, Py = pl.Py, Pz = pl.Pz;
@@ -353,6 +353,7 @@ int tma_maps_build(TmaMaps *m, const float2 *x0, const float2 *ph, const float2 
     const cuuint64_t ns[2] = {Px * 4, Px * Py * 4};
     const cuuint32_t nb[3] = {kNW, kNR, 1};
     if (encode(&m->x0, x0, 4, vd, vs, vb) || encode(&m->ph, ph, 4, vd, vs, vb) || encode(&m->sh, sh, 4, vd, vs, vb) ||
+        encode(&m->pw, pw, 4, vd, vs, vb) || encode(&m->sw, sw, 4, vd, vs, vb) ||
         encode(&m->sig, sig, 4, sd, ss, sb) || encode(&m->node, gdn ? gdn : sig, 3, nd, ns, nb))
         return 1;
     m->ok = 1;

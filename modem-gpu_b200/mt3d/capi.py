@@ -28,6 +28,7 @@ EXPORTS = ["mt3d_version", "mt3d_device_count", "mt3d_create", "mt3d_destroy", "
            "mt3d_mult_aii_device_noalloc", "mt3d_bicg", "mt3d_fwdsolve",
            "mt3d_fwdsolve_batch", "mt3d_fwdsolve_batch_device", "mt3d_fwdsolve_multi",
            "mt3d_fwdsolve_multi_device", "mt3d_set_stream", "mt3d_set_wait_limit", "mt3d_set_fused",
+           "mt3d_set_poly",
            "mt3d_apply_kernel", "mt3d_profile",
            "mt3d_kernel_time", "mt3d_get_diag", "mt3d_get_batch_diag", "mt3d_pmult_t", "mt3d_impedance", "mt3d_impedance_device", "mt3d_lmult_t", "mt3d_lmult_t_device", "mt3d_jmult_t", "mt3d_jmult_t_device", "mt3d_write_soln", "mt3d_read_soln", "mt3d_read_soln_header", "mt3d_launch_counter", "mt3d_alloc_counter",
            "mt3d_last_error"]
@@ -41,6 +42,19 @@ class MT3DError(RuntimeError):
         self.code = code
 
 
+def check_fresh(path: str = LIB_PATH):
+    """Raise if the library at `path` was built from other sources than the
+    ones beside it (a stale build would run old kernels under new tests)."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("_mt3d_build", os.path.join(os.path.dirname(_HERE), "build.py"))
+    b = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(b)
+    have, want = b.built_hash(path), b.expected_hash()
+    if have != want:
+        raise RuntimeError(f"{path} was built from sources {have}, the tree holds {want}: rebuild it "
+                           "(python modem-gpu_b200/build.py)")
+
+
 def load(path: str = LIB_PATH):
     """Load libmt3d.so; raises if it is missing (build it with build.py)."""
     global _lib
@@ -48,6 +62,8 @@ def load(path: str = LIB_PATH):
         return _lib
     if not os.path.exists(path):
         raise FileNotFoundError(f"{path} not found: build the CUDA library first (python modem-gpu_b200/build.py)")
+    if os.path.abspath(path) == os.path.abspath(LIB_PATH):
+        check_fresh(path)
     L = C.CDLL(path)
     P = C.c_void_p
     D = C.POINTER(C.c_double)
@@ -83,6 +99,7 @@ def load(path: str = LIB_PATH):
     for name in ("mt3d_fwdsolve_multi", "mt3d_fwdsolve_multi_device"):
         getattr(L, name).argtypes = [I, C.POINTER(P), IP, PP, PP, PP, PP, PP, PP, IP]
     L.mt3d_set_fused.argtypes = [P, I]
+    L.mt3d_set_poly.argtypes = [P, C.c_double]
     L.mt3d_jmult_t.argtypes = [P, C.c_double, I, D, D, D, D, D, D, D]
     L.mt3d_jmult_t_device.argtypes = [P, C.c_double, I, D, D, C.c_void_p, D, D, C.c_void_p, C.c_void_p]
     L.mt3d_apply_kernel.argtypes = [P, I, D, D]
@@ -345,6 +362,11 @@ class Solver:
 
     def set_fused(self, on: bool = True):
         self._check(self.L.mt3d_set_fused(self.h, int(bool(on))))
+
+    def set_poly(self, c: float):
+        """Polynomial preconditioner c D^-1 (2 I - c A D^-1) in the fused FP32
+        iteration (0: the diagonal preconditioner alone)."""
+        self._check(self.L.mt3d_set_poly(self.h, float(c)))
 
     def set_wait_limit(self, polls: int):
         self._check(self.L.mt3d_set_wait_limit(self.h, int(polls)))

@@ -178,3 +178,42 @@ def test_bounded_wait_reports_timeout_and_recovers(cuda):
         e, rc = s.fwdsolve(bc=bcv)
         assert rc == 0
         assert s.diagnostics()["final_relres"] <= 1e-7
+
+
+@pytest.mark.parametrize("formulation", [capi.FORM_CCDC, capi.FORM_CCGD], ids=["ccdc", "ccgd"])
+def test_polynomial_preconditioner_reaches_the_same_solution(cuda, formulation):
+    """The fused FP32 iteration with the polynomial preconditioner
+    c D^-1 (2 I - c A D^-1) (mt3d_set_poly, c = 0.8) and with the diagonal
+    one: both reach the FP64 tolerance 1e-8 and the same field within it
+    (relative 2-norm 1e-5 on the edges where the field is unique)."""
+    from helpers import earth_mask
+    from mt3d import bc as mbc
+    g = tiled_grid()
+    m = random_model(g, seed=11)
+    omega = 2 * np.pi * 3.0
+    bcv = mbc.boundary_1d(m, omega, 2)
+    out, its = [], []
+    for c in (0.0, 0.8):
+        s = capi.Solver(g)
+        s.set_formulation(formulation)
+        s.update_cond(m.m_earth, m.air_cond)
+        s.update_freq(omega)
+        s.set_control(IterPerDivCor=200, MaxDivCor=40, tolEMfwd=1e-8, precision=capi.PREC_MIXED)
+        s.set_poly(c)
+        e, rc = s.fwdsolve(bc=bcv)
+        d = s.diagnostics()
+        assert rc == 0 and d["final_relres"] <= 1e-8
+        out.append(e)
+        its.append(d["nIterTotal"])
+    print(f"formulation {formulation}: iterations diagonal {its[0]}, polynomial {its[1]}")
+    em = earth_mask(g, m)
+    assert relerr(out[0][em], out[1][em]) < 1e-5
+
+
+def test_polynomial_coefficient_range(cuda):
+    s = capi.Solver(tiled_grid())
+    for bad in (-0.1, 1.6, float("nan")):
+        with pytest.raises(capi.MT3DError):
+            s.set_poly(bad)
+    s.set_poly(1.0)
+    s.set_poly(0.0)

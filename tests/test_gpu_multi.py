@@ -86,6 +86,36 @@ def test_multi_device_entry_matches_host_entry(mprob):
         assert np.array_equal(d.cpu().numpy(), e)
 
 
+def test_multi_with_polynomial_preconditioner(mprob):
+    """The batch with the polynomial preconditioner (seven launches an
+    iteration) reaches the per-grid diagonal-preconditioned solutions; a
+    batch whose handles disagree on the coefficient is refused."""
+    probs, ss = mprob
+    refs = []
+    for (g, m, om, bc, src, tr), s in zip(probs, ss):
+        ref, _, rc1 = s.fwdsolve_batch(om, trans=tr, bc=bc, src=src)
+        assert rc1 == 0
+        refs.append(ref)
+    try:
+        ss[0].set_poly(0.8)
+        es = [np.zeros((5, g.n_edges), complex) for g, *_ in probs]
+        with pytest.raises(capi.MT3DError):
+            capi.fwdsolve_multi(ss, [p[2] for p in probs], es, trans=[p[5] for p in probs],
+                                bc=[p[3] for p in probs], src=[p[4] for p in probs])
+        for s in ss[1:]:
+            s.set_poly(0.8)
+        st, rc = capi.fwdsolve_multi(ss, [p[2] for p in probs], es, trans=[p[5] for p in probs],
+                                     bc=[p[3] for p in probs], src=[p[4] for p in probs])
+        assert rc == 0 and all(np.all(x == 0) for x in st)
+        for (g, m, *_), e, ref in zip(probs, es, refs):
+            em = earth_mask(g, m)
+            for r in range(5):
+                assert relerr(e[r][em], ref[r][em]) < 1e-5, (g.nx, r)
+    finally:
+        for s in ss:
+            s.set_poly(0.0)
+
+
 def test_chunk_tuner_returns_and_caches_a_choice(mprob, tmp_path):
     import torch
     from mt3d import tune
