@@ -61,8 +61,11 @@ def compile_flags() -> list:
 
 
 def expected_hash() -> str:
-    """The source hash a library built from the current sources reports."""
-    return source_hash(compile_flags() + [f"{k}={v}" for k, v in sorted(FILE_FLAGS.items())])
+    """The source hash a library built from the current sources reports.
+    Paths in the flags are hashed relative to this directory, so a tree
+    copied elsewhere (the library travels with it) keeps its hash."""
+    flags = [os.path.relpath(f, HERE) if os.path.isabs(f) else f for f in compile_flags()]
+    return source_hash(flags + [f"{k}={v}" for k, v in sorted(FILE_FLAGS.items())])
 
 
 def build(force: bool = False, verbose: bool = False) -> str:

@@ -279,15 +279,15 @@ template <int N> __device__ __forceinline__ void warp_sum(double (&v)[N])
 // Reduce v over the block, write this block's partial, and return true in
 // the (single) last block of this right-hand side, whose thread 0 then holds
 // the total in `tot`.  `parts` is [nrhs][nblk][N]; `cnt` one counter per rhs.
-// As block_reduce_last below, with its shared scratch (N * kThreads / 32
-// doubles and one flag) supplied by the caller, e.g. part of a ring buffer
-// the block no longer reads.
-template <int N>
+// As block_reduce_last below, for blocks of NT threads, with its shared
+// scratch (N * NT / 32 doubles and one flag) supplied by the caller, e.g.
+// part of a ring buffer the block no longer reads.
+template <int N, int NT = kThreads>
 __device__ __forceinline__ bool block_reduce_last_in(double (&v)[N], double *__restrict__ parts, unsigned *cnt,
                                                      int rhs, int blk, int nblk, double (&tot)[N], double *scratch,
                                                      int *flag)
 {
-    double(*sm)[kThreads / 32] = reinterpret_cast<double(*)[kThreads / 32]>(scratch);
+    double(*sm)[NT / 32] = reinterpret_cast<double(*)[NT / 32]>(scratch);
     int &s_last = *flag;
     warp_sum<N>(v);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -300,7 +300,7 @@ __device__ __forceinline__ bool block_reduce_last_in(double (&v)[N], double *__r
 #pragma unroll
         for (int n = 0; n < N; n++) {
             double s = 0.0;
-            for (int q = 0; q < kThreads / 32; q++) s += sm[n][q];
+            for (int q = 0; q < NT / 32; q++) s += sm[n][q];
             p[n] = s;
         }
         __threadfence();
@@ -314,7 +314,7 @@ __device__ __forceinline__ bool block_reduce_last_in(double (&v)[N], double *__r
 #pragma unroll
     for (int n = 0; n < N; n++) acc[n] = 0.0;
     const volatile double *pp = parts + (size_t)rhs * nblk * N;
-    for (int b = threadIdx.x; b < nblk; b += kThreads)
+    for (int b = threadIdx.x; b < nblk; b += NT)
 #pragma unroll
         for (int n = 0; n < N; n++) acc[n] += pp[(size_t)b * N + n];
     warp_sum<N>(acc);
@@ -327,7 +327,7 @@ __device__ __forceinline__ bool block_reduce_last_in(double (&v)[N], double *__r
 #pragma unroll
         for (int n = 0; n < N; n++) {
             double s = 0.0;
-            for (int q = 0; q < kThreads / 32; q++) s += sm[n][q];
+            for (int q = 0; q < NT / 32; q++) s += sm[n][q];
             tot[n] = s;
         }
         cnt[rhs] = 0u;

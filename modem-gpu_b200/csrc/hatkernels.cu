@@ -273,29 +273,38 @@ __device__ __forceinline__ void hat_xr(const KArgs<float> &a, int r, int bx)
 // ---------------------------------------------------------------------------
 
 // March planes [k0, k1) of tile (i0, j0), right-hand side r, calling
-// f(e, interior, yhat, x_e, W, aux_e) for every existing edge of the thread's
-// node column: yhat = D^-1 (A x)_e and W = |D_e|^2 at interior edges (zero
-// otherwise), e the padded index, aux_e the entry of the vector aux (read one
-// plane ahead, zero when aux is null).  Returns false (all threads of the
-// block alike) when a wait gave up.
+// f(e, yhat, x_e, W, aux_e) for the three edge slots (Ex, Ey, Ez) of every
+// node of the thread's two columns, padding slots included: yhat =
+// D^-1 (A x)_e and W = |D_e|^2 at interior edges (zero otherwise), e the
+// padded index, aux_e the entry of the vector aux (read one plane ahead,
+// zero when aux is null).  A block of kHatThreads threads covers the 32 x 8
+// node tile: thread (tx, ty) takes the node columns (i0 + tx, j0 + ty) and
+// (i0 + tx, j0 + ty + 4), so the per-plane work of a thread (waits,
+// barriers, plane geometry, loop control) is shared by six edges and the
+// register budget of four blocks per SM is 128 per thread.  Returns false
+// (all threads of the block alike) when a wait gave up.
 template <bool gd, typename F>
 __device__ __forceinline__ bool hat_march(TmaSmem &sm, const TmaParams &tp, const Geo<float> &g, PadLayout pl, int r,
                                           const float2 *__restrict__ aux, float wmu, int i0, int j0, int k0, int k1,
                                           int *err, int limit, F &&f)
 {
     const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
-    const int i = i0 + tx, j = j0 + ty;
-    const bool live = i <= g.nx && j <= g.ny;
-    const ColGeo<float> cg = col_geo(g, min(i, g.nx), min(j, g.ny));
-    const int hf = (ty + 1) * kFW + tx + 2;  // own column in a field plane of the tile
-    const int hs = (ty + 1) * kSW + tx + 4;  // own column in a sigma plane
-    const int hn = ty * kPhX + tx;           // own node in a potential plane
-    const int hw = ty * kNW + tx;            // own node in a node-weight plane
+    const int i = i0 + tx, jA = j0 + ty, jB = jA + kHatRows;
+    const bool liveA = i <= g.nx && jA <= g.ny, liveB = i <= g.nx && jB <= g.ny;
+    const ColGeo<float> cgA = col_geo(g, min(i, g.nx), min(jA, g.ny));
+    const ColGeo<float> cgB = col_geo(g, min(i, g.nx), min(jB, g.ny));
+    const int hfA = (ty + 1) * kFW + tx + 2;  // own column in a field plane of the tile
+    const int hsA = (ty + 1) * kSW + tx + 4;  // own column in a sigma plane
+    const int hnA = ty * kPhX + tx;           // own node in a potential plane
+    const int hwA = ty * kNW + tx;            // own node in a node-weight plane
+    constexpr int dF = kHatRows * kFW, dS = kHatRows * kSW, dN = kHatRows * kPhX, dW = kHatRows * kNW;
     const int cf = kFR * kFW, cs = kFR * kSW;
     const int pxy = pl.Px * pl.Py, pc = pl.Pz * pxy;
-    const int col = min(i, pl.Px - 1) + pl.Px * min(j, pl.Py - 1);
+    const int colA = min(i, pl.Px - 1) + pl.Px * min(jA, pl.Py - 1);
+    const int colB = min(i, pl.Px - 1) + pl.Px * min(jB, pl.Py - 1);
     const bool issuer = threadIdx.x == 0;
     const unsigned tx_bytes = kFBytes + kSBytes;
+    // halo nodes of the potentials: (i0 + 32, j0 .. j0 + 8) and (i0 .. i0 + 31, j0 + 8)
     const bool hasH = threadIdx.x < kTX + kTY + 1;
     const int hni = threadIdx.x < kTX ? threadIdx.x : kTX;
     const int hnj = threadIdx.x < kTX ? kTY : threadIdx.x - kTX;
@@ -340,27 +349,121 @@ __device__ __forceinline__ bool hat_march(TmaSmem &sm, const TmaParams &tp, cons
     };
     auto phi_plane = [&](int p) {
         const float dZ = (p >= 0 && p <= g.nz) ? g.delZ[p] : 0.f;
-        sm.phi[p & 1][hn] = tma_phi_node(sm, g, i, j, p, tx, ty, cg.delXi, cg.delYj, dZ);
-        if (hasH) sm.phi[p & 1][hnj * kPhX + hni] = tma_phi_node(sm, g, hi, hj, p, hni, hnj, hdX, hdY, dZ);
+        float2 *P = sm.phi[p & 1];
+        P[hnA] = tma_phi_node(sm, g, i, jA, p, tx, ty, cgA.delXi, cgA.delYj, dZ);
+        P[hnA + dN] = tma_phi_node(sm, g, i, jB, p, tx, ty + kHatRows, cgB.delXi, cgB.delYj, dZ);
+        if (hasH) P[hnj * kPhX + hni] = tma_phi_node(sm, g, hi, hj, p, hni, hnj, hdX, hdY, dZ);
     };
     const float2 zero = make_float2(0.f, 0.f);
-    // signed node weights of the thread's nodes (i, j), (i+1, j), (i, j+1) at
-    // the plane being computed
-    float wS = 0.f, wX = 0.f, wY = 0.f;
-    auto node_w = [&](int p, float &s, float &x, float &y) {
+    // signed node weights of each column's nodes (i, j), (i+1, j), (i, j+1)
+    // at the plane being computed
+    float wSA = 0.f, wXA = 0.f, wYA = 0.f, wSB = 0.f, wXB = 0.f, wYB = 0.f;
+    auto node_w = [&](int p, float &sa, float &xa, float &ya, float &sb, float &xb, float &yb) {
         const float *N = reinterpret_cast<const float *>(sm.nod[p & 1]);
-        s = N[hw];
-        x = N[hw + 1];
-        y = N[hw + kNW];
+        sa = N[hwA];
+        xa = N[hwA + 1];
+        ya = N[hwA + kNW];
+        sb = N[hwA + dW];
+        xb = N[hwA + dW + 1];
+        yb = N[hwA + dW + kNW];
+    };
+    // (padding entries of aux, where Ex, Ey or Ez does not exist, are zero)
+    float2 axA = zero, ayA = zero, azA = zero, axB = zero, ayB = zero, azB = zero;
+    auto load_aux = [&](int k) {
+        if (!aux || k > g.nz) return;
+        if (liveA) {
+            const int b = colA + pxy * k;
+            axA = aux[b];
+            ayA = aux[pc + b];
+            azA = aux[2 * pc + b];
+        }
+        if (liveB) {
+            const int b = colB + pxy * k;
+            axB = aux[b];
+            ayB = aux[pc + b];
+            azB = aux[2 * pc + b];
+        }
     };
 
-    float2 ax = zero, ay = zero, az = zero;
-    auto load_aux = [&](int k) {
-        if (!aux || !live || k > g.nz) return;
-        const int b = col + pxy * k;
-        if (cg.hasX) ax = aux[b];
-        if (cg.hasY) ay = aux[pc + b];
-        if (k < g.nz) az = aux[2 * pc + b];
+    // the three edges of one node column at plane k.  Every edge slot is
+    // formed without branches: an edge that is not interior (or does not
+    // exist: Ex at i = nx, Ey at j = ny, Ez at k = nz, all padding entries
+    // of the layout) gets yhat = 0 and W = 0, so it adds nothing to the
+    // inner products and keeps its zero.  The shared-memory reads stay
+    // inside the tile whatever the edge.
+    auto node_edges = [&](const ColGeo<float> &cg, const PlaneGeo<float> &pg, int k, bool kin, int h, int hs, int hn,
+                          float wS, float wX, float wY, float nS, int eb, float2 ax, float2 ay, float2 az) {
+        const float2 *Fm = reinterpret_cast<const float2 *>(sm.fld[(k - 1) & 3]);
+        const float2 *F0 = reinterpret_cast<const float2 *>(sm.fld[k & 3]);
+        const float2 *Fp = reinterpret_cast<const float2 *>(sm.fld[(k + 1) & 3]);
+        const float *S0 = reinterpret_cast<const float *>(sm.sig[k % 3]);
+        const float2 *Xm = Fm, *X0 = F0, *Xp = Fp;
+        const float2 *Ym = Fm + cf, *Y0 = F0 + cf, *Yp = Fp + cf;
+        const float2 *Zm = Fm + 2 * cf, *Z0 = F0 + 2 * cf;
+        const float2 *P0 = sm.phi[k & 1], *P1 = sm.phi[(k + 1) & 1];
+        // ---- Ex(i, j, k)
+        {
+            const float2 X1 = X0[h];
+            const bool in = cg.intX && kin;
+            float dr, di, W;
+            hat_diag(0, cg, pg, wmu, S0[hs], gd, wS, wX, dr, di);
+            const float2 yy = csub(cadd(csub(Y0[h + 1], Y0[h]), Y0[h - kFW]), Y0[h + 1 - kFW]);
+            const float2 zz = csub(cadd(csub(Z0[h + 1], Z0[h]), Zm[h]), Zm[h + 1]);
+            const float2 fyp = cscale(csub(X0[h + kFW], X1), cg.rdyj);
+            const float2 fym = cscale(csub(X1, X0[h - kFW]), cg.rdyjm1);
+            const float2 fzp = cscale(csub(Xp[h], X1), pg.rdzk);
+            const float2 fzm = cscale(csub(X1, Xm[h]), pg.rdzkm1);
+            float2 out = cadd(cscale(yy, pg.delZk), cscale(zz, cg.delYj));
+            out = csub(out, cscale(csub(fyp, fym), cg.dxi * pg.delZk));
+            out = csub(out, cscale(csub(fzp, fzm), cg.dxi * cg.delYj));
+            out.x -= di * X1.y;
+            out.y += di * X1.x;
+            if (gd) out = cadd(out, cscale(csub(P0[hn + 1], P0[hn]), cg.delYj * pg.delZk));
+            out = hat_div(out, dr, di, W);
+            f(eb, in ? out : zero, X1, in ? W : 0.f, ax);
+        }
+        // ---- Ey(i, j, k)
+        {
+            const float2 Y1 = Y0[h];
+            const bool in = cg.intY && kin;
+            float dr, di, W;
+            hat_diag(1, cg, pg, wmu, S0[cs + hs], gd, wS, wY, dr, di);
+            const float2 zz = csub(cadd(csub(Z0[h + kFW], Z0[h]), Zm[h]), Zm[h + kFW]);
+            const float2 xx = csub(cadd(csub(X0[h + kFW], X0[h]), X0[h - 1]), X0[h - 1 + kFW]);
+            const float2 fzp = cscale(csub(Yp[h], Y1), pg.rdzk);
+            const float2 fzm = cscale(csub(Y1, Ym[h]), pg.rdzkm1);
+            const float2 fxp = cscale(csub(Y0[h + 1], Y1), cg.rdxi);
+            const float2 fxm = cscale(csub(Y1, Y0[h - 1]), cg.rdxim1);
+            float2 out = cadd(cscale(zz, cg.delXi), cscale(xx, pg.delZk));
+            out = csub(out, cscale(csub(fzp, fzm), cg.dyj * cg.delXi));
+            out = csub(out, cscale(csub(fxp, fxm), cg.dyj * pg.delZk));
+            out.x -= di * Y1.y;
+            out.y += di * Y1.x;
+            if (gd) out = cadd(out, cscale(csub(P0[hn + kPhX], P0[hn]), cg.delXi * pg.delZk));
+            out = hat_div(out, dr, di, W);
+            f(pc + eb, in ? out : zero, Y1, in ? W : 0.f, ay);
+        }
+        // ---- Ez(i, j, k)
+        {
+            const float2 Z1 = Z0[h];
+            const bool in = cg.intZ && k < g.nz;
+            float dr, di, W;
+            hat_diag(2, cg, pg, wmu, S0[2 * cs + hs], gd, wS, nS, dr, di);
+            const float2 xx = csub(cadd(csub(Xp[h], X0[h]), X0[h - 1]), Xp[h - 1]);
+            const float2 yy = csub(cadd(csub(Yp[h], Y0[h]), Y0[h - kFW]), Yp[h - kFW]);
+            const float2 fxp = cscale(csub(Z0[h + 1], Z1), cg.rdxi);
+            const float2 fxm = cscale(csub(Z1, Z0[h - 1]), cg.rdxim1);
+            const float2 fyp = cscale(csub(Z0[h + kFW], Z1), cg.rdyj);
+            const float2 fym = cscale(csub(Z1, Z0[h - kFW]), cg.rdyjm1);
+            float2 out = cadd(cscale(xx, cg.delYj), cscale(yy, cg.delXi));
+            out = csub(out, cscale(csub(fxp, fxm), pg.dzk * cg.delYj));
+            out = csub(out, cscale(csub(fyp, fym), pg.dzk * cg.delXi));
+            out.x -= di * Z1.y;
+            out.y += di * Z1.x;
+            if (gd) out = cadd(out, cscale(csub(P1[hn], P0[hn]), cg.delXi * cg.delYj));
+            out = hat_div(out, dr, di, W);
+            f(2 * pc + eb, in ? out : zero, Z1, in ? W : 0.f, az);
+        }
     };
 
     load_aux(k0);
@@ -371,7 +474,7 @@ __device__ __forceinline__ bool hat_march(TmaSmem &sm, const TmaParams &tp, cons
         const bool w0 = wait(k0 - 1), w1 = w0 && wait(k0);
         if (w1 && gd) {
             phi_plane(k0);
-            node_w(k0, wS, wX, wY);
+            node_w(k0, wSA, wXA, wYA, wSB, wXB, wYB);
         }
         if (!__syncthreads_and(w1)) {
             give_up(w1 ? k0 + 1 : w0 ? k0 : k0 - 1, k0 + 1);
@@ -382,111 +485,29 @@ __device__ __forceinline__ bool hat_march(TmaSmem &sm, const TmaParams &tp, cons
         const int last = k + 2 <= k1 ? k + 2 : k + 1;
         if (k + 2 <= k1) issue(k + 2);
         const bool ok = wait(k + 1);
-        float nS = 0.f, nX = 0.f, nY = 0.f;  // plane k + 1
+        float nSA = 0.f, nXA = 0.f, nYA = 0.f, nSB = 0.f, nXB = 0.f, nYB = 0.f;  // plane k + 1
         if (ok && gd) {
             phi_plane(k + 1);
-            node_w(k + 1, nS, nX, nY);
+            node_w(k + 1, nSA, nXA, nYA, nSB, nXB, nYB);
         }
         if (!__syncthreads_and(ok)) {
             give_up(ok ? k + 2 : k + 1, last);
             return false;
         }
-        if (live) {
-            const float2 *Fm = reinterpret_cast<const float2 *>(sm.fld[(k - 1) & 3]);
-            const float2 *F0 = reinterpret_cast<const float2 *>(sm.fld[k & 3]);
-            const float2 *Fp = reinterpret_cast<const float2 *>(sm.fld[(k + 1) & 3]);
-            const float *S0 = reinterpret_cast<const float *>(sm.sig[k % 3]);
-            const float2 *Xm = Fm, *X0 = F0, *Xp = Fp;
-            const float2 *Ym = Fm + cf, *Y0 = F0 + cf, *Yp = Fp + cf;
-            const float2 *Zm = Fm + 2 * cf, *Z0 = F0 + 2 * cf;
-            const float2 *P0 = sm.phi[k & 1], *P1 = sm.phi[(k + 1) & 1];
-            const PlaneGeo<float> pg = plane_geo(g, k);
-            const bool kin = k >= 1 && k <= g.nz - 1;
-            const int h = hf;
-            const int eb = col + pxy * k;
-            // ---- Ex(i, j, k)
-            if (cg.hasX) {
-                const float2 X1 = X0[h];
-                const float sg = S0[hs];
-                float2 out = zero;
-                float W = 0.f;
-                const bool in = cg.intX && kin;
-                if (in) {
-                    float dr, di;
-                    hat_diag(0, cg, pg, wmu, sg, gd, wS, wX, dr, di);
-                    const float2 yy = csub(cadd(csub(Y0[h + 1], Y0[h]), Y0[h - kFW]), Y0[h + 1 - kFW]);
-                    const float2 zz = csub(cadd(csub(Z0[h + 1], Z0[h]), Zm[h]), Zm[h + 1]);
-                    const float2 fyp = cscale(csub(X0[h + kFW], X1), cg.rdyj);
-                    const float2 fym = cscale(csub(X1, X0[h - kFW]), cg.rdyjm1);
-                    const float2 fzp = cscale(csub(Xp[h], X1), pg.rdzk);
-                    const float2 fzm = cscale(csub(X1, Xm[h]), pg.rdzkm1);
-                    out = cadd(cscale(yy, pg.delZk), cscale(zz, cg.delYj));
-                    out = csub(out, cscale(csub(fyp, fym), cg.dxi * pg.delZk));
-                    out = csub(out, cscale(csub(fzp, fzm), cg.dxi * cg.delYj));
-                    out.x -= di * X1.y;
-                    out.y += di * X1.x;
-                    if (gd) out = cadd(out, cscale(csub(P0[hn + 1], P0[hn]), cg.delYj * pg.delZk));
-                    out = hat_div(out, dr, di, W);
-                }
-                f(eb, in, out, X1, W, ax);
-            }
-            // ---- Ey(i, j, k)
-            if (cg.hasY) {
-                const float2 Y1 = Y0[h];
-                const float sg = S0[cs + hs];
-                float2 out = zero;
-                float W = 0.f;
-                const bool in = cg.intY && kin;
-                if (in) {
-                    float dr, di;
-                    hat_diag(1, cg, pg, wmu, sg, gd, wS, wY, dr, di);
-                    const float2 zz = csub(cadd(csub(Z0[h + kFW], Z0[h]), Zm[h]), Zm[h + kFW]);
-                    const float2 xx = csub(cadd(csub(X0[h + kFW], X0[h]), X0[h - 1]), X0[h - 1 + kFW]);
-                    const float2 fzp = cscale(csub(Yp[h], Y1), pg.rdzk);
-                    const float2 fzm = cscale(csub(Y1, Ym[h]), pg.rdzkm1);
-                    const float2 fxp = cscale(csub(Y0[h + 1], Y1), cg.rdxi);
-                    const float2 fxm = cscale(csub(Y1, Y0[h - 1]), cg.rdxim1);
-                    out = cadd(cscale(zz, cg.delXi), cscale(xx, pg.delZk));
-                    out = csub(out, cscale(csub(fzp, fzm), cg.dyj * cg.delXi));
-                    out = csub(out, cscale(csub(fxp, fxm), cg.dyj * pg.delZk));
-                    out.x -= di * Y1.y;
-                    out.y += di * Y1.x;
-                    if (gd) out = cadd(out, cscale(csub(P0[hn + kPhX], P0[hn]), cg.delXi * pg.delZk));
-                    out = hat_div(out, dr, di, W);
-                }
-                f(pc + eb, in, out, Y1, W, ay);
-            }
-            // ---- Ez(i, j, k)
-            if (k < g.nz) {
-                const float2 Z1 = Z0[h];
-                const float sg = S0[2 * cs + hs];
-                float2 out = zero;
-                float W = 0.f;
-                const bool in = cg.intZ;
-                if (in) {
-                    float dr, di;
-                    hat_diag(2, cg, pg, wmu, sg, gd, wS, nS, dr, di);
-                    const float2 xx = csub(cadd(csub(Xp[h], X0[h]), X0[h - 1]), Xp[h - 1]);
-                    const float2 yy = csub(cadd(csub(Yp[h], Y0[h]), Y0[h - kFW]), Yp[h - kFW]);
-                    const float2 fxp = cscale(csub(Z0[h + 1], Z1), cg.rdxi);
-                    const float2 fxm = cscale(csub(Z1, Z0[h - 1]), cg.rdxim1);
-                    const float2 fyp = cscale(csub(Z0[h + kFW], Z1), cg.rdyj);
-                    const float2 fym = cscale(csub(Z1, Z0[h - kFW]), cg.rdyjm1);
-                    out = cadd(cscale(xx, cg.delYj), cscale(yy, cg.delXi));
-                    out = csub(out, cscale(csub(fxp, fxm), pg.dzk * cg.delYj));
-                    out = csub(out, cscale(csub(fyp, fym), pg.dzk * cg.delXi));
-                    out.x -= di * Z1.y;
-                    out.y += di * Z1.x;
-                    if (gd) out = cadd(out, cscale(csub(P1[hn], P0[hn]), cg.delXi * cg.delYj));
-                    out = hat_div(out, dr, di, W);
-                }
-                f(2 * pc + eb, in, out, Z1, W, az);
-            }
-            if (k + 1 < k1) load_aux(k + 1);
-        }
-        wS = nS;
-        wX = nX;
-        wY = nY;
+        const PlaneGeo<float> pg = plane_geo(g, k);
+        const bool kin = k >= 1 && k <= g.nz - 1;
+        if (liveA)
+            node_edges(cgA, pg, k, kin, hfA, hsA, hnA, wSA, wXA, wYA, nSA, colA + pxy * k, axA, ayA, azA);
+        if (liveB)
+            node_edges(cgB, pg, k, kin, hfA + dF, hsA + dS, hnA + dN, wSB, wXB, wYB, nSB, colB + pxy * k, axB, ayB,
+                       azB);
+        if (k + 1 < k1) load_aux(k + 1);
+        wSA = nSA;
+        wXA = nXA;
+        wYA = nYA;
+        wSB = nSB;
+        wXB = nXB;
+        wYB = nYB;
         __syncthreads();
     }
     return true;
@@ -535,29 +556,30 @@ __device__ __forceinline__ void hat_vt(const TmaParams &tp, const KArgs<float> &
     TmaSmem &sm = tma_smem();
     const bool ok = hat_march<gd>(
         sm, tp, a.g, a.pl, r, aux, (float)(a.dsgn * a.ost[r].omega * kMu0), i0, j0, k0, k1, a.err, a.wait_limit,
-        [&](int e, bool inn, float2 y, float2 x, float W, float2 xa) {
-            if (reset) Yr[e] = inn ? make_float2(W * x.x, W * x.y) : make_float2(0.f, 0.f);
-            if (poly && inn) y = make_float2(c2 * x.x - cc * y.x, c2 * x.y - cc * y.y);  // c (2 x - c D^-1 A x)
-            if (inn) {
-                if (kv) {
-                    const float2 z = reset ? make_float2(W * x.x, W * x.y) : xa;
-                    u[0] += (double)z.x * y.x + (double)z.y * y.y;  // conj(y) vh
-                    u[1] += (double)z.x * y.y - (double)z.y * y.x;
-                } else if (kt) {
-                    const float2 sv = stage == 5 ? xa : x;
-                    const double w = W;
-                    u[0] += w * ((double)y.x * sv.x + (double)y.y * sv.y);  // conj(t) s
-                    u[1] += w * ((double)y.x * sv.y - (double)y.y * sv.x);
-                    u[2] += w * ((double)y.x * y.x + (double)y.y * y.y);
-                    u[3] += w * ((double)sv.x * sv.x + (double)sv.y * sv.y);
-                }
+        // y and W are zero at edges that are not interior, and so are x
+        // and xa there (u, sh, w1, w2 and the shadow vanish off the
+        // interior): those edges add nothing and need no test
+        [&](int e, float2 y, float2 x, float W, float2 xa) {
+            if (reset) Yr[e] = make_float2(W * x.x, W * x.y);
+            if (poly) y = make_float2(c2 * x.x - cc * y.x, c2 * x.y - cc * y.y);  // c (2 x - c D^-1 A x)
+            if (kv) {
+                const float2 z = reset ? make_float2(W * x.x, W * x.y) : xa;
+                u[0] += (double)z.x * y.x + (double)z.y * y.y;  // conj(y) vh
+                u[1] += (double)z.x * y.y - (double)z.y * y.x;
+            } else if (kt) {
+                const float2 sv = stage == 5 ? xa : x;
+                const double w = W;
+                u[0] += w * ((double)y.x * sv.x + (double)y.y * sv.y);  // conj(t) s
+                u[1] += w * ((double)y.x * sv.y - (double)y.y * sv.x);
+                u[2] += w * ((double)y.x * y.x + (double)y.y * y.y);
+                u[3] += w * ((double)sv.x * sv.x + (double)sv.y * sv.y);
             }
             out[e] = y;
         });
     if (!ok || !dots) return;
     // the march has read its last staged plane: the field ring is free
     double tot[4];
-    if (block_reduce_last_in<4>(u, a.parts, a.cnt, r, bx + a.cmap.tiles * bz, a.cmap.tiles * gz, tot,
+    if (block_reduce_last_in<4, kHatThreads>(u, a.parts, a.cnt, r, bx + a.cmap.tiles * bz, a.cmap.tiles * gz, tot,
                                 reinterpret_cast<double *>(sm.fld[0]), reinterpret_cast<int *>(sm.fld[1])) &&
         threadIdx.x == 0) {
         if (kv) {
@@ -582,7 +604,7 @@ __global__ void __launch_bounds__(kThreads) kh_u(KArgs<float> a) { hat_u(a, bloc
 __global__ void __launch_bounds__(kThreads) kh_s(KArgs<float> a) { hat_s(a, blockIdx.y, blockIdx.x); }
 __global__ void __launch_bounds__(kThreads) kh_xr(KArgs<float> a) { hat_xr(a, blockIdx.y, blockIdx.x); }
 template <int stage, bool gd>
-__global__ void __launch_bounds__(kThreads, 4) kh_vt(const __grid_constant__ TmaParams tp, KArgs<float> a)
+__global__ void __launch_bounds__(kHatThreads, 4) kh_vt(const __grid_constant__ TmaParams tp, KArgs<float> a)
 {
     hat_vt<stage, gd>(tp, a, blockIdx.y, blockIdx.x, blockIdx.z, gridDim.z);
 }
@@ -620,7 +642,7 @@ __host__ __device__ constexpr int stage_input(int stage)
 {
     return stage == 0 || stage == 2 ? 0 : stage == 1 || stage == 4 ? 1 : stage == 3 ? 2 : 3;
 }
-template <int stage> __global__ void __launch_bounds__(kThreads, 4) kh_vt_multi(const __grid_constant__ HatMulti p)
+template <int stage> __global__ void __launch_bounds__(kHatThreads, 4) kh_vt_multi(const __grid_constant__ HatMulti p)
 {
     const int g = multi_grid_of(p.sb0, p.ng, blockIdx.x);
     const KArgs<float> &a = p.a[g];
@@ -648,8 +670,9 @@ template <int stage, bool gd> static void launch_hat_vt_t(const KArgs<float> &a,
                                                            cudaStream_t s)
 {
     const size_t sm = sizeof(TmaSmem);
-    const int res = tma_resident(kh_vt<stage, gd>, sm, 2 + 2 * stage + (gd ? 1 : 0));
-    kh_vt<stage, gd><<<dim3(a.cmap.tiles, nrhs, stage_chunks(a.g.nz, a.cmap.tiles, res)), kThreads, sm, s>>>(tp, a);
+    const int res = tma_resident(kh_vt<stage, gd>, sm, 2 + 2 * stage + (gd ? 1 : 0), kHatThreads);
+    kh_vt<stage, gd><<<dim3(a.cmap.tiles, nrhs, stage_chunks(a.g.nz, a.cmap.tiles, res)), kHatThreads, sm, s>>>(tp,
+                                                                                                              a);
 }
 template <int stage> static void launch_hat_stage(const KArgs<float> &a, int nrhs, cudaStream_t s)
 {
@@ -705,15 +728,13 @@ int launch_hat_iter_multi(const KArgs<float> *args, const int *nrhs, const int *
     HatMulti p;
     std::memset(&p, 0, sizeof p);
     p.ng = ng;
-    const int res = tma_resident(kh_vt_multi<0>, sizeof(TmaSmem), 14);
-    for (int q = 1; q < 6; q++) {
-        const size_t smb = sizeof(TmaSmem);
-        if (q == 1) tma_resident(kh_vt_multi<1>, smb, 15);
-        if (q == 2) tma_resident(kh_vt_multi<2>, smb, 16);
-        if (q == 3) tma_resident(kh_vt_multi<3>, smb, 17);
-        if (q == 4) tma_resident(kh_vt_multi<4>, smb, 18);
-        if (q == 5) tma_resident(kh_vt_multi<5>, smb, 19);
-    }
+    const size_t smb = sizeof(TmaSmem);
+    const int res = tma_resident(kh_vt_multi<0>, smb, 14, kHatThreads);
+    tma_resident(kh_vt_multi<1>, smb, 15, kHatThreads);
+    tma_resident(kh_vt_multi<2>, smb, 16, kHatThreads);
+    tma_resident(kh_vt_multi<3>, smb, 17, kHatThreads);
+    tma_resident(kh_vt_multi<4>, smb, 18, kHatThreads);
+    tma_resident(kh_vt_multi<5>, smb, 19, kHatThreads);
     p.eb0[0] = p.sb0[0] = 0;
     for (int g = 0; g < ng; g++) {
         p.a[g] = args[g];
@@ -737,17 +758,17 @@ int launch_hat_iter_multi(const KArgs<float> *args, const int *nrhs, const int *
     const size_t sm = sizeof(TmaSmem);
     kh_elem_multi<0><<<p.eb0[ng], kThreads, 0, s>>>(p);
     if (poly) {
-        kh_vt_multi<2><<<p.sb0[ng], kThreads, sm, s>>>(p);
-        kh_vt_multi<3><<<p.sb0[ng], kThreads, sm, s>>>(p);
+        kh_vt_multi<2><<<p.sb0[ng], kHatThreads, sm, s>>>(p);
+        kh_vt_multi<3><<<p.sb0[ng], kHatThreads, sm, s>>>(p);
     } else {
-        kh_vt_multi<0><<<p.sb0[ng], kThreads, sm, s>>>(p);
+        kh_vt_multi<0><<<p.sb0[ng], kHatThreads, sm, s>>>(p);
     }
     kh_elem_multi<1><<<p.eb0[ng], kThreads, 0, s>>>(p);
     if (poly) {
-        kh_vt_multi<4><<<p.sb0[ng], kThreads, sm, s>>>(p);
-        kh_vt_multi<5><<<p.sb0[ng], kThreads, sm, s>>>(p);
+        kh_vt_multi<4><<<p.sb0[ng], kHatThreads, sm, s>>>(p);
+        kh_vt_multi<5><<<p.sb0[ng], kHatThreads, sm, s>>>(p);
     } else {
-        kh_vt_multi<1><<<p.sb0[ng], kThreads, sm, s>>>(p);
+        kh_vt_multi<1><<<p.sb0[ng], kHatThreads, sm, s>>>(p);
     }
     kh_elem_multi<2><<<p.eb0[ng], kThreads, 0, s>>>(p);
     return 0;

@@ -164,7 +164,11 @@ __device__ __forceinline__ TmaSmem &tma_smem()
 // kernels; `slot` identifies the kernel (its shared-memory attribute is set
 // the first time its slot is seen), so every kernel needs its own slot
 constexpr int kTmaSlots = 20;
-template <typename K> inline int tma_resident(K kern, size_t smem, int slot)
+// the fused stencil of hatkernels.cu: 128 threads, each on two node rows
+// (ty and ty + 4) of the 32 x 8 tile
+constexpr int kHatThreads = 128, kHatRows = kTY / 2;
+static_assert(kHatThreads == kTX * kHatRows, "fused stencil thread layout");
+template <typename K> inline int tma_resident(K kern, size_t smem, int slot, int threads = kThreads)
 {
     static std::mutex mu;
     static int occ[64][kTmaSlots] = {};
@@ -176,7 +180,7 @@ template <typename K> inline int tma_resident(K kern, size_t smem, int slot)
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         int n = 0, sms = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, kThreads, smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, threads, smem);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         occ[dev][slot] = std::max(1, n) * std::max(1, sms);
     }

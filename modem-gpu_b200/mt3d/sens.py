@@ -59,3 +59,37 @@ def misfit_gradient(s, m_earth, freqs, bcs, sites, d_obs, err, origin=(0.0, 0.0,
             raise RuntimeError(f"transposed solves at {f} Hz did not converge")
         grad += dm
     return phi, -2.0 / ndata * grad
+
+
+def taylor_test(s, m_earth, air_cond, dm, freqs, bcs, sites, d_obs, err, origin=(0.0, 0.0, 0.0)):
+    """The total-derivative test of the reference's TEST_GRAD job
+    (f90/Mod3DMT.f90:297-333) for the data term: f(m0 + dm) - f(m0) against
+    grad f(m0) . dm.  Leaves the handle at m0.  Returns (f(m0), the
+    difference, the linear prediction)."""
+    m0 = np.asarray(m_earth, np.float64)
+    s.update_cond(m0, air_cond)
+    f1, grad = misfit_gradient(s, m0, freqs, bcs, sites, d_obs, err, origin)
+    s.update_cond(m0 + dm, air_cond)
+    Z, _ = predict(s, freqs, bcs, sites, origin)
+    f2 = misfit(Z, d_obs, err)[0]
+    s.update_cond(m0, air_cond)
+    return f1, f2 - f1, float(np.dot(grad, dm))
+
+
+def central_differences(s, m_earth, air_cond, cells, freqs, bcs, sites, d_obs, err, h=1e-4,
+                        origin=(0.0, 0.0, 0.0)):
+    """(f(m + h e_c) - f(m - h e_c)) / 2h for each earth cell c (flat index
+    into m_earth).  Leaves the handle at m."""
+    m0 = np.asarray(m_earth, np.float64)
+    out = np.zeros(len(cells))
+    for n, c in enumerate(cells):
+        f = []
+        for sign in (1.0, -1.0):
+            m = m0.copy()
+            m[c] += sign * h
+            s.update_cond(m, air_cond)
+            Z, _ = predict(s, freqs, bcs, sites, origin)
+            f.append(misfit(Z, d_obs, err)[0])
+        out[n] = (f[0] - f[1]) / (2 * h)
+    s.update_cond(m0, air_cond)
+    return out
