@@ -524,7 +524,7 @@ def main():
     kp = 1 if kms[1] > 0 else 0
     # with the polynomial preconditioner each timed event pair brackets the
     # two stencil launches of one preconditioned product
-    launches = kn[kp] * (2 if (kp and POLY > 0) else 1)
+    st_launches = kn[kp] * (2 if (kp and POLY > 0) else 1)
     achieved = (alg[kp] / (kms[kp] / 1e3) / 1e9) if kms[kp] > 0 else None
     traffic = (TRAFFIC_PER_EDGE_RHS * units[kp] / kn[kp]) if (TRAFFIC_PER_EDGE_RHS and kn[kp] and kp and not FUSED) \
         else None
@@ -534,11 +534,11 @@ def main():
                              f"polynomial preconditioner c = {POLY}: two launches per product)" if FUSED
                             else "kct_vt (TMA-staged stencil + grad-div + fused dots)") + ", FP32" if kp else
                            "kcs_vt (cp.async-staged stencil + grad-div + fused dots), FP64") + " complex",
-                "peak_kind": peak_kind, "timed_launches": launches,
+                "peak_kind": peak_kind, "timed_launches": st_launches,
                 "timing": "CUDA events around every stencil launch on the solver stream, in a separate pass "
                           "over the first step after the timed region",
                 "bytes_per_edge_rhs": alg[kp] / units[kp] if units[kp] else None,
-                "algorithmic_bytes_per_launch": alg[kp] / launches if launches else None,
+                "algorithmic_bytes_per_launch": alg[kp] / st_launches if st_launches else None,
                 "fp64_fallback": {"launches": kn[0], "ms": kms[0],
                                   "achieved_gbs": (alg[0] / (kms[0] / 1e3) / 1e9) if kms[0] > 0 else None,
                                   "share_of_stencil_time": kms[0] / (kms[0] + kms[1]) if kms[0] + kms[1] > 0 else 0.0}}

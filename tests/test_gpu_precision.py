@@ -9,7 +9,8 @@ fields on 4096 seeded earth edges (2-norm) and of the Full_Impedance tensors
 at 100 surface sites (per site, max_ij |dZ_ij| / max_ij |Z_ij|, the largest
 over the sites).  Bounds, about five times the measured errors:
   * grad-div formulation (the benchmark's), FP64 and mixed precision with
-    FP64 refinement: at residual 1e-7 impedances within 1e-5 and fields
+    FP64 refinement (with the diagonal and with the benchmark's polynomial
+    preconditioner): at residual 1e-7 impedances within 1e-5 and fields
     within 2e-5 (measured 1.7e-6 / 2.5e-6); at 1e-8 within 1e-6 and 2e-6
     (1.3e-7 / 1.7e-7); at 1e-9 within 1e-7 and 2e-7 (1.5e-8 / 2.0e-8);
   * the reference's formulation (curl-curl + divergence correction), FP64
@@ -52,13 +53,21 @@ BOUNDS = {  # (formulation, tol): (impedance, field)
 }
 
 
-@pytest.mark.parametrize("precision", [capi.PREC_FP64, capi.PREC_MIXED], ids=["fp64", "mixed"])
-@pytest.mark.parametrize("formulation,tol", list(BOUNDS), ids=[f"{'ccgd' if f else 'ccdc'}-{t:g}" for f, t in BOUNDS])
-def test_precision_against_converged_oracle(precision_case, precision, formulation, tol):
+# (precision, polynomial preconditioner coefficient): FP64, mixed with the
+# diagonal preconditioner, and mixed with the benchmark's polynomial one
+# (grad-div formulation only, the one the benchmark runs)
+PATHS = {"fp64": (capi.PREC_FP64, 0.0), "mixed": (capi.PREC_MIXED, 0.0), "mixed-poly": (capi.PREC_MIXED, 0.9)}
+CASES = [(f, t, p) for f, t in BOUNDS for p in PATHS if not (p == "mixed-poly" and f == capi.FORM_CCDC)]
+
+
+@pytest.mark.parametrize("formulation,tol,path", CASES, ids=[f"{'ccgd' if f else 'ccdc'}-{t:g}-{p}" for f, t, p in CASES])
+def test_precision_against_converged_oracle(precision_case, formulation, tol, path):
     f, m, omega, bcs = precision_case
+    precision, poly = PATHS[path]
     s = capi.Solver(m.grid)
     s.set_formulation(formulation)
     s.set_restart(0)
+    s.set_poly(poly)
     s.update_cond(m.m_earth, m.air_cond)
     if formulation == capi.FORM_CCGD:
         s.set_control(IterPerDivCor=300, MaxDivCor=60, tolEMfwd=tol, tolEMadj=tol, precision=precision)
@@ -73,7 +82,7 @@ def test_precision_against_converged_oracle(precision_case, precision, formulati
     idx = f["edges"]
     eerr = max(np.linalg.norm(e[0][idx] - f["E1"]) / np.linalg.norm(f["E1"]),
                np.linalg.norm(e[1][idx] - f["E2"]) / np.linalg.norm(f["E2"]))
-    print(f"formulation {formulation} precision {precision} tol {tol:g}: iterations {it.tolist()}, "
+    print(f"formulation {formulation} path {path} tol {tol:g}: iterations {it.tolist()}, "
           f"relres {rr.tolist()}, Z error {zerr:.3e}, E error {eerr:.3e}")
     zb, eb = BOUNDS[(formulation, tol)]
     assert zerr <= zb and eerr <= eb
