@@ -481,34 +481,43 @@ __device__ __forceinline__ bool hat_march(TmaSmem &sm, const TmaParams &tp, cons
             return false;
         }
     }
+    // One barrier per plane.  Plane k reads the potentials of plane k at the
+    // thread's node and at its +x and +y neighbours, published by the
+    // barrier that ended the previous plane, and those of plane k + 1 at its
+    // own node only, which it has just formed; so it can be computed as soon
+    // as the thread's own wait for plane k + 1 has completed.  The barrier at
+    // the end publishes plane k + 1's potentials, frees the ring slots of
+    // plane k - 1 for the copies the next plane issues, and makes a wait
+    // that gave up end the block as a whole.
     for (int k = k0; k < k1; k++) {
         const int last = k + 2 <= k1 ? k + 2 : k + 1;
         if (k + 2 <= k1) issue(k + 2);
         const bool ok = wait(k + 1);
         float nSA = 0.f, nXA = 0.f, nYA = 0.f, nSB = 0.f, nXB = 0.f, nYB = 0.f;  // plane k + 1
-        if (ok && gd) {
-            phi_plane(k + 1);
-            node_w(k + 1, nSA, nXA, nYA, nSB, nXB, nYB);
+        if (ok) {
+            if (gd) {
+                phi_plane(k + 1);
+                node_w(k + 1, nSA, nXA, nYA, nSB, nXB, nYB);
+            }
+            const PlaneGeo<float> pg = plane_geo(g, k);
+            const bool kin = k >= 1 && k <= g.nz - 1;
+            if (liveA)
+                node_edges(cgA, pg, k, kin, hfA, hsA, hnA, wSA, wXA, wYA, nSA, colA + pxy * k, axA, ayA, azA);
+            if (liveB)
+                node_edges(cgB, pg, k, kin, hfA + dF, hsA + dS, hnA + dN, wSB, wXB, wYB, nSB, colB + pxy * k, axB,
+                           ayB, azB);
+            if (k + 1 < k1) load_aux(k + 1);
         }
-        if (!__syncthreads_and(ok)) {
-            give_up(ok ? k + 2 : k + 1, last);
-            return false;
-        }
-        const PlaneGeo<float> pg = plane_geo(g, k);
-        const bool kin = k >= 1 && k <= g.nz - 1;
-        if (liveA)
-            node_edges(cgA, pg, k, kin, hfA, hsA, hnA, wSA, wXA, wYA, nSA, colA + pxy * k, axA, ayA, azA);
-        if (liveB)
-            node_edges(cgB, pg, k, kin, hfA + dF, hsA + dS, hnA + dN, wSB, wXB, wYB, nSB, colB + pxy * k, axB, ayB,
-                       azB);
-        if (k + 1 < k1) load_aux(k + 1);
         wSA = nSA;
         wXA = nXA;
         wYA = nYA;
         wSB = nSB;
         wXB = nXB;
         wYB = nYB;
-        __syncthreads();
+        if (!__syncthreads_and(ok)) {
+            give_up(ok ? k + 2 : k + 1, last);
+            return false;
+        }
     }
     return true;
 }
