@@ -20,7 +20,8 @@ value: device time (CUDA events on the solver stream) of the K timed steps,
 inputs resident in HBM.  e2e: the same solves through mt3d_fwdsolve_batch
 with pinned host buffers (host->device copies of the inputs and the
 device->host copy of the fields inside the timed region), over min(K, 2)
-steps.  fp64: the same right-hand sides as the first timed step, solved one
+steps (the first ones, whose own device-time rate it reports beside it, as
+device_value_same_steps: the steps differ in frequency and so in cost).  fp64: the same right-hand sides as the first timed step, solved one
 at a time by the plain FP64 path.  With N > 1 (torchrun) every rank solves its
 own copy of the workload (replicas; the right-hand sides are independent),
 timed between barriers, max over ranks.
@@ -319,10 +320,12 @@ def stencil_bytes(kprec: int, nE: int, nN: int, fused: bool = False) -> float:
     return (2.5 if (fused and kprec) else 3) * sc + sr + sr * nN / nE
 
 
-# DRAM bytes (read + write) per edge and right-hand side of one kct_vt launch,
-# measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum) on the
-# 200x200x100 workload with 8 right-hand sides
+# DRAM bytes (read + write) per edge and right-hand side of one stencil
+# launch, measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum) on
+# the 200x200x100 workload with 8 right-hand sides: the unfused kct_vt, and
+# the fused kh_vt averaged over the four stages of the polynomial iteration
 TRAFFIC_PER_EDGE_RHS = 28.7
+TRAFFIC_PER_EDGE_RHS_FUSED = 23.8
 
 
 def surface_sites(model: models.Model, nrec: int) -> np.ndarray:
@@ -526,8 +529,10 @@ def main():
     # two stencil launches of one preconditioned product
     st_launches = kn[kp] * (2 if (kp and POLY > 0) else 1)
     achieved = (alg[kp] / (kms[kp] / 1e3) / 1e9) if kms[kp] > 0 else None
-    traffic = (TRAFFIC_PER_EDGE_RHS * units[kp] / kn[kp]) if (TRAFFIC_PER_EDGE_RHS and kn[kp] and kp and not FUSED) \
-        else None
+    traffic = None
+    if kp and st_launches:
+        per_unit = (TRAFFIC_PER_EDGE_RHS_FUSED if POLY > 0 else None) if FUSED else TRAFFIC_PER_EDGE_RHS
+        traffic = per_unit * units[kp] / st_launches if per_unit else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                 "kernel": ((f"kh_vt (TMA-staged stencil + grad-div + D^-1 at the output edge + fused dots; "
@@ -558,13 +563,13 @@ def main():
                 he = torch.empty_like(hb).pin_memory()
                 hb.copy_(d_bc.cpu())
                 hs_.copy_(d_src.cpu())
-                per.append((om, hb.numpy(), hs_.numpy(), he.numpy(), tr))
+                per.append((om, hb.numpy(), hs_.numpy(), he.numpy(), tr, he))
             pinned.append(per)
         barrier()
         t0 = time.perf_counter()
         for per in pinned:
             for p in per:
-                p[3][:] = 0
+                p[5].zero_()  # zero first guesses in the pinned in/out buffers
             capi.fwdsolve_multi([s for s, *_ in solvers], [p[0] for p in per], [p[3] for p in per],
                                 trans=[p[4] for p in per], bc=[p[1] for p in per], src=[p[2] for p in per],
                                 zchunks=zchunks)
@@ -573,7 +578,9 @@ def main():
         barrier()
         e2e_s = max_over_ranks(time.perf_counter() - t0)
         e2e = {"value": world * sum(per_step[:ke]) / e2e_s, "unit": "solves/s", "steps": ke,
-               "h2d_bytes_per_step": h2d // ke, "d2h_bytes_per_step": d2h // ke, "entry": "mt3d_fwdsolve_multi"}
+               "h2d_bytes_per_step": h2d // ke, "d2h_bytes_per_step": d2h // ke, "entry": "mt3d_fwdsolve_multi",
+               "device_value_same_steps": replica_rate(sum(per_step[:ke]), sum(step_ms[:ke]) / 1e3, world,
+                                                       max_over_ranks)}
         del pinned
     elif not args.no_e2e:
         ke = min(args.steps, 2)
@@ -587,7 +594,7 @@ def main():
                 he = torch.empty_like(hbc).pin_memory()
                 hbc.copy_(d_bc.cpu())
                 hsrc.copy_(d_src.cpu())
-                per.append((om, hbc.numpy(), hsrc.numpy(), he.numpy(), tr))
+                per.append((om, hbc.numpy(), hsrc.numpy(), he, tr))
             pinned.append(per)
         h2d = d2h = 0
         barrier()
@@ -595,14 +602,19 @@ def main():
         for k in range(ke):
             for (s, batches, d_e, _), per in zip(solvers, pinned):
                 om, hbc, hsrc, he, tr = per[k]
-                he[:] = 0
-                s.fwdsolve_batch(om, bc=hbc, src=hsrc, e0=he, trans=tr)
-                h2d += hbc.nbytes + hsrc.nbytes + he.nbytes
-                d2h += he.nbytes
+                # zero first guess in the pinned in/out buffer (host threads),
+                # copied to the device and the solution back by the library
+                he.zero_()
+                s.fwdsolve_batch(om, bc=hbc, src=hsrc, trans=tr, out=he.numpy())
+                h2d += hbc.nbytes + hsrc.nbytes + he.numel() * he.element_size()
+                d2h += he.numel() * he.element_size()
         barrier()
         e2e_s = max_over_ranks(time.perf_counter() - t0)
         e2e = {"value": world * sum(per_step[:ke]) / e2e_s, "unit": "solves/s", "steps": ke,
-               "h2d_bytes_per_step": h2d // ke, "d2h_bytes_per_step": d2h // ke}
+               "h2d_bytes_per_step": h2d // ke, "d2h_bytes_per_step": d2h // ke,
+               "entry": "mt3d_fwdsolve_batch (pinned host buffers)",
+               "device_value_same_steps": replica_rate(sum(per_step[:ke]), sum(step_ms[:ke]) / 1e3, world,
+                                                       max_over_ranks)}
         del pinned
 
     # plain FP64 path on the right-hand sides of the first step, one at a

@@ -331,11 +331,24 @@ class Solver:
         rc = self._check(self.L.mt3d_fwdsolve(self.h, int(trans), _d(bcp), _d(srcp), _d(e)), allow=(0, 1, 2, 3))
         return e, rc
 
-    def fwdsolve_batch(self, omegas, trans=None, bc=None, src=None, e0=None):
+    def fwdsolve_batch(self, omegas, trans=None, bc=None, src=None, e0=None, out=None):
+        """Batched FWDsolve3D on host arrays.  e0: first guesses (zero if
+        None; copied).  out: a C-contiguous complex128 [n, nE] array used in
+        place as mt3d_fwdsolve_batch's e (first guess in, solution out), so
+        a pinned buffer is copied to and from the device directly; then e0
+        must be None.  Returns (e, status, rc)."""
         omegas = np.ascontiguousarray(omegas, np.float64)
         n = omegas.size
         tr = np.zeros(n, np.int32) if trans is None else np.ascontiguousarray(trans, np.int32)
-        e = np.zeros((n, self.nE), np.complex128) if e0 is None else np.array(e0, np.complex128)
+        if out is not None:
+            if e0 is not None:
+                raise ValueError("fwdsolve_batch: give the first guess in out, not in e0")
+            if not (isinstance(out, np.ndarray) and out.dtype == np.complex128 and out.flags.c_contiguous and
+                    out.shape == (n, self.nE) and out.flags.writeable):
+                raise ValueError("fwdsolve_batch: out must be a writeable C-contiguous complex128 [n, nE] array")
+            e = out
+        else:
+            e = np.zeros((n, self.nE), np.complex128) if e0 is None else np.array(e0, np.complex128)
         bcp = None if bc is None else np.ascontiguousarray(bc, np.complex128)
         srcp = None if src is None else np.ascontiguousarray(src, np.complex128)
         st = np.zeros(n, np.int32)

@@ -52,3 +52,23 @@ def test_invalid_arguments_rejected_before_device_use():
     assert L.mt3d_create(0, 3, 3, 3, 3, p, p, p, C.byref(h)) == 5  # nzAir >= nz
     assert L.mt3d_set_control(None, 40, 20, 100, 1e-7, 1e-7, 1e-5, 1, 0) == 5
     assert L.mt3d_fwdsolve(None, 0, None, None, None) == 5
+
+
+def test_fwdsolve_batch_out_buffer_is_checked_before_the_library():
+    """fwdsolve_batch(out=...) takes the caller's array as the library's
+    in/out buffer; arrays it cannot pass through unchanged are refused before
+    any device call."""
+    import pytest
+
+    class Fake:
+        nE = 10
+        fwdsolve_batch = capi.Solver.fwdsolve_batch
+
+    f = Fake()
+    om = np.ones(2)
+    for bad in (np.zeros((2, 10), np.complex64), np.zeros((2, 20), np.complex128)[:, ::2],
+                np.zeros((3, 10), np.complex128)):
+        with pytest.raises(ValueError):
+            f.fwdsolve_batch(om, out=bad)
+    with pytest.raises(ValueError):
+        f.fwdsolve_batch(om, e0=np.zeros((2, 10)), out=np.zeros((2, 10), np.complex128))
