@@ -64,6 +64,10 @@ __device__ __forceinline__ bool tma_march(TmaSmem &sm, const TmaParams &tp, cons
     const float hdX = (hasH && hi <= g.nx) ? g.delX[hi] : 0.f, hdY = (hasH && hj <= g.ny) ? g.delY[hj] : 0.f;
 
     // tensor-copy destinations must be 128-byte aligned: refuse otherwise
+    // a chunk past the last node plane (the last chunks when the chunk count
+    // does not divide the planes) has no work; it must return before it
+    // issues a copy, since it would never wait for its third plane
+    if (k0 >= k1) return true;
     if ((smem_addr(sm.fld[0]) | smem_addr(sm.sig[0]) | smem_addr(sm.nod[0])) & 127u) {
         if (issuer) atomicExch(err, 2);
         return false;

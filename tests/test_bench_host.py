@@ -88,3 +88,17 @@ def test_cpu_iterations_source_is_named():
     assert it > 0 and src
     it2, src2 = bench.cpu_iterations("precision")
     assert it2 == bench.CPU_ITERS_PRECISION and "100x100x60" in src2
+
+
+def test_reference_arm_times_bounded_sample_steps():
+    """The CPU baseline (the reference arm's measurement) on the small
+    workload: the oracle is set up once per process and each timed step runs
+    a fixed number of Krylov iterations in every process, so each step's wall
+    time is measured and the projected rate follows from the time per
+    iteration."""
+    cb, walls = bench.cpu_baseline("small", 2, steps=2, warmup=1)
+    assert len(walls) == 2 and all(w > 0 for w in walls)
+    assert cb["kind"] == "port-projected" and cb["cores"] == 2
+    assert cb["value"] == pytest.approx(2.0 / (cb["seconds_per_iteration"] * cb["iterations_per_solve"]))
+    # every timed step ran CPU_SAMPLE_ITERS iterations per process
+    assert max(walls) >= bench.CPU_SAMPLE_ITERS * cb["seconds_per_iteration"] * 0.5

@@ -121,6 +121,28 @@ def test_multi_with_polynomial_preconditioner(mprob):
             s.set_control(IterPerDivCor=150, MaxDivCor=40, precision=capi.PREC_MIXED)
 
 
+def test_chunk_counts_with_empty_chunks(mprob):
+    """Chunk counts whose last chunk starts past the last node plane (6 of 15
+    planes for the first grid: chunks of 3, the sixth empty; 6 of 19 and 9 of
+    23 likewise) give the solutions of the default counts: the blocks of an
+    empty chunk issue no copy and add nothing."""
+    probs, ss = mprob
+    for (g, *_), c in zip(probs, (6, 6, 9)):
+        planes = g.nz + 1
+        assert (c - 1) * (-(-planes // c)) >= planes
+    out = []
+    for zch in ([0, 0, 0], [6, 6, 9]):
+        es = [np.zeros((5, g.n_edges), complex) for g, *_ in probs]
+        st, rc = capi.fwdsolve_multi(ss, [p[2] for p in probs], es, trans=[p[5] for p in probs],
+                                     bc=[p[3] for p in probs], src=[p[4] for p in probs], zchunks=zch)
+        assert rc == 0
+        out.append(es)
+    for (g, m, *_), a, b in zip(probs, *out):
+        em = earth_mask(g, m)
+        for r in range(5):
+            assert relerr(b[r][em], a[r][em]) < 1e-5, (g.nx, r)
+
+
 def test_chunk_tuner_returns_and_caches_a_choice(mprob, tmp_path):
     import torch
     from mt3d import tune
