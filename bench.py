@@ -459,7 +459,8 @@ def main():
                             [b[1].data_ptr() for b in b0], [b[2].data_ptr() for b in b0], [b[3] for b in b0],
                             lambda: torch.cuda.synchronize(dev),
                             cache_path=os.environ.get("MT3D_TUNE_CACHE",
-                                                      os.path.join(tempfile.gettempdir(), "mt3d_tune.json")))
+                                                      os.path.join(tempfile.gettempdir(), "mt3d_tune.json")),
+                            reset=lambda: [d_e.zero_() for _, _, d_e, _ in solvers])
 
     def step(k):
         if multi:

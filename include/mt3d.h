@@ -233,7 +233,10 @@ MT3D_API int mt3d_bicg(mt3d_handle h, const double *b, double *x, int maxit, dou
  *              optional boundary data.
  *   e: full edge vector; interior entries are the initial guess on entry, the
  *      solution on return (boundary entries as in the reference's post-
- *      processing).
+ *      processing).  A transposed solve returns its interior entries
+ *      multiplied by the edge volumes V_E, as FWDsolve3D does
+ *      (EMsolve3D.f90:356-359), so its output is no first guess for
+ *      another transposed solve.
  * Returns MT3D_OK when converged. */
 MT3D_API int mt3d_fwdsolve(mt3d_handle h, int trans, const double *bc, const double *src, double *e);
 

@@ -33,9 +33,11 @@ def candidates(nz: int):
     return [0] + [c for c in CANDIDATES if (nz + 1) // c >= 4]
 
 
-def _time(solvers, omegas, e_ptrs, bc_ptrs, src_ptrs, trans, zch, sync, reps: int) -> float:
+def _time(solvers, omegas, e_ptrs, bc_ptrs, src_ptrs, trans, zch, sync, reset, reps: int) -> float:
     best = float("inf")
     for _ in range(reps):
+        if reset is not None:
+            reset()
         sync()
         t0 = time.perf_counter()
         capi.fwdsolve_multi(solvers, omegas, e_ptrs, trans=trans, bc=bc_ptrs, src=src_ptrs, zchunks=zch, device=True)
@@ -45,12 +47,16 @@ def _time(solvers, omegas, e_ptrs, bc_ptrs, src_ptrs, trans, zch, sync, reps: in
 
 
 def tune(solvers, omegas, e_ptrs, bc_ptrs, src_ptrs, trans, sync, cache_path: str | None = None, iters: int = 60,
-         reps: int = 2):
+         reps: int = 2, reset=None):
     """Per-grid chunk counts for a multi-grid batch (list of ints, 0 = the
     library's choice).  The timed runs are mt3d_fwdsolve_multi calls on the
     caller's device buffers (e_ptrs are overwritten) with one FP32 cycle of
-    `iters` iterations per grid; sync() must wait for the device.  The
-    handles' control is restored afterwards."""
+    `iters` iterations per grid; sync() must wait for the device, and
+    reset() (if given) must zero the e buffers, which every run then starts
+    from.  Without it a run starts from the previous run's output, and a
+    transposed solve returns its interior field multiplied by the edge
+    volumes (as FWDsolve3D does), which is no first guess: repeated runs
+    then grow without bound.  The handles' control is restored afterwards."""
     key = key_of(solvers, omegas)
     cache = {}
     if cache_path and os.path.exists(cache_path):
@@ -63,13 +69,13 @@ def tune(solvers, omegas, e_ptrs, bc_ptrs, src_ptrs, trans, sync, cache_path: st
         for s, c in zip(solvers, keep):
             s.set_control(**dict(c, IterPerDivCor=iters, MaxDivCor=1))
         zch = [0] * len(solvers)
-        t_best = _time(solvers, omegas, e_ptrs, bc_ptrs, src_ptrs, trans, zch, sync, reps)
+        t_best = _time(solvers, omegas, e_ptrs, bc_ptrs, src_ptrs, trans, zch, sync, reset, reps)
         t_default = t_best
         for g, s in enumerate(solvers):
             for c in candidates(s.grid.nz)[1:]:
                 trial = list(zch)
                 trial[g] = c
-                t = _time(solvers, omegas, e_ptrs, bc_ptrs, src_ptrs, trans, trial, sync, reps)
+                t = _time(solvers, omegas, e_ptrs, bc_ptrs, src_ptrs, trans, trial, sync, reset, reps)
                 if t < 0.98 * t_best:
                     t_best, zch = t, trial
     finally:

@@ -144,14 +144,20 @@ def test_chunk_counts_with_empty_chunks(mprob):
 
 
 def test_chunk_tuner_returns_and_caches_a_choice(mprob, tmp_path):
+    """The tuner's timed runs (forward and transposed right-hand sides, each
+    run from a zero first guess) return a valid choice, cache it and leave
+    the handles' control and finite fields behind."""
     import torch
     from mt3d import tune
     probs, ss = mprob
     dbc = [torch.from_numpy(p[3]).cuda() for p in probs]
+    dsrc = [torch.from_numpy(p[4]).cuda() for p in probs]
     de = [torch.zeros((5, g.n_edges), dtype=torch.complex128, device="cuda") for g, *_ in probs]
     path = str(tmp_path / "tune.json")
     zch = tune.tune(ss, [p[2] for p in probs], [x.data_ptr() for x in de], [x.data_ptr() for x in dbc],
-                    None, [np.zeros(5, np.int32)] * 3, torch.cuda.synchronize, cache_path=path, iters=20, reps=1)
+                    [x.data_ptr() for x in dsrc], [p[5] for p in probs], torch.cuda.synchronize, cache_path=path,
+                    iters=20, reps=2, reset=lambda: [x.zero_() for x in de])
     assert len(zch) == 3 and all(z in tune.candidates(s.grid.nz) for z, s in zip(zch, ss))
+    assert all(bool(torch.isfinite(x).all()) for x in de)
     assert tune.tune(ss, [p[2] for p in probs], None, None, None, None, None, cache_path=path) == zch
     assert all(s.control["IterPerDivCor"] == 150 for s in ss)
