@@ -314,7 +314,9 @@ MT3D_API int mt3d_apply_kernel(mt3d_handle h, int kernel, const double *x, doubl
  * summed device time in milliseconds and rhs_sweeps: the number of
  * (launch, right-hand side) pairs in which the staged stencil kernels swept a
  * still-running right-hand side, i.e. the stencil work in units of nE edges.
- * Any output may be NULL. */
+ * In a multi-grid batch (mt3d_fwdsolve_multi) the shared stencil launches
+ * are timed on the first grid's handle and every handle counts its own
+ * grid's sweeps.  Any output may be NULL. */
 MT3D_API int mt3d_profile(mt3d_handle h, int enable);
 MT3D_API int mt3d_kernel_time(mt3d_handle h, int precision, int *launches, double *ms, int64_t *rhs_sweeps);
 

@@ -734,7 +734,10 @@ void launch_hat_apply(const KArgs<float> &a, int nrhs, cudaStream_t s) { launch_
 // batch: five launches in all, each over the right-hand sides of every grid
 // (zch[g]: node-plane chunks of grid g's stencil blocks, 0 for the
 // occupancy-based choice)
-int launch_hat_iter_multi(const KArgs<float> *args, const int *nrhs, const int *zch, int ng, cudaStream_t s)
+// as launch_hat_iter, for the grids of a multi-grid batch; ev (4 events, may
+// be null) brackets the operator launches
+int launch_hat_iter_multi(const KArgs<float> *args, const int *nrhs, const int *zch, int ng, cudaStream_t s,
+                          cudaEvent_t *ev)
 {
     if (ng < 1 || ng > kMaxMultiGrids) return 1;
     static_assert(sizeof(HatMulti) <= 32000, "multi-grid parameters exceed the kernel parameter space");
@@ -770,19 +773,23 @@ int launch_hat_iter_multi(const KArgs<float> *args, const int *nrhs, const int *
     counted(poly ? 7 : 5);
     const size_t sm = sizeof(TmaSmem);
     kh_elem_multi<0><<<p.eb0[ng], kThreads, 0, s>>>(p);
+    if (ev) cudaEventRecord(ev[0], s);
     if (poly) {
         kh_vt_multi<2><<<p.sb0[ng], kHatThreads, sm, s>>>(p);
         kh_vt_multi<3><<<p.sb0[ng], kHatThreads, sm, s>>>(p);
     } else {
         kh_vt_multi<0><<<p.sb0[ng], kHatThreads, sm, s>>>(p);
     }
+    if (ev) cudaEventRecord(ev[1], s);
     kh_elem_multi<1><<<p.eb0[ng], kThreads, 0, s>>>(p);
+    if (ev) cudaEventRecord(ev[2], s);
     if (poly) {
         kh_vt_multi<4><<<p.sb0[ng], kHatThreads, sm, s>>>(p);
         kh_vt_multi<5><<<p.sb0[ng], kHatThreads, sm, s>>>(p);
     } else {
         kh_vt_multi<1><<<p.sb0[ng], kHatThreads, sm, s>>>(p);
     }
+    if (ev) cudaEventRecord(ev[3], s);
     kh_elem_multi<2><<<p.eb0[ng], kThreads, 0, s>>>(p);
     return 0;
 }

@@ -139,7 +139,8 @@ void launch_tma_vt(const KArgs<float> &a, const TmaMaps *m, int which, int nrhs,
 void launch_hat_cast(const KArgs<float> &a, const double2 *r64, size_t stride64, int nrhs, cudaStream_t s);
 void launch_hat_iter(const KArgs<float> &a, int nrhs, cudaStream_t s, cudaEvent_t *ev = nullptr);
 void launch_hat_apply(const KArgs<float> &a, int nrhs, cudaStream_t s);
-int launch_hat_iter_multi(const KArgs<float> *args, const int *nrhs, const int *zch, int ng, cudaStream_t s);
+int launch_hat_iter_multi(const KArgs<float> *args, const int *nrhs, const int *zch, int ng, cudaStream_t s,
+                          cudaEvent_t *ev = nullptr);
 void launch_cast_padded(const Geo<double> &g, const OuterState *ost, size_t stride64, const double2 *r64,
                         PadLayout pl, float2 *b32, float2 *x32, int nrhs, cudaStream_t s);
 void launch_update_padded(const Geo<double> &g, const OuterState *ost, size_t stride64, PadLayout pl,

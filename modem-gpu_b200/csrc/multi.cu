@@ -106,8 +106,12 @@ int fwdsolve_multi(int nh, Solver *const *hs, const int *nrhs, const double *con
             }
         }
         if (!ids.empty()) {
+            // with mt3d_profile on, the stencil launches of the whole batch
+            // are timed on the first grid's handle (each handle counts its
+            // own grid's sweeps)
             for (int it = 0; it < maxit; it++)
-                if (launch_hat_iter_multi(args.data(), nr.data(), zc.data(), (int)ids.size(), s)) {
+                if (launch_hat_iter_multi(args.data(), nr.data(), zc.data(), (int)ids.size(), s,
+                                          hs[ids[0]]->fp32_events(4))) {
                     err = "mt3d_fwdsolve_multi: too many grids";
                     restore();
                     return 5;

@@ -122,6 +122,8 @@ class Solver {
     // FP32 cycle, its cast and end kernels, and its stream and device
     KArgs<float> hat_args(int nrhs);
     int hat_cycle_begin(int nrhs, KArgs<float> &a);
+    // n profiling events of the FP32 stencil launches (null unless mt3d_profile is on)
+    cudaEvent_t *fp32_events(int n);
     int hat_cycle_end(int nrhs, const KArgs<float> &a);
     cudaStream_t stream() const { return stream_; }
     int device() const { return dev_; }
