@@ -686,7 +686,6 @@ KArgs<float> Solver::hat_args(int nrhs)
 {
     KArgs<float> a = kargs<float>(nrhs, 1);
     a.maxit = ctl.IterPerDivCor;
-    a.sweeps = nullptr;
     return a;
 }
 
