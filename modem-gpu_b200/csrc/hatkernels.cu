@@ -8,14 +8,17 @@
 // preconditioner is one division at the output edge of the operator kernels
 // (vh = D^-1 A u, th = D^-1 A sh), and no vector of D^-1 exists:
 //
-//   kh_u     u  = rh + beta (u - omega vh)   (u = rh on the first iteration)
-//   kh_vt 0  vh = D^-1 A u,       (rt, v)                  -> alpha
-//   kh_s     sh = rh - alpha vh
-//   kh_vt 1  th = D^-1 A sh,      (t, s), (t, t), (s, s)   -> omega, ||r||
-//   kh_xr    x += alpha u + omega sh,  rh = sh - omega th,  (rt, r) -> beta
+//   kh_u         u  = rh + beta (u - omega vh)   (u = rh on the first iteration)
+//   kh_vt st. 0  vh = D^-1 A u,       (rt, v)                  -> alpha
+//   kh_s         sh = rh - alpha vh
+//   kh_vt st. 1  th = D^-1 A sh,      (t, s), (t, t), (s, s)   -> omega, ||r||
+//   kh_xr        x += alpha u + omega sh,  rh = sh - omega th,  (rt, r) -> beta
 //
 // 163 bytes per edge and iteration instead of the 211 of the unfused
-// kernels (kb_p, kct_vt, kb_s, kct_vt, kb_xr).  The inner products of the
+// kernels (kb_p, kct_vt, kb_s, kct_vt, kb_xr).  With the polynomial
+// preconditioner M^-1 = c D^-1 (2 I - c A D^-1) each operator launch becomes
+// two (stages 2, 3 and 4, 5 of hat_vt) and kh_xr forms M^-1 p and M^-1 s
+// from u, w1, sh and w2.  The inner products of the
 // method in the original variables follow from the hat ones:
 //   - the shadow residual is the reference's rt = r0 = b; with y =
 //     conj(D) b stored once per cycle (written by kh_cast), (rt, r) =
@@ -34,9 +37,9 @@
 // The operator kernels stage u or sh with the tensor copies of tma.cuh.  D =
 // V_E xXO-diagonal of the curl-curl term (col_ccdiag) + the grad-div diagonal
 // DFA^2 (w_s c_s + w_e c_e) + i omega mu0 sigma V_E, from the staged sigma
-// and signed node weights (the weights of the thread's three nodes at plane
-// k are kept in registers from the previous plane, so the node ring keeps
-// two slots).  kh_cast computes the same D from the global tables.
+// and signed node weights (the weights of each node column's three nodes at
+// plane k are kept in registers from the previous plane, so the node ring
+// keeps two slots).  kh_cast computes the same D from the global tables.
 #include <atomic>
 #include <cstring>
 
@@ -176,7 +179,8 @@ __device__ __forceinline__ void hat_s(const KArgs<float> &a, int r, int bx)
 
 // x += alpha u + omega sh (into the buffer that does not hold the best
 // iterate); rh = sh - omega th; rho = (z, rh).  The true residual norm of the
-// new iterate comes from the inner products of kh_vt 1 (BicgState::rn2).
+// new iterate comes from the inner products of kh_vt stage 1 or 5
+// (BicgState::rn2).
 template <bool poly> __device__ __forceinline__ void hat_xr_t(const KArgs<float> &a, int r, int bx)
 {
     BicgState &st = a.st[r];
@@ -245,7 +249,7 @@ template <bool poly> __device__ __forceinline__ void hat_xr_t(const KArgs<float>
         if (a.restart > 0 && st.iter % a.restart == 0) {
             // restart towards steepest descent (cuBiCG, f90/3D_MT/FWD_SP2/
             // solver.f90:1545-1573): rt = r, rho = (rt, r) = ||r||^2, p = r,
-            // omega = 1; the next kh_vt 0 writes the new shadow y = W rh
+            // omega = 1; the next kh_vt stage 0 or 2 writes the new shadow y = W rh
             st.first = 1;
             st.pad = 1;
             st.rho = {st.rn2, 0.0};
