@@ -734,6 +734,92 @@ void launch_hat_iter(const KArgs<float> &a, int nrhs, cudaStream_t s, cudaEvent_
 
 void launch_hat_apply(const KArgs<float> &a, int nrhs, cudaStream_t s) { launch_hat_stage<0>(a, nrhs, s); }
 
+// the shared-memory attribute and occupancy of every operator kernel, set
+// before a capture (tma_resident calls the runtime only the first time)
+template <int stage> static void hat_prime_stage()
+{
+    const size_t sm = sizeof(TmaSmem);
+    tma_resident(kh_vt<stage, false>, sm, 2 + 2 * stage, kHatThreads);
+    tma_resident(kh_vt<stage, true>, sm, 3 + 2 * stage, kHatThreads);
+    tma_resident(kh_vt_multi<stage>, sm, 14 + stage, kHatThreads);
+}
+static void hat_prime()
+{
+    hat_prime_stage<0>();
+    hat_prime_stage<1>();
+    hat_prime_stage<2>();
+    hat_prime_stage<3>();
+    hat_prime_stage<4>();
+    hat_prime_stage<5>();
+}
+
+void HatGraph::reset()
+{
+    if (exec) cudaGraphExecDestroy(exec);
+    exec = nullptr;
+    key.clear();
+}
+HatGraph::~HatGraph()
+{
+    reset();
+    if (cap) cudaStreamDestroy(cap);
+}
+
+cudaError_t hat_graph_run(HatGraph &hg, const KArgs<float> *args, const int *nrhs, const int *zch, int ng, int maxit,
+                          cudaStream_t s)
+{
+    const int n = ng > 0 ? ng : 1;
+    if (ng > kMaxMultiGrids) return cudaErrorInvalidValue;
+    // the key: the launch arguments, the tensor maps they point to, the
+    // right-hand-side and chunk counts and the cycle length
+    std::vector<unsigned char> k;
+    auto put = [&](const void *p, size_t b) {
+        const unsigned char *c = static_cast<const unsigned char *>(p);
+        k.insert(k.end(), c, c + b);
+    };
+    for (int g = 0; g < n; g++) {
+        put(&args[g], sizeof(KArgs<float>));
+        if (args[g].tma) put(args[g].tma, sizeof(TmaMaps));
+        put(&nrhs[g], sizeof(int));
+        const int z = zch ? zch[g] : 0;
+        put(&z, sizeof z);
+    }
+    put(&ng, sizeof ng);
+    put(&maxit, sizeof maxit);
+    if (!hg.exec || k != hg.key) {
+        hg.reset();
+        if (!hg.cap) {
+            cudaError_t e = cudaStreamCreateWithFlags(&hg.cap, cudaStreamNonBlocking);
+            if (e != cudaSuccess) return e;
+        }
+        hat_prime();
+        const long long c0 = g_launch_count.load();
+        cudaError_t e = cudaStreamBeginCapture(hg.cap, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return e;
+        for (int it = 0; it < maxit; it++) {
+            if (ng > 0) launch_hat_iter_multi(args, nrhs, zch, ng, hg.cap);
+            else launch_hat_iter(args[0], nrhs[0], hg.cap);
+        }
+        cudaGraph_t graph = nullptr;
+        e = cudaStreamEndCapture(hg.cap, &graph);
+        hg.launches = g_launch_count.load() - c0;
+        g_launch_count.fetch_sub(hg.launches);
+        if (e != cudaSuccess) {
+            if (graph) cudaGraphDestroy(graph);
+            return e;
+        }
+        e = cudaGraphInstantiate(&hg.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) {
+            hg.exec = nullptr;
+            return e;
+        }
+        hg.key.swap(k);
+    }
+    g_launch_count.fetch_add(hg.launches);
+    return cudaGraphLaunch(hg.exec, s);
+}
+
 // one iteration of the fused FP32 BiCGStab over the grids of a multi-grid
 // batch: five launches in all, each over the right-hand sides of every grid
 // (zch[g]: node-plane chunks of grid g's stencil blocks, 0 for the

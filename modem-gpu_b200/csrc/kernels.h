@@ -1,5 +1,7 @@
 // kernels.h -- kernel argument blocks and launchers (host-visible).
 #pragma once
+#include <vector>
+
 #include "common.cuh"
 
 namespace mt3d {
@@ -139,6 +141,21 @@ void launch_tma_vt(const KArgs<float> &a, const TmaMaps *m, int which, int nrhs,
 void launch_hat_cast(const KArgs<float> &a, const double2 *r64, size_t stride64, int nrhs, cudaStream_t s);
 void launch_hat_iter(const KArgs<float> &a, int nrhs, cudaStream_t s, cudaEvent_t *ev = nullptr);
 void launch_hat_apply(const KArgs<float> &a, int nrhs, cudaStream_t s);
+// One FP32 cycle of the fused iteration (maxit iterations of launch_hat_iter,
+// or of launch_hat_iter_multi over ng grids) captured as a CUDA graph and
+// replayed while the launch arguments stay the same; the graph is captured
+// on a private stream and launched on the caller's.
+struct HatGraph {
+    cudaGraphExec_t exec = nullptr;
+    cudaStream_t cap = nullptr;
+    std::vector<unsigned char> key;
+    long long launches = 0;  // kernel launches in one replay
+    void reset();
+    ~HatGraph();
+};
+// ng = 0: one grid (args[0], nrhs[0]); returns a CUDA error code
+cudaError_t hat_graph_run(HatGraph &hg, const KArgs<float> *args, const int *nrhs, const int *zch, int ng, int maxit,
+                          cudaStream_t s);
 int launch_hat_iter_multi(const KArgs<float> *args, const int *nrhs, const int *zch, int ng, cudaStream_t s,
                           cudaEvent_t *ev = nullptr);
 void launch_cast_padded(const Geo<double> &g, const OuterState *ost, size_t stride64, const double2 *r64,

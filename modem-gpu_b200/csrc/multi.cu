@@ -106,19 +106,19 @@ int fwdsolve_multi(int nh, Solver *const *hs, const int *nrhs, const double *con
             }
         }
         if (!ids.empty()) {
-            // with mt3d_profile on, the stencil launches of the whole batch
-            // are timed on the first grid's handle (each handle counts its
-            // own grid's sweeps)
-            for (int it = 0; it < maxit; it++)
-                if (launch_hat_iter_multi(args.data(), nr.data(), zc.data(), (int)ids.size(), s,
-                                          hs[ids[0]]->fp32_events(4))) {
-                    err = "mt3d_fwdsolve_multi: too many grids";
-                    restore();
-                    return 5;
-                }
+            // the cycle of the whole batch as one CUDA graph kept on the
+            // first grid's handle; with mt3d_profile on, timed launches
+            // instead (each handle counts its own grid's sweeps)
+            const int mrc = hs[ids[0]]->run_hat_multi(args.data(), nr.data(), zc.data(), (int)ids.size(), maxit, s);
+            if (mrc == 5) {
+                err = "mt3d_fwdsolve_multi: too many grids";
+                restore();
+                return 5;
+            }
             const cudaError_t ce = cudaGetLastError();
-            if (ce != cudaSuccess) {
-                err = std::string("mt3d_fwdsolve_multi: launch failed: ") + cudaGetErrorString(ce);
+            if (mrc == 4 || ce != cudaSuccess) {
+                err = std::string("mt3d_fwdsolve_multi: launch failed: ") +
+                      cudaGetErrorString(ce != cudaSuccess ? ce : cudaErrorUnknown);
                 restore();
                 return 4;
             }

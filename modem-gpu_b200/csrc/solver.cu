@@ -494,7 +494,10 @@ template <> KArgs<double> Solver::kargs<double>(int nrhs, int)
 }
 template <> KArgs<float> Solver::kargs<float>(int nrhs, int)
 {
-    KArgs<float> a{};
+    // zeroed as bytes: the captured FP32 cycle is keyed on the bytes of its
+    // arguments, padding included
+    KArgs<float> a;
+    std::memset(&a, 0, sizeof a);
     Workspace &w = ws_;
     a.sweeps = prof_ ? prof_cnt_.as<unsigned long long>() + 1 : nullptr;
     a.g = g32_;
@@ -677,9 +680,26 @@ int Solver::run_hat(int nrhs, int maxit)
     KArgs<float> a = kargs<float>(nrhs, 1);
     a.maxit = maxit;
     launch_hat_cast(a, ws_.tmp.as<double2>(), nE, nrhs, stream_);
-    for (int it = 0; it < maxit; it++) launch_hat_iter(a, nrhs, stream_, next_events(4));
+    if (prof_) {
+        // timed launches, events around the operator kernels
+        for (int it = 0; it < maxit; it++) launch_hat_iter(a, nrhs, stream_, next_events(4));
+    } else {
+        // the cycle as one CUDA graph, replayed while its arguments hold
+        const cudaError_t e = hat_graph_run(hat_graph_, &a, &nrhs, nullptr, 0, maxit, stream_);
+        if (e != cudaSuccess) return check(e, "fused BiCGStab graph");
+    }
     launch_bicg_finish(a, nrhs, stream_);
     return check(cudaGetLastError(), "fused BiCGStab launch");
+}
+
+int Solver::run_hat_multi(const KArgs<float> *args, const int *nrhs, const int *zch, int ng, int maxit, cudaStream_t s)
+{
+    if (prof_) {
+        for (int it = 0; it < maxit; it++)
+            if (launch_hat_iter_multi(args, nrhs, zch, ng, s, fp32_events(4))) return 5;
+        return 0;
+    }
+    return hat_graph_run(hat_graph_multi_, args, nrhs, zch, ng, maxit, s) == cudaSuccess ? 0 : 4;
 }
 
 KArgs<float> Solver::hat_args(int nrhs)

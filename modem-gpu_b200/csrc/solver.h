@@ -124,6 +124,9 @@ class Solver {
     int hat_cycle_begin(int nrhs, KArgs<float> &a);
     // n profiling events of the FP32 stencil launches (null unless mt3d_profile is on)
     cudaEvent_t *fp32_events(int n);
+    // maxit fused FP32 iterations of a multi-grid batch on stream s: one
+    // captured graph (kept on this handle) or, when profiling, timed launches
+    int run_hat_multi(const KArgs<float> *args, const int *nrhs, const int *zch, int ng, int maxit, cudaStream_t s);
     int hat_cycle_end(int nrhs, const KArgs<float> &a);
     cudaStream_t stream() const { return stream_; }
     int device() const { return dev_; }
@@ -185,6 +188,7 @@ class Solver {
     double prof_ms_[2] = {0.0, 0.0};
     std::vector<int> ev_prec_;  // precision of each recorded event
     DevBuf prof_cnt_;           // device sweep counters [FP64, FP32]
+    HatGraph hat_graph_, hat_graph_multi_;  // captured FP32 cycles (single grid, multi-grid batch)
     cudaEvent_t *next_events(int n);
     void collect_events();
     Geo<double> g64_{};
