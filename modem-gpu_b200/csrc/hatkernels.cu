@@ -17,8 +17,10 @@
 // 163 bytes per edge and iteration instead of the 211 of the unfused
 // kernels (kb_p, kct_vt, kb_s, kct_vt, kb_xr).  With the polynomial
 // preconditioner M^-1 = c D^-1 (2 I - c A D^-1) each operator launch becomes
-// two (stages 2, 3 and 4, 5 of hat_vt) and kh_xr forms M^-1 p and M^-1 s
-// from u, w1, sh and w2.  The inner products of the
+// two (stages 2, 3 and 4, 5 of hat_vt); kh_xr accumulates yhat = sum (alpha
+// u + omega sh) as in the diagonal case, and the end of the cycle turns the
+// best yhat into x = M^-1 D yhat = c (2 yhat - c D^-1 A yhat) (stage 6 and
+// kh_conv).  The inner products of the
 // method in the original variables follow from the hat ones:
 //   - the shadow residual is the reference's rt = r0 = b; with y =
 //     conj(D) b stored once per cycle (written by kh_cast), (rt, r) =
@@ -181,7 +183,7 @@ __device__ __forceinline__ void hat_s(const KArgs<float> &a, int r, int bx)
 // iterate); rh = sh - omega th; rho = (z, rh).  The true residual norm of the
 // new iterate comes from the inner products of kh_vt stage 1 or 5
 // (BicgState::rn2).
-template <bool poly> __device__ __forceinline__ void hat_xr_t(const KArgs<float> &a, int r, int bx)
+__device__ __forceinline__ void hat_xr(const KArgs<float> &a, int r, int bx)
 {
     BicgState &st = a.st[r];
     if (st.status != KS_RUNNING || !a.ost[r].active) return;
@@ -194,27 +196,17 @@ template <bool poly> __device__ __forceinline__ void hat_xr_t(const KArgs<float>
     const float4 *U = reinterpret_cast<const float4 *>(a.ph) + off;
     const float4 *SH = reinterpret_cast<const float4 *>(a.sh) + off;
     const float4 *TH = reinterpret_cast<const float4 *>(a.t) + off;
-    const float4 *W1 = reinterpret_cast<const float4 *>(a.p) + off;
-    const float4 *W2 = reinterpret_cast<const float4 *>(a.s) + off;
     float4 *RH = reinterpret_cast<float4 *>(a.r) + off;
     const float4 *Y = reinterpret_cast<const float4 *>(a.rt) + off;
-    // with the polynomial preconditioner the directions are M^-1 p =
-    // c (2 u - c w1) and M^-1 s = c (2 sh - c w2)
-    const float c2 = 2.f * a.pc, cc = a.pc * a.pc;
+    // with the polynomial preconditioner the iterate is x = M^-1 yhat, and
+    // yhat = sum (alpha u + omega sh) accumulates here like the diagonal
+    // case's x (u = D^-1 p, sh = D^-1 s); launch_hat_conv turns the cycle's
+    // best yhat into x = c (2 yhat - c D^-1 A yhat) at its end
     double u[2] = {0.0, 0.0};
     HAT_PAIRS(a, bx)
     {
         const float4 sh = SH[q];
-        if (poly) {
-            const float4 pu = U[q], w1 = W1[q], w2 = W2[q];
-            const float4 dp = make_float4(c2 * pu.x - cc * w1.x, c2 * pu.y - cc * w1.y, c2 * pu.z - cc * w1.z,
-                                          c2 * pu.w - cc * w1.w);
-            const float4 ds = make_float4(c2 * sh.x - cc * w2.x, c2 * sh.y - cc * w2.y, c2 * sh.z - cc * w2.z,
-                                          c2 * sh.w - cc * w2.w);
-            XD[q] = add4(add4(XS[q], c2mul2(al, dp)), c2mul2(om, ds));
-        } else {
-            XD[q] = add4(add4(XS[q], c2mul2(al, U[q])), c2mul2(om, sh));
-        }
+        XD[q] = add4(add4(XS[q], c2mul2(al, U[q])), c2mul2(om, sh));
         const float4 rn = sub4(sh, c2mul2(om, TH[q]));
         RH[q] = rn;
         const float4 y = Y[q];  // conj(y) rh
@@ -263,12 +255,6 @@ template <bool poly> __device__ __forceinline__ void hat_xr_t(const KArgs<float>
         st.beta = cd_mul(cd_div(st.rho, st.rho1), cd_div(st.alpha, st.omega));
         if (cd_zero(st.beta)) st.status = KS_BREAKDOWN;
     }
-}
-
-__device__ __forceinline__ void hat_xr(const KArgs<float> &a, int r, int bx)
-{
-    if (a.pc > 0.f) hat_xr_t<true>(a, r, bx);
-    else hat_xr_t<false>(a, r, bx);
 }
 
 // ---------------------------------------------------------------------------
@@ -539,6 +525,7 @@ __device__ __forceinline__ bool hat_march(TmaSmem &sm, const TmaParams &tp, cons
 //     3  vh = c (2 w1 - c D^-1 A w1),  (rt, v)              -> alpha
 //     4  w2 = D^-1 A sh
 //     5  th = c (2 w2 - c D^-1 A w2),  (t, s)_W ... with s = sh read from memory
+//     6  p = D^-1 A yhat at the end of a cycle (yhat in x0; see kh_conv)
 // (D^-1 A (M^-1 p) = c (2 D^-1 A u - c D^-1 A w1) since u = D^-1 p.)  Stages
 // 0 and 2 stage u and, after a restart, write the new shadow y = W rh
 // (u = rh on that iteration).  For column tile bx and plane chunk bz of gz of
@@ -550,14 +537,15 @@ __device__ __forceinline__ void hat_vt(const TmaParams &tp, const KArgs<float> &
     constexpr bool kt = stage == 1 || stage == 5;  // omega and ||r||
     constexpr bool poly = stage == 3 || stage == 5;
     constexpr bool dots = kv || kt;
+    constexpr bool conv = stage == 6;  // after the cycle, whatever the status
     BicgState &st = a.st[r];
-    if (st.status != KS_RUNNING || !a.ost[r].active) return;
-    if (a.sweeps && threadIdx.x == 0 && bx == 0 && bz == 0) atomicAdd(a.sweeps, 1ULL);
+    if ((!conv && st.status != KS_RUNNING) || !a.ost[r].active) return;
+    if (!conv && a.sweeps && threadIdx.x == 0 && bx == 0 && bz == 0) atomicAdd(a.sweeps, 1ULL);
     int i0, j0, k0, k1;
     tma_tile_at(a.cmap, bx, i0, j0);
     tma_range_at(a.g.nz, bz, gz, k0, k1);
     const size_t off = (size_t)r * a.stride;
-    float2 *out = (stage == 0 || stage == 3 ? a.v : stage == 2 ? a.p : stage == 4 ? a.s : a.t) + off;
+    float2 *out = (stage == 0 || stage == 3 ? a.v : stage == 2 || stage == 6 ? a.p : stage == 4 ? a.s : a.t) + off;
     float2 *Yr = a.rt + off;
     // after a restart (first iteration, pad set) the shadow becomes the
     // current residual: y = W rh, rh being the staged u of this launch
@@ -654,10 +642,10 @@ template <int K> __global__ void __launch_bounds__(kThreads) kh_elem_multi(const
     else if (K == 1) hat_s(a, r, bx);
     else hat_xr(a, r, bx);
 }
-// input map of each stage: u, sh, u, w1, sh, w2
+// input map of each stage: u, sh, u, w1, sh, w2, x0
 __host__ __device__ constexpr int stage_input(int stage)
 {
-    return stage == 0 || stage == 2 ? 0 : stage == 1 || stage == 4 ? 1 : stage == 3 ? 2 : 3;
+    return stage == 0 || stage == 2 ? 0 : stage == 1 || stage == 4 ? 1 : stage == 3 ? 2 : stage == 6 ? 4 : 3;
 }
 template <int stage> __global__ void __launch_bounds__(kHatThreads, 4) kh_vt_multi(const __grid_constant__ HatMulti p)
 {
@@ -697,7 +685,7 @@ template <int stage> static void launch_hat_stage(const KArgs<float> &a, int nrh
     const TmaMaps *m = a.tma;
     TmaParams tp;
     constexpr int in = stage_input(stage);
-    tp.in = in == 0 ? m->ph : in == 1 ? m->sh : in == 2 ? m->pw : m->sw;
+    tp.in = in == 0 ? m->ph : in == 1 ? m->sh : in == 2 ? m->pw : in == 3 ? m->sw : m->x0;
     tp.sig = m->sig;
     tp.node = m->node;
     if (a.gd) launch_hat_vt_t<stage, true>(a, tp, nrhs, s);
@@ -734,6 +722,31 @@ void launch_hat_iter(const KArgs<float> &a, int nrhs, cudaStream_t s, cudaEvent_
 
 void launch_hat_apply(const KArgs<float> &a, int nrhs, cudaStream_t s) { launch_hat_stage<0>(a, nrhs, s); }
 
+// x = c (2 yhat - c p) with p = D^-1 A yhat (stage 6): the cycle's iterate
+// from its accumulation in the D^-1-scaled space, for every active right-hand
+// side (x0 holds the best yhat after launch_bicg_finish)
+__global__ void __launch_bounds__(kThreads) kh_conv(KArgs<float> a)
+{
+    const int r = blockIdx.y, bx = blockIdx.x;
+    if (!a.ost[r].active) return;
+    const size_t off = (size_t)r * a.stride / 2;
+    float4 *X = reinterpret_cast<float4 *>(a.x0) + off;
+    const float4 *P = reinterpret_cast<const float4 *>(a.p) + off;
+    const float c2 = 2.f * a.pc, cc = a.pc * a.pc;
+    HAT_PAIRS(a, bx)
+    {
+        const float4 x = X[q], w = P[q];
+        X[q] = make_float4(c2 * x.x - cc * w.x, c2 * x.y - cc * w.y, c2 * x.z - cc * w.z, c2 * x.w - cc * w.w);
+    }
+}
+void launch_hat_conv(const KArgs<float> &a, int nrhs, cudaStream_t s)
+{
+    if (!(a.pc > 0.f)) return;
+    launch_hat_stage<6>(a, nrhs, s);
+    counted(1);
+    kh_conv<<<dim3(a.nblk, nrhs), kThreads, 0, s>>>(a);
+}
+
 // the shared-memory attribute and occupancy of every operator kernel, set
 // before a capture (tma_resident calls the runtime only the first time)
 template <int stage> static void hat_prime_stage()
@@ -741,7 +754,7 @@ template <int stage> static void hat_prime_stage()
     const size_t sm = sizeof(TmaSmem);
     tma_resident(kh_vt<stage, false>, sm, 2 + 2 * stage, kHatThreads);
     tma_resident(kh_vt<stage, true>, sm, 3 + 2 * stage, kHatThreads);
-    tma_resident(kh_vt_multi<stage>, sm, 14 + stage, kHatThreads);
+    if (stage < 6) tma_resident(kh_vt_multi<(stage < 6 ? stage : 0)>, sm, 16 + stage, kHatThreads);
 }
 static void hat_prime()
 {
@@ -751,6 +764,7 @@ static void hat_prime()
     hat_prime_stage<3>();
     hat_prime_stage<4>();
     hat_prime_stage<5>();
+    hat_prime_stage<6>();
 }
 
 void HatGraph::reset()
@@ -835,12 +849,12 @@ int launch_hat_iter_multi(const KArgs<float> *args, const int *nrhs, const int *
     std::memset(&p, 0, sizeof p);
     p.ng = ng;
     const size_t smb = sizeof(TmaSmem);
-    const int res = tma_resident(kh_vt_multi<0>, smb, 14, kHatThreads);
-    tma_resident(kh_vt_multi<1>, smb, 15, kHatThreads);
-    tma_resident(kh_vt_multi<2>, smb, 16, kHatThreads);
-    tma_resident(kh_vt_multi<3>, smb, 17, kHatThreads);
-    tma_resident(kh_vt_multi<4>, smb, 18, kHatThreads);
-    tma_resident(kh_vt_multi<5>, smb, 19, kHatThreads);
+    const int res = tma_resident(kh_vt_multi<0>, smb, 16, kHatThreads);
+    tma_resident(kh_vt_multi<1>, smb, 17, kHatThreads);
+    tma_resident(kh_vt_multi<2>, smb, 18, kHatThreads);
+    tma_resident(kh_vt_multi<3>, smb, 19, kHatThreads);
+    tma_resident(kh_vt_multi<4>, smb, 20, kHatThreads);
+    tma_resident(kh_vt_multi<5>, smb, 21, kHatThreads);
     p.eb0[0] = p.sb0[0] = 0;
     for (int g = 0; g < ng; g++) {
         p.a[g] = args[g];

@@ -141,6 +141,9 @@ void launch_tma_vt(const KArgs<float> &a, const TmaMaps *m, int which, int nrhs,
 void launch_hat_cast(const KArgs<float> &a, const double2 *r64, size_t stride64, int nrhs, cudaStream_t s);
 void launch_hat_iter(const KArgs<float> &a, int nrhs, cudaStream_t s, cudaEvent_t *ev = nullptr);
 void launch_hat_apply(const KArgs<float> &a, int nrhs, cudaStream_t s);
+// with the polynomial preconditioner: the cycle's iterate x = M^-1 yhat in x0
+// (after launch_bicg_finish); nothing otherwise
+void launch_hat_conv(const KArgs<float> &a, int nrhs, cudaStream_t s);
 // One FP32 cycle of the fused iteration (maxit iterations of launch_hat_iter,
 // or of launch_hat_iter_multi over ng grids) captured as a CUDA graph and
 // replayed while the launch arguments stay the same; the graph is captured

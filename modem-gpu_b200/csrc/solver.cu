@@ -689,6 +689,7 @@ int Solver::run_hat(int nrhs, int maxit)
         if (e != cudaSuccess) return check(e, "fused BiCGStab graph");
     }
     launch_bicg_finish(a, nrhs, stream_);
+    launch_hat_conv(a, nrhs, stream_);
     return check(cudaGetLastError(), "fused BiCGStab launch");
 }
 
@@ -729,6 +730,7 @@ cudaEvent_t *Solver::fp32_events(int n)
 int Solver::hat_cycle_end(int nrhs, const KArgs<float> &a)
 {
     launch_bicg_finish(a, nrhs, stream_);
+    launch_hat_conv(a, nrhs, stream_);
     return check(cudaGetLastError(), "fused BiCGStab end");
 }
 

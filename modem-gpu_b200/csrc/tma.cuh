@@ -163,7 +163,7 @@ __device__ __forceinline__ TmaSmem &tma_smem()
 // the chunk count of stagekernels.cu, for the resident blocks of these
 // kernels; `slot` identifies the kernel (its shared-memory attribute is set
 // the first time its slot is seen), so every kernel needs its own slot
-constexpr int kTmaSlots = 20;
+constexpr int kTmaSlots = 24;
 // the fused stencil of hatkernels.cu: 128 threads, each on two node rows
 // (ty and ty + 4) of the 32 x 8 tile
 constexpr int kHatThreads = 128, kHatRows = kTY / 2;
