@@ -5,6 +5,7 @@ import os
 import re
 
 import numpy as np
+import pytest
 
 from mt3d import capi, models
 
@@ -72,3 +73,24 @@ def test_fwdsolve_batch_out_buffer_is_checked_before_the_library():
             f.fwdsolve_batch(om, out=bad)
     with pytest.raises(ValueError):
         f.fwdsolve_batch(om, e0=np.zeros((2, 10)), out=np.zeros((2, 10), np.complex128))
+
+
+def test_missing_or_stale_library_fails_loudly(tmp_path):
+    """The binding has no fallback: a library that is not there, or one built
+    from other sources than the tree holds, is an error, not a slower path."""
+    with pytest.raises(FileNotFoundError):
+        _load_fresh(str(tmp_path / "libmt3d.so"))
+    # a file that carries no source hash of this tree
+    stale = tmp_path / "stale.so"
+    stale.write_bytes(b"\x7fELF" + bytes(64))
+    with pytest.raises(RuntimeError, match="rebuild"):
+        capi.check_fresh(str(stale))
+
+
+def _load_fresh(path):
+    saved = capi._lib
+    capi._lib = None
+    try:
+        return capi.load(path)
+    finally:
+        capi._lib = saved
