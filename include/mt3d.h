@@ -229,8 +229,13 @@ MT3D_API int mt3d_bicg(mt3d_handle h, const double *b, double *x, int maxit, dou
  *              holds the tangential boundary field, src (full edge vector,
  *              interior entries used, may be NULL) an interior source already
  *              multiplied by -ISIGN i omega mu0.
- *   trans = 1: transposed problem; src is the adjoint source (required), bc
- *              optional boundary data.
+ *   trans = 1: transposed problem; src is the adjoint source, bc optional
+ *              boundary data.  Without a source (src NULL or zero) the
+ *              interior solution is zero and no Krylov call runs (0
+ *              iterations), as in f90/3D_MT/FWD_SP2/EMsolve3D.f90:233-245.
+ *   A right-hand side that is zero otherwise (no boundary data, no source)
+ *   gives a zero solution reported as one iteration with relative residual
+ *   0, as BICG reports b = 0 (f90/3D_MT/FWD_SP2/solver.f90:780-786).
  *   e: full edge vector; interior entries are the initial guess on entry, the
  *      solution on return (boundary entries as in the reference's post-
  *      processing).  A transposed solve returns its interior entries

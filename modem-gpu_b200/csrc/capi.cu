@@ -240,10 +240,6 @@ int mt3d_bicg(mt3d_handle h, const double *b, double *x, int maxit, double tol, 
 int mt3d_fwdsolve(mt3d_handle h, int trans, const double *bc, const double *src, double *e)
 {
     return wrap(h, [&] {
-        if (trans && !src) {
-            // the reference returns the boundary data (or zero) when the
-            // transposed problem has no source (EMsolve3D.f90:170-181)
-        }
         double om = h->s.omega;
         if (!(om > 0)) {
             h->s.last_error = "mt3d_fwdsolve: frequency not set (call mt3d_update_freq)";

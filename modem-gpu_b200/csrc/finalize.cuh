@@ -68,7 +68,9 @@ __device__ inline void fin_t(BicgState &st, const double *tot)
 __device__ inline void fin_res64(OuterState &os, const double *tot)
 {
     const double rn = sqrt(tot[0]);
-    os.relres = rn / os.bnorm64;
+    // a zero right-hand side with its zero solution has residual 0, as BICG
+    // reports for b = 0 (not 0 / 0)
+    os.relres = (os.bnorm64 == 0.0 && rn == 0.0) ? 0.0 : rn / os.bnorm64;
     os.scale = rn > 0.0 ? 1.0 / rn : 0.0;
 }
 

@@ -1012,9 +1012,11 @@ int Solver::solve_begin(SolveRun &run, int nrhs, const double *omegas, const int
         KArgs<double> a = kargs<double>(nrhs, 0);
         launch_norm_b(a, nrhs, stream_);
     }
-    // transposed problem without a source: zero solution (plus boundary data)
+    // transposed problem without a source: zero solution (plus boundary
+    // data), whatever the first guess (f90/3D_MT/FWD_SP2/EMsolve3D.f90:233-245)
     for (int r = 0; r < nrhs; r++)
         if (os[r].trans && !os[r].has_src) {
+            cudaMemsetAsync(X + (size_t)r * nE, 0, ebytes, stream_);
             os[r].active = 0;
             os[r].converged = 1;
         }
@@ -1027,10 +1029,15 @@ int Solver::solve_begin(SolveRun &run, int nrhs, const double *omegas, const int
             os[r].failed = 3;
         } else if (os[r].active && os[r].bnorm64 == 0.0) {
             // zero right-hand side (no boundary data, no source): zero
-            // interior solution, as BICG returns for b = 0
+            // interior solution, reported as BICG reports b = 0 (one
+            // iteration, relative residual 0; f90/3D_MT/FWD_SP2/
+            // solver.f90:780-786)
             cudaMemsetAsync(X + (size_t)r * nE, 0, ebytes, stream_);
             os[r].active = 0;
             os[r].converged = 1;
+            os[r].nIterTotal = 1;
+            os[r].relres = 0.0;
+            run.dg[r].EMrelErr.push_back(0.0);
         }
     }
     // initial divergence correction for a source term (EMsolve3D.f90:298-303)
