@@ -251,7 +251,8 @@ MT3D_API int mt3d_fwdsolve(mt3d_handle h, int trans, const double *bc, const dou
  * (either may be NULL; an individual vector may be all zero); e holds nrhs full
  * edge vectors (initial guess in, solution out); status[r] receives each
  * right-hand side's mt3d_status.  The handle's frequency (mt3d_update_freq) is
- * left unchanged. */
+ * left unchanged.  1 <= nrhs <= 65535 (MT3D_INVALID_ARGUMENT otherwise, before
+ * any buffer is read). */
 MT3D_API int mt3d_fwdsolve_batch(mt3d_handle h, int nrhs, const double *omegas, const int *trans, const double *bc,
                         const double *src, double *e, int *status);
 

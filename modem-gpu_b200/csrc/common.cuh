@@ -19,6 +19,7 @@ constexpr double kSigmaAir = (double)1.0e-10f;  // single-precision literal in t
 
 constexpr int kThreads = 256;
 constexpr int kMaxParts = 4;  // doubles reduced per kernel (two complex numbers)
+constexpr int kMaxBatch = 65535;  // right-hand sides per solve call (the launch grids' y extent)
 
 // ---------------------------------------------------------------------------
 // complex helpers

@@ -933,6 +933,8 @@ int Solver::solve_begin(SolveRun &run, int nrhs, const double *omegas, const int
                         const double *src, double *e, int *status, bool device)
 {
     if (!cond_set) return fail(5, "fwdsolve: conductivity not set (call mt3d_update_cond)");
+    // the kernels index the right-hand sides by the grid's y dimension
+    if (nrhs > kMaxBatch) return fail(5, "fwdsolve: at most 65535 right-hand sides per call");
     if (nrhs < 1 || !omegas || !e) return fail(5, "fwdsolve: invalid arguments");
     for (int r = 0; r < nrhs; r++)
         if (!(omegas[r] > 0) || !std::isfinite(omegas[r])) return fail(5, "fwdsolve: omega must be positive and finite");

@@ -91,3 +91,52 @@ def test_batch_of_zero_rows_only(cuda, name):
     it, rr = s.batch_diagnostics(n)
     assert rc == 0 and np.all(st == 0)
     assert np.all(e == 0) and it.tolist() == [1, 0, 1] and np.all(rr == 0.0)
+
+
+@pytest.mark.parametrize("name", list(CONFIGS))
+def test_nan_row_leaves_the_others_alone(cuda, name):
+    """A row whose source holds a NaN is reported with status 3 (the
+    reference stops on `isnan(bnorm)`, f90/3D_MT/FWD_SP2/solver.f90:776-779;
+    a library must not stop its host) and the call returns 3; the rows beside
+    it still equal their single solves (each row's inner products are its
+    own, so a NaN cannot reach them)."""
+    cfg = CONFIGS[name]
+    g = small_grid()
+    m = random_model(g, seed=6)
+    s = _solver(g, m, cfg)
+    w = 2 * np.pi * 0.5
+    mask = interior_edge_mask(g) & earth_mask(g, m)
+    rng = np.random.default_rng(22)
+    src = np.where(mask, rng.standard_normal(g.n_edges) + 1j * rng.standard_normal(g.n_edges), 0)
+    bad = src.copy()
+    bad[np.flatnonzero(mask)[5]] = np.nan
+    zero = np.zeros(s.nE, complex)
+    oms = np.full(3, w)
+    trans = np.array([0, 1, 1], np.int32)
+    bcs = np.stack([mbc.boundary_1d(m, w, 1), zero, zero])
+    srcs = np.stack([zero, bad, src])
+    e, st, rc = s.fwdsolve_batch(oms, trans=trans, bc=bcs, src=srcs)
+    assert rc == 3 and st.tolist() == [0, 3, 0], st
+    s.update_freq(w)
+    for r in (0, 2):
+        e1, rc1 = s.fwdsolve(trans=bool(trans[r]), bc=bcs[r], src=srcs[r])
+        assert rc1 == 0
+        err = relerr(e[r], e1)
+        print(f"{name} row {r} beside a NaN row: batch vs single {err:.2e}")
+        assert err <= (1e-12 if cfg["precision"] == capi.PREC_FP64 else 1e-5)
+
+
+def test_batch_larger_than_the_launch_limit_is_refused(cuda):
+    """More right-hand sides than a launch grid's y extent (65535) are
+    refused with MT3D_INVALID_ARGUMENT before any buffer is read (the
+    device buffer given here holds one edge vector only)."""
+    import torch
+    g = small_grid()
+    m = random_model(g, seed=6)
+    s = _solver(g, m, CONFIGS["ccgd-mixed-poly"])
+    e = torch.zeros(s.nE, dtype=torch.complex128, device="cuda")
+    with pytest.raises(capi.MT3DError) as ei:
+        s.fwdsolve_batch_device(np.full(65536, 2 * np.pi), e.data_ptr())
+    assert ei.value.code == 5 and "65535" in str(ei.value)
+    st, rc = s.fwdsolve_batch_device(np.array([2 * np.pi]), e.data_ptr(), bc_ptr=None)
+    assert rc == 0  # the handle stays usable (a zero right-hand side)
