@@ -121,6 +121,32 @@ def test_multi_with_polynomial_preconditioner(mprob):
             s.set_control(IterPerDivCor=150, MaxDivCor=40, precision=capi.PREC_MIXED)
 
 
+def test_grid_with_nothing_to_solve(mprob):
+    """A grid of the batch whose right-hand sides are all zero (forward rows
+    without boundary data, a transposed row without a source) is done before
+    the first cycle: its fields come back zero with status 0 (one iteration
+    for a zero right-hand side, none for the source-less transposed row, as
+    the reference reports them), and the grids beside it, whose cycles run
+    on without it, give their per-grid solutions."""
+    probs, ss = mprob
+    bcs = [p[3] for p in probs]
+    srcs = [p[4] for p in probs]
+    bcs[1] = np.zeros_like(bcs[1])
+    srcs[1] = np.zeros_like(srcs[1])
+    es = [np.zeros((5, g.n_edges), complex) for g, *_ in probs]
+    st, rc = capi.fwdsolve_multi(ss, [p[2] for p in probs], es, trans=[p[5] for p in probs], bc=bcs, src=srcs)
+    assert rc == 0 and all(np.all(x == 0) for x in st)
+    it, rr = ss[1].batch_diagnostics(5)
+    assert np.all(es[1] == 0) and it.tolist() == [1, 1, 1, 1, 0] and np.all(rr == 0.0)
+    for k in (0, 2):
+        g, m, om, bc, src, tr = probs[k]
+        ref, _, rc1 = ss[k].fwdsolve_batch(om, trans=tr, bc=bc, src=src)
+        assert rc1 == 0
+        em = earth_mask(g, m)
+        for r in range(5):
+            assert relerr(es[k][r][em], ref[r][em]) < 1e-5, (g.nx, r)
+
+
 def test_chunk_counts_with_empty_chunks(mprob):
     """Chunk counts whose last chunk starts past the last node plane (6 of 15
     planes for the first grid: chunks of 3, the sixth empty; 6 of 19 and 9 of
