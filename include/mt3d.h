@@ -288,7 +288,12 @@ MT3D_API int mt3d_fwdsolve_multi_device(int nh, mt3d_handle *hs, const int *nrhs
                                         const int *zchunks);
 
 /* Run the handle's work on a caller-owned CUDA stream (a cudaStream_t passed
- * as void*); NULL restores the handle's own stream. */
+ * as void*); NULL restores the handle's own stream.  The handle's own stream
+ * is a blocking stream: it is ordered with the legacy default stream (whose
+ * handle is also NULL, e.g. torch's default stream), so device buffers a
+ * caller writes there are complete before the handle's next call reads them,
+ * and its results are complete before later default-stream work uses them.
+ * Work on other non-blocking streams must be ordered by the caller. */
 MT3D_API int mt3d_set_stream(mt3d_handle h, void *stream);
 
 /* Polls of one bounded device-side wait (the mbarrier waits of the FP32

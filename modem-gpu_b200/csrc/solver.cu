@@ -185,7 +185,11 @@ int Solver::create(int dev, int nx_, int ny_, int nz_, int nzAir_, const double 
     dev_ = dev;
     int rc;
     if ((rc = check(cudaSetDevice(dev_), "cudaSetDevice"))) return rc;
-    if ((rc = check(cudaStreamCreateWithFlags(&own_stream_, cudaStreamNonBlocking), "cudaStreamCreate"))) return rc;
+    // a blocking stream: ordered with the legacy default stream, so device
+    // buffers a caller fills there (stream handle 0, as torch's default
+    // stream reports itself, which mt3d_set_stream also reads as "the
+    // handle's own stream") are complete before the handle's work reads them
+    if ((rc = check(cudaStreamCreateWithFlags(&own_stream_, cudaStreamDefault), "cudaStreamCreate"))) return rc;
     stream_ = own_stream_;
 
     pl_.Px = (nx + 1 + 3) / 4 * 4;
